@@ -1,0 +1,366 @@
+#!/usr/bin/env python3
+"""Benchmark: 24^3 x 64 Iwasaki (beta = 2.13, c1 = -0.331) pure-gauge HMC,
+force-gradient integrator with 8 steps per unit trajectory, on one B200 per
+rank.  One "step" is one full trajectory (momentum refresh, molecular
+dynamics, both Hamiltonians, Metropolis) through the qlat-compatible API.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is trajectories/s of the mixed form
+(FP32 molecular dynamics, FP64 Hamiltonians, FP64 re-unitarisation every 4
+steps), summed over ranks (independent chains, one per GPU: the path has no
+cross-chain exchange, so multi-GPU runs are replicas).  The plain FP64 form is
+timed in the same run and reported beside it.
+
+`--impl reference` times the reference Qlattice CPU implementation (built
+from source into oracle/_ref by oracle/ref/Makefile) on this host's cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LATTICE = (24, 24, 24, 64)
+BETA, C1 = 2.13, -0.331
+N_STEP = 8
+SIGMA = 0.3
+SEED = "b200-c2-24x64-iwasaki"
+METRIC = "24^3x64 Iwasaki HMC traj/s (force-gradient, 8 steps/traj; mixed FP32/FP64)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--lattice", type=str, default=",".join(map(str, LATTICE)))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline (oracle/_ref: the reference's own C++ library)
+
+def ref_bench_path():
+    p = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    return p if os.path.exists(p) else None
+
+
+def run_ref_sample(lattice, samples, threads):
+    """Time the reference CPU code: the per-trajectory ends once and
+    `samples` (set_gm_force + gf_evolve) pairs; a force-gradient trajectory
+    with 8 steps is 32 such pairs plus the ends (one extra gf_evolve ignored)."""
+    exe = ref_bench_path()
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), q_verbose="-1")
+    t0 = time.time()
+    out = subprocess.run([exe, *map(str, lattice), str(BETA), str(C1), str(SIGMA), str(samples)],
+                         capture_output=True, text=True, env=env, check=True).stdout
+    wall = time.time() - t0
+    line = [ln for ln in out.splitlines() if ln.startswith("{")][-1]
+    r = json.loads(line)
+    traj_s = 4 * N_STEP * r["t_force_evolve"] + r["t_ends"]
+    return r, traj_s, wall
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    lattice = tuple(int(v) for v in args.lattice.split(","))
+    if ref_bench_path() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built "
+                          "(the reference sources were not present when build() ran)"}))
+        return 0
+    threads = os.cpu_count() or 1
+    # warm-up: one sample; timed: `steps` samples of one force + evolve pair each
+    run_ref_sample(lattice, max(1, min(args.warmup, 1)), threads)
+    r, traj_s, wall = run_ref_sample(lattice, max(1, args.steps), threads)
+    value = 1.0 / traj_s
+    sample = (f"{r['samples']} x (set_gm_force + gf_evolve) on {'x'.join(map(str, lattice))} + one set of "
+              f"trajectory ends (momentum refresh, 2 x H, unitarize); traj time = 32 pairs + ends")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": traj_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded hot start set_rand(sigma=0.3)",
+        "config": {"workload": f"{'x'.join(map(str, lattice))} Iwasaki beta=2.13 FG n_step=8 (reference CPU, FP64)",
+                   "lattice": list(lattice), "sites": r["sites"]},
+        "cpu_baseline": {"value": value, "unit": "traj/s", "cores": r["threads"], "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "detail": {"t_force_evolve_s": r["t_force_evolve"], "t_ends_s": r["t_ends"], "wall_s": wall},
+    }))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in out.splitlines():
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(lattice):
+    """Bounded sample of the reference CPU code on this host (rank 0, N = 1)."""
+    if ref_bench_path() is None:
+        return {"value": None, "unit": "traj/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/ref_bench not built"}
+    threads = os.cpu_count() or 1
+    r, traj_s, wall = run_ref_sample(lattice, 2, threads)
+    return {"value": 1.0 / traj_s, "unit": "traj/s", "cores": r["threads"], "kind": "reference",
+            "sample": f"2 x (set_gm_force + gf_evolve) + trajectory ends on {'x'.join(map(str, lattice))}, "
+                      f"extrapolated to 32 pairs + ends per trajectory ({wall:.1f} s of CPU work)"}
+
+
+def our_arm(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    from qlat_b200 import build as B
+    B.build()
+    import qlat_b200 as q
+    q.set_device(torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    q.set_stream(stream.cuda_stream)
+
+    lattice = tuple(int(v) for v in args.lattice.split(","))
+    V = 1
+    for v in lattice:
+        V *= v
+    geo = q.Geometry(lattice)
+    ga = q.GaugeAction(BETA, C1)
+    rs = q.RngState(SEED).split(f"rank-{rank}")
+    gf = q.GaugeField(geo)
+    gf.set_rand(rs.split("gf-init"), SIGMA, 1)
+    gf0 = q.GaugeField(geo)
+    gm = q.GaugeMomentum(geo)
+
+    def trajectory(traj, precision):
+        r = rs.split(f"{traj}")
+        gf0 @= gf
+        gm.set_rand(r.split("set_rand_gauge_momentum"), 1.0)
+        dh = q.run_hmc_evolve_pure_gauge(gm, gf0, ga, r, N_STEP, 1.0, precision=precision, reunit_interval=4)
+        flag, _ = q.metropolis_accept(dh, traj, r.split("metropolis_accept"))
+        if flag:
+            gf @= gf0
+        return dh, flag
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(n, precision, first_traj, prof=False):
+        dhs, flags = [], []
+        barrier()
+        torch.cuda.synchronize()
+        if prof:
+            q.prof_reset()
+            q.prof_enable(True)
+        l0 = q.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(n):
+            dh, fl = trajectory(first_traj + i, precision)
+            dhs.append(dh)
+            flags.append(fl)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if prof:
+            q.prof_enable(False)
+        launches = q.launch_count() - l0
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, dhs, flags, launches
+
+    # warm-up (W trajectories of each form; always accepted state evolves normally)
+    traj = 0
+    for _ in range(max(args.warmup, 3)):
+        traj += 1
+        trajectory(traj, "mixed")
+    for _ in range(max(args.warmup, 3)):
+        traj += 1
+        trajectory(traj, "fp64")
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ms_mixed, dh_mixed, fl_mixed, launches = timed(args.steps, "mixed", traj + 1, prof=True)
+    traj += args.steps
+    clk = clocks.stop()
+    prof = {k: q.prof_get(k) for k in ("force_update", "force_evolve", "evolve", "reduce", "rng", "convert",
+                                          "unitarize")}
+    ms_fp64, dh_fp64, fl_fp64, _ = timed(args.steps, "fp64", traj + 1)
+    traj += args.steps
+
+    # matched-delta-H check: both forms from the same state and momenta
+    r = rs.split("dh-check")
+    g_a, g_b = gf.copy(), gf.copy()
+    m_a = q.GaugeMomentum(geo)
+    m_a.set_rand(r.split("mom"), 1.0)
+    m_b = m_a.copy()
+    dh_chk64 = q.run_hmc_evolve_pure_gauge(m_a, g_a, ga, r, N_STEP, 1.0, precision="fp64")
+    dh_chkmx = q.run_hmc_evolve_pure_gauge(m_b, g_b, ga, r, N_STEP, 1.0, precision="mixed", reunit_interval=4)
+    plaq_64, plaq_mx = q.gf_avg_plaq(g_a), q.gf_avg_plaq(g_b)
+    del g_a, g_b, m_a, m_b
+
+    # end to end through the public API: host gauge configuration in pinned
+    # memory uploaded every step, trajectory, delta_h + plaquette read back
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((V, 4, 3, 3), dtype=torch.complex128, pin_memory=True)
+        host.numpy()[...] = gf.to_numpy()
+        n_e2e = max(2, min(args.steps, 5))
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(n_e2e):
+            q._lib.call("qgb_field_upload", gf.handle, q._lib.ctypes.cast(host.data_ptr(), q._lib.c_dbl_p))
+            dh, fl = trajectory(traj + 1 + i, "mixed")
+            _ = q.gf_avg_plaq(gf)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e2e = float(t.item())
+        e2e = {"value": world * n_e2e / (ms_e2e / 1e3), "unit": "traj/s",
+               "h2d_bytes_per_step": V * 4 * 9 * 16, "d2h_bytes_per_step": 8 * 2 + 8 * 6}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    value = world * args.steps / (ms_mixed / 1e3)
+    fp64_value = world * args.steps / (ms_fp64 / 1e3)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    # dominant kernel: the fused force + momentum update (FP32, Iwasaki):
+    # reads U (288 B/site) and P (288 B/site), writes P (288 B/site)
+    t_fu, n_fu = prof["force_update"]
+    bytes_fu = 864.0 * V
+    achieved = bytes_fu / (t_fu / n_fu / 1e3) / 1e9 if n_fu else None
+    flops_site = 4 * (6 * 11 + 1) * 198.0  # matrix products per link x flops per product
+    tflops = flops_site * V / (t_fu / n_fu / 1e3) / 1e12 if n_fu else None
+    traffic = None
+    tf_path = os.path.join(ROOT, "profiles", "force_update_traffic.json")
+    if os.path.exists(tf_path):
+        try:
+            traffic = json.load(open(tf_path)).get("bytes_per_launch_full_size")
+        except Exception:
+            traffic = None
+    out = {
+        "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (MD) + f64 (H, unitarize)",
+        "data": "synthetic: seeded hot start set_rand(RngState('b200-c2-24x64-iwasaki').split('gf-init'), 0.3)",
+        "config": {"workload": f"{'x'.join(map(str, lattice))} Iwasaki beta=2.13 c1=-0.331, force-gradient "
+                               f"n_step=8 md_time=1, one chain per GPU", "lattice": list(lattice), "sites": V,
+                   "l2_policy": "inputs larger than L2 (FP64 links 509.6 MB, FP32 254.8 MB per chain)",
+                   "parallelism": f"replicas x{world}"},
+        "fp64_traj_per_s": fp64_value, "mixed_over_fp64": value / fp64_value,
+        "link_updates_per_s": value * 4 * V * N_STEP,
+        "delta_h": {"mixed_mean": statistics.fmean(dh_mixed), "fp64_mean": statistics.fmean(dh_fp64),
+                    "check_same_start_fp64": dh_chk64, "check_same_start_mixed": dh_chkmx,
+                    "check_plaq_fp64": plaq_64, "check_plaq_mixed": plaq_mx,
+                    "accept_rate_mixed": sum(fl_mixed) / len(fl_mixed)},
+        "roofline": {"kernel": "force_update (FP32 Iwasaki force fused with P += dt F)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
+                     "algorithmic_bytes_per_launch": bytes_fu, "mean_launch_ms": t_fu / n_fu if n_fu else None,
+                     "fp32_tflops_achieved": tflops, "flops_per_site": flops_site,
+                     "note": "compute-bound on CUDA cores (FP32); HBM fraction is reported as the metric asks"},
+        "kernel_ms_per_traj": {k: v[0] / args.steps for k, v in prof.items()},
+        "clocks": clk, "gpu_launches": launches,
+    }
+    if e2e:
+        out["e2e"] = e2e
+    if not args.no_cpu_baseline and world == 1:
+        out["cpu_baseline"] = cpu_baseline(lattice)
+    print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

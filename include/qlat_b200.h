@@ -1,0 +1,195 @@
+/* qlat_b200.h -- C ABI of the B200-native pure-gauge SU(3) hot path.
+ *
+ * This is the drop-in boundary for Qlattice's pure-gauge HMC and gradient-flow
+ * path.  Every entry point below replaces one C++ function that Qlattice's
+ * Cython layer binds (qlat/qlat/everything.pxd) or that the C++ drivers call
+ * (examples-cpp/hmc/main.cpp); the reference declaration is cited beside it.
+ * Paths are inside the Qlattice project.
+ *
+ * Conventions
+ *  - Every function returns an int status: QGB_OK (0) or one of the QGB_ERR_*
+ *    codes; qgb_last_error() gives a message for the calling thread.  This
+ *    replaces the reference's `qerr` C++ exceptions, which Cython turns into
+ *    RuntimeError (`except +`).
+ *  - A qgb_field is an opaque handle to a lattice field resident in GPU
+ *    memory: a GaugeField (multiplicity 4, color matrices), a GaugeMomentum
+ *    (same shape), or a Field<RealD> (real numbers, any multiplicity).  It is
+ *    stored in FP64 or FP32 (QGB_F64 / QGB_F32).
+ *  - Host buffers passed to upload/download use the reference memory image
+ *    (core.h:753-861): site-major, x fastest (coordinate.h:182-188), then the
+ *    multiplicity index, then a row-major 3x3 complex matrix of (re, im)
+ *    doubles -- i.e. exactly what np.asarray(qlat.GaugeField) exposes.
+ *  - RngState crosses the boundary in its 24 x uint32 serialised form
+ *    (rng-state.cpp:61-81, exportRngState / importRngState).
+ *  - Work is queued on the library's current CUDA stream (qgb_set_stream);
+ *    functions that return host scalars synchronise that stream.
+ *  - Single GPU, single node: the `_node` functions are whole-lattice sums.
+ */
+#ifndef QLAT_B200_H
+#define QLAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QGB_OK 0
+#define QGB_ERR_INVALID_ARG 1
+#define QGB_ERR_BAD_GEOMETRY 2
+#define QGB_ERR_ALLOC 3
+#define QGB_ERR_CUDA 4
+#define QGB_ERR_NAN 5
+#define QGB_ERR_TIMEOUT 6
+#define QGB_ERR_MISMATCH 7
+#define QGB_ERR_NO_DEVICE 8
+
+#define QGB_F64 64
+#define QGB_F32 32
+
+#define QGB_KIND_COLOR_MATRIX 0
+#define QGB_KIND_REAL 1
+
+#define QGB_INTEGRATOR_FORCE_GRADIENT 0
+#define QGB_INTEGRATOR_LEAPFROG 1
+
+typedef struct qgb_field_s qgb_field;
+
+/* ---- library state ---------------------------------------------------- */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* qgb_last_error(void);
+/* Library version as an integer (major*10000 + minor*100 + patch). */
+int qgb_version(void);
+/* Select the CUDA device used by subsequent calls of this thread. */
+int qgb_set_device(int32_t device);
+/* Use `stream` (a cudaStream_t, may be NULL for the legacy default stream)
+ * for all subsequent work; the library otherwise creates its own stream. */
+int qgb_set_stream(void* stream);
+int qgb_synchronize(void);
+
+/* ---- fields (Field<M> / GaugeField / GaugeMomentum: core.h:753-969) ------ */
+
+/* Geometry(total_site) + Field::init(geo, multiplicity) (core.h:92-359,
+ * 753-781); kind is QGB_KIND_COLOR_MATRIX or QGB_KIND_REAL. */
+int qgb_field_create(qgb_field** out, const int32_t total_site[4], int32_t multiplicity, int32_t kind,
+                     int32_t precision);
+int qgb_field_destroy(qgb_field* f);
+int qgb_field_info(const qgb_field* f, int32_t total_site[4], int32_t* multiplicity, int32_t* kind,
+                   int32_t* precision);
+/* Copy a host buffer in the reference memory image into the field (and back).
+ * Color-matrix fields take complex128 (double pairs); real fields take double. */
+int qgb_field_upload(qgb_field* f, const double* host);
+int qgb_field_download(const qgb_field* f, double* host);
+/* Same, from / into a device buffer in the reference memory image. */
+int qgb_field_upload_device(qgb_field* f, const double* dev);
+int qgb_field_download_device(const qgb_field* f, double* dev);
+/* f1 @= f2 (field_types.pyx.in:92 `@=`); converts between FP64 and FP32. */
+int qgb_field_copy(qgb_field* dst, const qgb_field* src);
+int qgb_field_set_zero(qgb_field* f);
+/* y = a*x + b*y: covers `f *= s` (x = y or a = 0), `f += g`, `f -= g`
+ * (field.h operators used by hmc.pyx:166-167 and wilson-flow.cpp:36-46). */
+int qgb_field_axpby(qgb_field* y, double a, const qgb_field* x, double b);
+/* qnorm(field) = sum of |element|^2 (field.h, qnorm). */
+int qgb_field_qnorm(const qgb_field* f, double* out);
+
+/* ---- RngState (rng-state.h:12-99, lib/rng-state.cpp:150-281) ------------ */
+
+/* RngState(seed): reset(rs, seed). */
+int qgb_rng_seed(uint32_t out[24], const char* seed);
+/* rs.split(sindex) (split_rng_state, rng-state.cpp:173-201). */
+int qgb_rng_split(uint32_t out[24], const uint32_t rs[24], const char* sindex);
+/* rand_gen / u_rand_gen / g_rand_gen (rng-state.cpp:203-281); update rs. */
+int qgb_rng_rand_gen(uint32_t rs[24], uint64_t* out);
+int qgb_rng_u_rand_gen(uint32_t rs[24], double upper, double lower, double* out);
+int qgb_rng_g_rand_gen(uint32_t rs[24], double center, double sigma, double* out);
+
+/* ---- hot path: gauge field set-up (qcd-utils.cpp:47-92, qcd.pyx:69) ----- */
+
+/* set_unit(gf) (field.h set_unit, everything.pxd:187). */
+int qgb_set_unit(qgb_field* gf);
+/* GaugeField.set_rand(rs, sigma, n_step) -> set_g_rand_color_matrix_field
+ * (qcd-utils.cpp:71-92): per site RngState(rs, gindex), n_step products of
+ * exp(X) (order-20 Taylor, then unitarize) with X from 8 Gaussians of std
+ * sigma/sqrt(2). */
+int qgb_gf_set_rand(qgb_field* gf, const uint32_t rs[24], double sigma, int32_t n_step);
+
+/* ---- hot path: HMC (hmc.h:20-114, everything.pxd:437-456) --------------- */
+
+/* set_rand_gauge_momentum(gm, sigma, rs) (hmc.cpp:107-119). */
+int qgb_set_rand_gauge_momentum(qgb_field* gm, double sigma, const uint32_t rs[24]);
+/* gm_hamilton_node(gm) (hmc.cpp:151-173). */
+int qgb_gm_hamilton_node(const qgb_field* gm, double* out);
+/* gf_hamilton_node(gf, ga) (hmc.cpp:254-298). */
+int qgb_gf_hamilton_node(const qgb_field* gf, double beta, double c1, double* out);
+/* gf_sum_re_tr_plaq_node_no_comm / gf_sum_re_tr_rect_node_no_comm (hmc.cpp:203-252). */
+int qgb_gf_sum_re_tr_plaq_node(const qgb_field* gf, double* out);
+int qgb_gf_sum_re_tr_rect_node(const qgb_field* gf, double* out);
+/* gf_avg_plaq(gf) (qcd.cpp:94-142). */
+int qgb_gf_avg_plaq(const qgb_field* gf, double* out);
+/* set_gm_force(gm_force, gf, GaugeAction(beta, c1)) (hmc.cpp:466-490). */
+int qgb_set_gm_force(qgb_field* gm_force, const qgb_field* gf, double beta, double c1);
+/* gf_evolve(gf, gm, step_size) (hmc.cpp:311-328). */
+int qgb_gf_evolve(qgb_field* gf, const qgb_field* gm, double step_size);
+/* gm_evolve_fg_pure_gauge(gm, gf_init, ga, fg_dt, dt) (hmc.pyx:157-167). */
+int qgb_gm_evolve_fg(qgb_field* gm, const qgb_field* gf_init, double beta, double c1, double fg_dt,
+                     double dt);
+/* unitarize(gf) (qcd.cpp:346-359). */
+int qgb_unitarize(qgb_field* gf);
+/* metropolis_accept(accept_prob, delta_h, traj, rs) (hmc.cpp:77-105). */
+int qgb_metropolis_accept(double delta_h, int32_t traj, const uint32_t rs[24], double* accept_prob,
+                          int32_t* flag);
+/* run_hmc_evolve_pure_gauge(gm, gf, ga, rs, n_step, md_time) (hmc.pyx:169-188),
+ * force-gradient or leapfrog (examples-py/hmc-pure-gauge-fgf.py:57-69), all
+ * in the fields' precision (FP64 for the plain form); writes delta_h. */
+int qgb_run_hmc_evolve(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step,
+                       double md_time, int32_t integrator, double* delta_h);
+/* Mixed form of the same trajectory: gm and gf are FP64; molecular dynamics
+ * runs on FP32 copies, links are re-unitarised in FP64 arithmetic every
+ * `reunit_interval` steps, and both Hamiltonians are FP64 sums on FP64 fields. */
+int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step,
+                             double md_time, int32_t integrator, int32_t reunit_interval,
+                             double* delta_h);
+
+/* ---- hot path: gradient flow (wilson-flow.h:9-43, everything.pxd:514-521) --- */
+
+/* set_wilson_flow_z(z, gf, c1) = set_gm_force with beta = 3 (wilson-flow.cpp:12-17). */
+int qgb_set_wilson_flow_z(qgb_field* z, const qgb_field* gf, double c1);
+/* gf_wilson_flow_step(gf, epsilon, c1): Luescher RK3 (wilson-flow.cpp:29-50). */
+int qgb_gf_wilson_flow_step(qgb_field* gf, double epsilon, double c1);
+/* gf_wilson_flow_step_euler(gf, epsilon, c1) (wilson-flow.cpp:19-27). */
+int qgb_gf_wilson_flow_step_euler(qgb_field* gf, double epsilon, double c1);
+/* gf_energy_density_field(fd, gf) (wilson-flow.cpp:99-129); fd: real, multiplicity 1. */
+int qgb_gf_energy_density_field(qgb_field* fd, const qgb_field* gf);
+/* gf_energy_density(gf) (wilson-flow.cpp:131-141). */
+int qgb_gf_energy_density(const qgb_field* gf, double* out);
+/* gf_wilson_flow(gf, existing_flow_time, flow_time, steps, c1) (wilson-flow.cpp:144-162);
+ * energy_list receives `steps` energy densities. */
+int qgb_gf_wilson_flow(qgb_field* gf, double flow_time, int32_t steps, double c1, double* energy_list);
+
+/* ---- hot path: topology (qcd-topology.h, everything.pxd:531-535) --------- */
+
+/* clf_topology_field(topf, gf) (qcd.cpp:416-423, 608-619); topf: real, multiplicity 1. */
+int qgb_clf_topology_field(qgb_field* topf, const qgb_field* gf);
+/* gf_topology_clf(gf) = glb_sum of clf_topology_field (topology.pyx:89-96). */
+int qgb_gf_topology_clf(const qgb_field* gf, double* out);
+
+/* ---- instrumentation (timer.h:48-414 TIMER / Timer::display) ------------ */
+
+/* Per-kernel-class device timing with CUDA events on the library stream. */
+int qgb_prof_enable(int32_t on);
+int qgb_prof_reset(void);
+/* name: "force", "force_update", "force_evolve", "evolve", "reduce", "rng",
+ * "unitarize", "convert", "clover", "flow_stage"; totals since the last reset. */
+int qgb_prof_get(const char* name, double* total_ms, int64_t* launches);
+/* Number of kernels this library has launched since it was loaded. */
+int qgb_launch_count(int64_t* out);
+/* Number of Gaussian draws whose logarithm could not be proven correctly
+ * rounded (expected 0); cumulative since library load. */
+int qgb_rng_ambiguous_count(int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QLAT_B200_H */

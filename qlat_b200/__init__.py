@@ -1,0 +1,76 @@
+"""qlat_b200 -- B200-native pure-gauge SU(3) hot path with Qlattice's API.
+
+``import qlat_b200 as q`` gives the names a Qlattice user calls for
+pure-gauge HMC and gradient flow (GaugeField, GaugeMomentum, GaugeAction,
+RngState, set_gm_force, gf_evolve, run_hmc_pure_gauge, gf_wilson_flow, ...),
+backed by hand-written sm_100a CUDA kernels behind the C ABI declared in
+include/qlat_b200.h.  Fields live in GPU memory.  There is no CPU fallback:
+the first call loads the built libqlat_b200.so and raises if it is missing
+(build it with `python -m qlat_b200.build`).
+"""
+
+from ._lib import QlatB200Error, load as _load
+from .field import (F32, F64, Coordinate, Field, FieldColorMatrix, FieldRealD, GaugeAction, GaugeField,
+                    GaugeMomentum, Geometry, RngState, set_unit)
+from .hmc import (gf_avg_plaq, gf_evolve, gf_hamilton, gf_hamilton_node, gf_sum_re_tr_plaq_node_no_comm,
+                  gf_sum_re_tr_rect_node_no_comm, glb_sum_double, gm_evolve_fg_pure_gauge, gm_hamilton_node,
+                  metropolis_accept, metropolis_accept_cpp, run_hmc_evolve_pure_gauge, run_hmc_pure_gauge,
+                  set_gm_force, set_rand_gauge_momentum, unitarize)
+from .wilson_flow import (gf_energy_density, gf_energy_density_field, gf_energy_derivative_density_field,
+                          gf_topology_clf, gf_topology_field_clf, gf_wilson_flow, gf_wilson_flow_force,
+                          gf_wilson_flow_step)
+
+__version__ = "0.1.0"
+
+
+def prof_enable(on: bool = True):
+    from ._lib import call
+    call("qgb_prof_enable", int(bool(on)))
+
+
+def prof_reset():
+    from ._lib import call
+    call("qgb_prof_reset")
+
+
+def prof_get(name: str):
+    """(total_ms, launches) of a kernel class since the last reset."""
+    import ctypes
+    from ._lib import call
+    t = ctypes.c_double()
+    n = ctypes.c_int64()
+    call("qgb_prof_get", name.encode(), ctypes.byref(t), ctypes.byref(n))
+    return t.value, int(n.value)
+
+
+def rng_ambiguous_count() -> int:
+    import ctypes
+    from ._lib import call
+    n = ctypes.c_int64()
+    call("qgb_rng_ambiguous_count", ctypes.byref(n))
+    return int(n.value)
+
+
+def launch_count() -> int:
+    import ctypes
+    from ._lib import call
+    n = ctypes.c_int64()
+    call("qgb_launch_count", ctypes.byref(n))
+    return int(n.value)
+
+
+def set_stream(stream_ptr: int):
+    """Queue all library work on this cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
+    import ctypes
+    from ._lib import call
+    call("qgb_set_stream", ctypes.c_void_p(stream_ptr))
+
+
+def set_device(device: int):
+    from ._lib import call
+    call("qgb_set_device", int(device))
+
+
+def synchronize():
+    from ._lib import call
+    call("qgb_synchronize")

@@ -1,0 +1,1053 @@
+// capi.cu -- host runtime behind the C ABI (include/qlat_b200.h).
+//
+// One process-wide context per device holds the CUDA stream, the reduction
+// scratch (per-block partial sums and result slots), upload/download staging
+// and the temporary fields of the integrators, all allocated once and reused.
+// Entry points queue kernels on the context stream and synchronise only when
+// they return a host scalar, so a trajectory is a single stream of kernels
+// with one device-to-host read at its end.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/qlat_b200.h"
+#include "kernels.h"
+
+using qgb::ForceArgs;
+using qgb::Geo;
+
+struct qgb_field_s {
+  int32_t dims[4];
+  long V;
+  int32_t mult;
+  int32_t kind;
+  int32_t prec;
+  void* d;
+  size_t bytes;
+};
+
+namespace
+{
+
+thread_local std::string g_err;
+std::recursive_mutex g_mu;
+
+int fail(int code, const std::string& msg)
+{
+  g_err = msg;
+  return code;
+}
+
+#define QGB_TRY_CUDA(expr)                                                             \
+  do {                                                                                 \
+    cudaError_t e_ = (expr);                                                           \
+    if (e_ != cudaSuccess) return fail(QGB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define QGB_CHECK(cond, code, msg) \
+  do {                             \
+    if (!(cond)) return fail((code), (msg)); \
+  } while (0)
+
+struct ProfEntry {
+  double total_ms = 0;
+  int64_t launches = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+};
+
+struct Ctx {
+  bool ready = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double* partials = nullptr;
+  size_t partials_cap = 0;  // doubles
+  double* results = nullptr;  // device result slots
+  double* results_host = nullptr;  // pinned mirror
+  static const int NSLOT = 64;
+  int* ambiguous = nullptr;  // device counter of uncertified log roundings
+  double* staging = nullptr;
+  size_t staging_cap = 0;  // bytes
+  std::map<std::pair<size_t, int>, std::vector<void*>> scratch;  // (bytes, tag) -> buffers
+  bool prof_on = false;
+  std::map<std::string, ProfEntry> prof;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+Ctx g_ctx;
+int64_t g_launches = 0;  // kernels launched by this library
+
+int ensure_ctx()
+{
+  if (g_ctx.ready) return QGB_OK;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(QGB_ERR_NO_DEVICE, "no CUDA device available");
+  QGB_TRY_CUDA(cudaGetDevice(&g_ctx.device));
+  QGB_TRY_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+  g_ctx.own_stream = true;
+  QGB_TRY_CUDA(cudaMalloc(&g_ctx.results, Ctx::NSLOT * sizeof(double)));
+  QGB_TRY_CUDA(cudaMallocHost(&g_ctx.results_host, Ctx::NSLOT * sizeof(double)));
+  QGB_TRY_CUDA(cudaMalloc(&g_ctx.ambiguous, sizeof(int)));
+  QGB_TRY_CUDA(cudaMemset(g_ctx.ambiguous, 0, sizeof(int)));
+  qgb::init_constants();
+  QGB_TRY_CUDA(cudaGetLastError());
+  g_ctx.ready = true;
+  return QGB_OK;
+}
+
+#define QGB_CTX()                      \
+  std::lock_guard<std::recursive_mutex> lock_(g_mu); \
+  do {                                 \
+    int rc_ = ensure_ctx();            \
+    if (rc_ != QGB_OK) return rc_;     \
+  } while (0)
+
+cudaEvent_t get_event()
+{
+  if (!g_ctx.event_pool.empty()) {
+    cudaEvent_t e = g_ctx.event_pool.back();
+    g_ctx.event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// RAII timing of one kernel launch on the context stream (when enabled).
+struct Prof {
+  const char* name;
+  cudaEvent_t a = nullptr, b = nullptr;
+  explicit Prof(const char* n, int nk = 1) : name(n)
+  {
+    g_launches += nk;
+    if (!g_ctx.prof_on) return;
+    a = get_event();
+    b = get_event();
+    cudaEventRecord(a, g_ctx.stream);
+  }
+  ~Prof()
+  {
+    if (!a) return;
+    cudaEventRecord(b, g_ctx.stream);
+    g_ctx.prof[name].pending.emplace_back(a, b);
+  }
+};
+
+void prof_collect()
+{
+  for (auto& kv : g_ctx.prof) {
+    ProfEntry& p = kv.second;
+    if (p.pending.empty()) continue;
+    cudaStreamSynchronize(g_ctx.stream);
+    for (auto& ev : p.pending) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev.first, ev.second);
+      p.total_ms += ms;
+      p.launches += 1;
+      g_ctx.event_pool.push_back(ev.first);
+      g_ctx.event_pool.push_back(ev.second);
+    }
+    p.pending.clear();
+  }
+}
+
+Geo geo_of(const qgb_field_s* f)
+{
+  Geo g;
+  for (int i = 0; i < 4; ++i) g.d[i] = f->dims[i];
+  g.V = f->V;
+  return g;
+}
+
+size_t elem_reals(const qgb_field_s* f) { return f->kind == QGB_KIND_COLOR_MATRIX ? 18 : 1; }
+long n_reals(const qgb_field_s* f) { return f->V * f->mult * (long)elem_reals(f); }
+
+int ensure_partials(size_t n)
+{
+  if (g_ctx.partials_cap >= n) return QGB_OK;
+  if (g_ctx.partials) cudaFree(g_ctx.partials);
+  g_ctx.partials = nullptr;
+  QGB_TRY_CUDA(cudaMalloc(&g_ctx.partials, n * sizeof(double)));
+  g_ctx.partials_cap = n;
+  return QGB_OK;
+}
+
+int ensure_staging(size_t bytes)
+{
+  if (g_ctx.staging_cap >= bytes) return QGB_OK;
+  if (g_ctx.staging) cudaFree(g_ctx.staging);
+  g_ctx.staging = nullptr;
+  QGB_TRY_CUDA(cudaMalloc(&g_ctx.staging, bytes));
+  g_ctx.staging_cap = bytes;
+  return QGB_OK;
+}
+
+// Reusable device buffers of a given size; `tag` distinguishes simultaneous uses.
+int get_scratch(size_t bytes, int tag, void** out)
+{
+  auto& v = g_ctx.scratch[std::make_pair(bytes, tag)];
+  if (v.empty()) {
+    void* p = nullptr;
+    QGB_TRY_CUDA(cudaMalloc(&p, bytes));
+    v.push_back(p);
+  }
+  *out = v[0];
+  return QGB_OK;
+}
+
+int read_results(int slot, int n, double* out)
+{
+  QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.results_host + slot, g_ctx.results + slot, n * sizeof(double),
+                               cudaMemcpyDeviceToHost, g_ctx.stream));
+  QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  for (int i = 0; i < n; ++i) out[i] = g_ctx.results_host[slot + i];
+  return QGB_OK;
+}
+
+int check_field(const qgb_field* f, int kind, const char* what)
+{
+  if (!f) return fail(QGB_ERR_INVALID_ARG, std::string(what) + ": null field");
+  if (kind >= 0 && f->kind != kind) return fail(QGB_ERR_MISMATCH, std::string(what) + ": wrong field kind");
+  return QGB_OK;
+}
+
+bool same_geo(const qgb_field* a, const qgb_field* b)
+{
+  for (int i = 0; i < 4; ++i)
+    if (a->dims[i] != b->dims[i]) return false;
+  return true;
+}
+
+#define QGB_RC(expr)            \
+  do {                          \
+    int rc__ = (expr);          \
+    if (rc__ != QGB_OK) return rc__; \
+  } while (0)
+
+// ---- reductions --------------------------------------------------------
+
+template <typename R>
+int gm_hamilton_to(const qgb_field* gm, int slot)
+{
+  const Geo g = geo_of(gm);
+  const int nb = qgb::reduce_blocks(g);
+  QGB_RC(ensure_partials((size_t)nb));
+  {
+    Prof p("reduce", 2);
+    QGB_TRY_CUDA(qgb::launch_gm_hamilton<R>(g, gm->d, g_ctx.partials, g_ctx.stream));
+    QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, slot, g_ctx.stream));
+  }
+  return QGB_OK;
+}
+
+int gm_hamilton_slot(const qgb_field* gm, int slot)
+{
+  return gm->prec == QGB_F64 ? gm_hamilton_to<double>(gm, slot) : gm_hamilton_to<float>(gm, slot);
+}
+
+// slots: slot = plaq sum, slot+1 = rect sum (if rect)
+int action_slot(const qgb_field* gf, int rect, int slot)
+{
+  const Geo g = geo_of(gf);
+  const int nb = qgb::reduce_blocks(g);
+  QGB_RC(ensure_partials((size_t)nb * 2));
+  Prof p("reduce", 2);
+  if (gf->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_action<double>(g, gf->d, rect, g_ctx.partials, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_action<float>(g, gf->d, rect, g_ctx.partials, g_ctx.stream));
+  QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, rect ? 2 : 1, nb, g_ctx.results, slot, g_ctx.stream));
+  return QGB_OK;
+}
+
+int clover_slot(const qgb_field* gf, qgb_field* ef, qgb_field* qf, int slot)
+{
+  const Geo g = geo_of(gf);
+  const int nb = qgb::reduce_blocks(g);
+  QGB_RC(ensure_partials((size_t)nb * 2));
+  Prof p("clover", 2);
+  if (gf->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_clover<double>(g, gf->d, ef ? ef->d : nullptr, qf ? qf->d : nullptr, g_ctx.partials,
+                                            g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_clover<float>(g, gf->d, ef ? ef->d : nullptr, qf ? qf->d : nullptr, g_ctx.partials,
+                                           g_ctx.stream));
+  QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 2, nb, g_ctx.results, slot, g_ctx.stream));
+  return QGB_OK;
+}
+
+double gf_hamilton_from(double sp, double sr, double beta, double c1)
+{
+  // hmc.cpp:254-277
+  return -beta / 3.0 * ((1.0 - 8.0 * c1) * sp + c1 * (c1 == 0.0 ? 0.0 : sr));
+}
+
+// ---- elementary launches with profiling -----------------------------------
+
+template <typename R>
+int force(const Geo& g, qgb::ForceMode mode, const ForceArgs& a)
+{
+  static const char* names[] = {"force", "force_update", "force_evolve", "flow_stage"};
+  Prof p(names[mode]);
+  QGB_TRY_CUDA(qgb::launch_force<R>(g, mode, a, g_ctx.stream));
+  return QGB_OK;
+}
+
+template <typename R>
+int evolve(const Geo& g, void* U, const void* P, double eps, int unit)
+{
+  Prof p("evolve");
+  QGB_TRY_CUDA(qgb::launch_evolve<R>(g, U, P, eps, unit, 0, g_ctx.stream));
+  return QGB_OK;
+}
+
+ForceArgs fargs(const void* U, void* out, double beta, double c1, double dt)
+{
+  ForceArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U = U;
+  a.out = out;
+  a.beta = beta;
+  a.c1 = c1;
+  a.dt = dt;
+  a.unitarize = 1;
+  return a;
+}
+
+// Molecular dynamics of one trajectory in precision R on raw SoA buffers
+// (no Hamiltonians).  gf, gm updated in place; tmp: a link buffer.
+// Force-gradient: hmc.pyx:169-188 with gm_evolve_fg_pure_gauge fused as
+// [tmp = exp(fg_dt F(gf)) gf] then [gm += dt F(tmp)].  Leapfrog:
+// examples-py/hmc-pure-gauge-fgf.py:57-69 (gf_evolve dt/2, gm += dt F, gf_evolve dt/2).
+// unit_each: unitarize after every exponential; reunit_every > 0 re-unitarises
+// the links with FP64 arithmetic every that many steps.
+template <typename R>
+int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, double c1, int n_step, double md_time,
+                  int integrator, int unit_each, int reunit_every)
+{
+  const double dt = md_time / n_step;
+  if (integrator == QGB_INTEGRATOR_FORCE_GRADIENT) {
+    const double lam = 0.5 * (1.0 - 1.0 / sqrt(3.0));
+    const double theta = (2.0 - sqrt(3.0)) / 48.0;
+    const double ttheta = theta * dt * dt * dt;
+    const double fg_dt = 4.0 * ttheta / dt;
+    QGB_RC(evolve<R>(g, gf, gm, lam * dt, unit_each));
+    for (int i = 0; i < n_step; ++i) {
+      for (int half = 0; half < 2; ++half) {
+        ForceArgs a = fargs(gf, tmp, beta, c1, fg_dt);
+        a.unitarize = unit_each;
+        QGB_RC(force<R>(g, qgb::FORCE_EVOLVE, a));
+        ForceArgs b = fargs(tmp, gm, beta, c1, 0.5 * dt);
+        QGB_RC(force<R>(g, qgb::FORCE_UPDATE, b));
+        if (half == 0) QGB_RC(evolve<R>(g, gf, gm, (1.0 - 2.0 * lam) * dt, unit_each));
+      }
+      QGB_RC(evolve<R>(g, gf, gm, (i < n_step - 1 ? 2.0 * lam : lam) * dt, unit_each));
+      if (reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step) {
+        Prof p("unitarize");
+        QGB_TRY_CUDA((qgb::launch_unitarize<R, double>(g, 4, gf, g_ctx.stream)));
+      }
+    }
+  } else if (integrator == QGB_INTEGRATOR_LEAPFROG) {
+    for (int i = 0; i < n_step; ++i) {
+      QGB_RC(evolve<R>(g, gf, gm, 0.5 * dt, unit_each));
+      ForceArgs b = fargs(gf, gm, beta, c1, dt);
+      QGB_RC(force<R>(g, qgb::FORCE_UPDATE, b));
+      QGB_RC(evolve<R>(g, gf, gm, 0.5 * dt, unit_each));
+      if (reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step) {
+        Prof p("unitarize");
+        QGB_TRY_CUDA((qgb::launch_unitarize<R, double>(g, 4, gf, g_ctx.stream)));
+      }
+    }
+  } else {
+    return fail(QGB_ERR_INVALID_ARG, "unknown integrator");
+  }
+  return QGB_OK;
+}
+
+// Hamiltonian pieces into slots: slot = gm, slot+1 = plaq sum, slot+2 = rect sum.
+int hamiltonian_slots(const qgb_field* gm, const qgb_field* gf, double c1, int slot)
+{
+  QGB_RC(gm_hamilton_slot(gm, slot));
+  QGB_RC(action_slot(gf, c1 != 0.0, slot + 1));
+  return QGB_OK;
+}
+
+}  // namespace
+
+// ========================================================================
+// C ABI
+
+extern "C" {
+
+const char* qgb_last_error(void) { return g_err.c_str(); }
+
+int qgb_version(void) { return 10000; }
+
+int qgb_set_device(int32_t device)
+{
+  std::lock_guard<std::recursive_mutex> lock(g_mu);
+  if (g_ctx.ready && device != g_ctx.device)
+    return fail(QGB_ERR_INVALID_ARG, "qgb_set_device: the library context is already bound to another device");
+  QGB_TRY_CUDA(cudaSetDevice(device));
+  return QGB_OK;
+}
+
+int qgb_set_stream(void* stream)
+{
+  QGB_CTX();
+  QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  if (g_ctx.own_stream) cudaStreamDestroy(g_ctx.stream);
+  g_ctx.stream = (cudaStream_t)stream;
+  g_ctx.own_stream = false;
+  return QGB_OK;
+}
+
+int qgb_synchronize(void)
+{
+  QGB_CTX();
+  QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_field_create(qgb_field** out, const int32_t total_site[4], int32_t multiplicity, int32_t kind,
+                     int32_t precision)
+{
+  QGB_CTX();
+  QGB_CHECK(out && total_site, QGB_ERR_INVALID_ARG, "qgb_field_create: null argument");
+  QGB_CHECK(multiplicity >= 1, QGB_ERR_INVALID_ARG, "qgb_field_create: multiplicity must be >= 1");
+  QGB_CHECK(kind == QGB_KIND_COLOR_MATRIX || kind == QGB_KIND_REAL, QGB_ERR_INVALID_ARG,
+            "qgb_field_create: unknown kind");
+  QGB_CHECK(precision == QGB_F64 || precision == QGB_F32, QGB_ERR_INVALID_ARG,
+            "qgb_field_create: precision must be 64 or 32");
+  long V = 1;
+  for (int i = 0; i < 4; ++i) {
+    QGB_CHECK(total_site[i] >= 1 && total_site[i] <= (1 << 20), QGB_ERR_BAD_GEOMETRY,
+              "qgb_field_create: each lattice extent must be in [1, 2^20]");
+    V *= total_site[i];
+  }
+  QGB_CHECK(V <= (1L << 34), QGB_ERR_BAD_GEOMETRY, "qgb_field_create: lattice too large");
+  qgb_field_s* f = new qgb_field_s;
+  for (int i = 0; i < 4; ++i) f->dims[i] = total_site[i];
+  f->V = V;
+  f->mult = multiplicity;
+  f->kind = kind;
+  f->prec = precision;
+  f->bytes = (size_t)V * multiplicity * (kind == QGB_KIND_COLOR_MATRIX ? 18 : 1) * (precision == QGB_F64 ? 8 : 4);
+  f->d = nullptr;
+  cudaError_t e = cudaMalloc(&f->d, f->bytes);
+  if (e != cudaSuccess) {
+    delete f;
+    cudaGetLastError();
+    return fail(QGB_ERR_ALLOC, std::string("qgb_field_create: cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  e = cudaMemsetAsync(f->d, 0, f->bytes, g_ctx.stream);
+  if (e != cudaSuccess) {
+    cudaFree(f->d);
+    delete f;
+    return fail(QGB_ERR_CUDA, cudaGetErrorString(e));
+  }
+  *out = f;
+  return QGB_OK;
+}
+
+int qgb_field_destroy(qgb_field* f)
+{
+  if (!f) return QGB_OK;
+  std::lock_guard<std::recursive_mutex> lock(g_mu);
+  if (g_ctx.ready) cudaStreamSynchronize(g_ctx.stream);
+  cudaFree(f->d);
+  delete f;
+  return QGB_OK;
+}
+
+int qgb_field_info(const qgb_field* f, int32_t total_site[4], int32_t* multiplicity, int32_t* kind,
+                   int32_t* precision)
+{
+  QGB_CHECK(f, QGB_ERR_INVALID_ARG, "qgb_field_info: null field");
+  if (total_site)
+    for (int i = 0; i < 4; ++i) total_site[i] = f->dims[i];
+  if (multiplicity) *multiplicity = f->mult;
+  if (kind) *kind = f->kind;
+  if (precision) *precision = f->prec;
+  return QGB_OK;
+}
+
+static int upload_from_device_aos(qgb_field* f, const double* aos)
+{
+  const Geo g = geo_of(f);
+  Prof p("convert");
+  if (f->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_aos_to_soa<double>(g, f->mult, (int)elem_reals(f), aos, f->d, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_aos_to_soa<float>(g, f->mult, (int)elem_reals(f), aos, f->d, g_ctx.stream));
+  return QGB_OK;
+}
+
+static int download_to_device_aos(const qgb_field* f, double* aos)
+{
+  const Geo g = geo_of(f);
+  Prof p("convert");
+  if (f->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_soa_to_aos<double>(g, f->mult, (int)elem_reals(f), f->d, aos, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_soa_to_aos<float>(g, f->mult, (int)elem_reals(f), f->d, aos, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_field_upload(qgb_field* f, const double* host)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_upload"));
+  QGB_CHECK(host, QGB_ERR_INVALID_ARG, "qgb_field_upload: null host buffer");
+  const size_t bytes = (size_t)n_reals(f) * sizeof(double);
+  QGB_RC(ensure_staging(bytes));
+  QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.staging, host, bytes, cudaMemcpyHostToDevice, g_ctx.stream));
+  QGB_RC(upload_from_device_aos(f, g_ctx.staging));
+  return QGB_OK;
+}
+
+int qgb_field_download(const qgb_field* f, double* host)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_download"));
+  QGB_CHECK(host, QGB_ERR_INVALID_ARG, "qgb_field_download: null host buffer");
+  const size_t bytes = (size_t)n_reals(f) * sizeof(double);
+  QGB_RC(ensure_staging(bytes));
+  QGB_RC(download_to_device_aos(f, g_ctx.staging));
+  QGB_TRY_CUDA(cudaMemcpyAsync(host, g_ctx.staging, bytes, cudaMemcpyDeviceToHost, g_ctx.stream));
+  QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_field_upload_device(qgb_field* f, const double* dev)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_upload_device"));
+  QGB_CHECK(dev, QGB_ERR_INVALID_ARG, "qgb_field_upload_device: null buffer");
+  return upload_from_device_aos(f, dev);
+}
+
+int qgb_field_download_device(const qgb_field* f, double* dev)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_download_device"));
+  QGB_CHECK(dev, QGB_ERR_INVALID_ARG, "qgb_field_download_device: null buffer");
+  return download_to_device_aos(f, dev);
+}
+
+int qgb_field_copy(qgb_field* dst, const qgb_field* src)
+{
+  QGB_CTX();
+  QGB_RC(check_field(dst, -1, "qgb_field_copy"));
+  QGB_RC(check_field(src, -1, "qgb_field_copy"));
+  QGB_CHECK(same_geo(dst, src) && dst->mult == src->mult && dst->kind == src->kind, QGB_ERR_MISMATCH,
+            "qgb_field_copy: geometry / multiplicity / kind mismatch");
+  if (dst == src) return QGB_OK;
+  const long n = n_reals(dst);
+  Prof p("convert");
+  if (dst->prec == src->prec) {
+    QGB_TRY_CUDA(cudaMemcpyAsync(dst->d, src->d, dst->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  } else if (src->prec == QGB_F64) {
+    QGB_TRY_CUDA((qgb::launch_convert<double, float>(n, src->d, dst->d, g_ctx.stream)));
+  } else {
+    QGB_TRY_CUDA((qgb::launch_convert<float, double>(n, src->d, dst->d, g_ctx.stream)));
+  }
+  return QGB_OK;
+}
+
+int qgb_field_set_zero(qgb_field* f)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_set_zero"));
+  QGB_TRY_CUDA(cudaMemsetAsync(f->d, 0, f->bytes, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_field_axpby(qgb_field* y, double a, const qgb_field* x, double b)
+{
+  QGB_CTX();
+  QGB_RC(check_field(y, -1, "qgb_field_axpby"));
+  if (x) {
+    QGB_CHECK(same_geo(x, y) && x->mult == y->mult && x->kind == y->kind && x->prec == y->prec, QGB_ERR_MISMATCH,
+              "qgb_field_axpby: field mismatch");
+  }
+  const long n = n_reals(y);
+  Prof p("axpby");
+  if (y->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_axpby<double>(n, y->d, a, x ? x->d : nullptr, b, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_axpby<float>(n, y->d, a, x ? x->d : nullptr, b, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_field_qnorm(const qgb_field* f, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_qnorm"));
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_field_qnorm: null output");
+  const int nb = 148 * 8;
+  QGB_RC(ensure_partials(nb));
+  Prof p("reduce", 2);
+  if (f->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_qnorm<double>(n_reals(f), f->d, g_ctx.partials, nb, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_qnorm<float>(n_reals(f), f->d, g_ctx.partials, nb, g_ctx.stream));
+  QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 0, g_ctx.stream));
+  return read_results(0, 1, out);
+}
+
+// ---- RngState ------------------------------------------------------------
+
+int qgb_rng_seed(uint32_t out[24], const char* seed)
+{
+  QGB_CHECK(out && seed, QGB_ERR_INVALID_ARG, "qgb_rng_seed: null argument");
+  QGB_CHECK(strlen(seed) < 200, QGB_ERR_INVALID_ARG, "qgb_rng_seed: seed string too long");
+  qgb::rng_host_seed(out, seed);
+  return QGB_OK;
+}
+
+int qgb_rng_split(uint32_t out[24], const uint32_t rs[24], const char* sindex)
+{
+  QGB_CHECK(out && rs && sindex, QGB_ERR_INVALID_ARG, "qgb_rng_split: null argument");
+  QGB_CHECK(qgb::rng_host_split(out, rs, sindex), QGB_ERR_INVALID_ARG, "qgb_rng_split: index string too long");
+  return QGB_OK;
+}
+
+int qgb_rng_rand_gen(uint32_t rs[24], uint64_t* out)
+{
+  QGB_CHECK(rs && out, QGB_ERR_INVALID_ARG, "qgb_rng_rand_gen: null argument");
+  *out = qgb::rng_host_rand_gen(rs);
+  return QGB_OK;
+}
+
+int qgb_rng_u_rand_gen(uint32_t rs[24], double upper, double lower, double* out)
+{
+  QGB_CHECK(rs && out, QGB_ERR_INVALID_ARG, "qgb_rng_u_rand_gen: null argument");
+  *out = qgb::rng_host_u_rand_gen(rs, upper, lower);
+  return QGB_OK;
+}
+
+int qgb_rng_g_rand_gen(uint32_t rs[24], double center, double sigma, double* out)
+{
+  QGB_CHECK(rs && out, QGB_ERR_INVALID_ARG, "qgb_rng_g_rand_gen: null argument");
+  *out = qgb::rng_host_g_rand_gen(rs, center, sigma);
+  return QGB_OK;
+}
+
+// ---- set-up --------------------------------------------------------------
+
+int qgb_set_unit(qgb_field* gf)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_set_unit"));
+  const Geo g = geo_of(gf);
+  Prof p("set_unit");
+  if (gf->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_set_unit<double>(g, gf->mult, gf->d, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_set_unit<float>(g, gf->mult, gf->d, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_gf_set_rand(qgb_field* gf, const uint32_t rs[24], double sigma, int32_t n_step)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_set_rand"));
+  QGB_CHECK(gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_set_rand: multiplicity must be 4");
+  QGB_CHECK(rs, QGB_ERR_INVALID_ARG, "qgb_gf_set_rand: null RngState");
+  const Geo g = geo_of(gf);
+  Prof p("rng");
+  if (gf->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_hot_start<double>(g, gf->d, rs, sigma, n_step, g_ctx.ambiguous, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_hot_start<float>(g, gf->d, rs, sigma, n_step, g_ctx.ambiguous, g_ctx.stream));
+  return QGB_OK;
+}
+
+// ---- HMC -------------------------------------------------------------------
+
+int qgb_set_rand_gauge_momentum(qgb_field* gm, double sigma, const uint32_t rs[24])
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_set_rand_gauge_momentum"));
+  QGB_CHECK(gm->mult == 4, QGB_ERR_INVALID_ARG, "qgb_set_rand_gauge_momentum: multiplicity must be 4");
+  QGB_CHECK(rs, QGB_ERR_INVALID_ARG, "qgb_set_rand_gauge_momentum: null RngState");
+  const Geo g = geo_of(gm);
+  Prof p("rng");
+  if (gm->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_rand_momentum<double>(g, gm->d, rs, sigma, g_ctx.ambiguous, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_rand_momentum<float>(g, gm->d, rs, sigma, g_ctx.ambiguous, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_gm_hamilton_node(const qgb_field* gm, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_gm_hamilton_node"));
+  QGB_CHECK(out && gm->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gm_hamilton_node: bad argument");
+  QGB_RC(gm_hamilton_slot(gm, 0));
+  return read_results(0, 1, out);
+}
+
+int qgb_gf_sum_re_tr_plaq_node(const qgb_field* gf, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_sum_re_tr_plaq_node"));
+  QGB_CHECK(out && gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_sum_re_tr_plaq_node: bad argument");
+  QGB_RC(action_slot(gf, 0, 0));
+  return read_results(0, 1, out);
+}
+
+int qgb_gf_sum_re_tr_rect_node(const qgb_field* gf, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_sum_re_tr_rect_node"));
+  QGB_CHECK(out && gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_sum_re_tr_rect_node: bad argument");
+  QGB_RC(action_slot(gf, 1, 0));
+  double r[2];
+  QGB_RC(read_results(0, 2, r));
+  *out = r[1];
+  return QGB_OK;
+}
+
+int qgb_gf_hamilton_node(const qgb_field* gf, double beta, double c1, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_hamilton_node"));
+  QGB_CHECK(out && gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_hamilton_node: bad argument");
+  QGB_RC(action_slot(gf, c1 != 0.0, 0));
+  double r[2] = {0, 0};
+  QGB_RC(read_results(0, c1 != 0.0 ? 2 : 1, r));
+  *out = gf_hamilton_from(r[0], r[1], beta, c1);
+  return QGB_OK;
+}
+
+int qgb_gf_avg_plaq(const qgb_field* gf, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_avg_plaq"));
+  QGB_CHECK(out && gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_avg_plaq: bad argument");
+  QGB_RC(action_slot(gf, 0, 0));
+  double sp;
+  QGB_RC(read_results(0, 1, &sp));
+  // sum over sites and planes of (Re tr P - 3) -> mean of Re tr P / 3
+  *out = 1.0 + sp / (18.0 * (double)gf->V);
+  if (isnan(*out)) return fail(QGB_ERR_NAN, "qgb_gf_avg_plaq: NaN in gauge field");
+  return QGB_OK;
+}
+
+int qgb_set_gm_force(qgb_field* gm_force, const qgb_field* gf, double beta, double c1)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm_force, QGB_KIND_COLOR_MATRIX, "qgb_set_gm_force"));
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_set_gm_force"));
+  QGB_CHECK(gf->mult == 4 && gm_force->mult == 4 && same_geo(gf, gm_force) && gf->prec == gm_force->prec,
+            QGB_ERR_MISMATCH, "qgb_set_gm_force: field mismatch");
+  QGB_CHECK(gm_force != gf, QGB_ERR_INVALID_ARG, "qgb_set_gm_force: output aliases the gauge field");
+  const Geo g = geo_of(gf);
+  ForceArgs a = fargs(gf->d, gm_force->d, beta, c1, 0.0);
+  if (gf->prec == QGB_F64) return force<double>(g, qgb::FORCE_SET, a);
+  return force<float>(g, qgb::FORCE_SET, a);
+}
+
+int qgb_gf_evolve(qgb_field* gf, const qgb_field* gm, double step_size)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_evolve"));
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_gf_evolve"));
+  QGB_CHECK(gf->mult == 4 && gm->mult == 4 && same_geo(gf, gm) && gf->prec == gm->prec, QGB_ERR_MISMATCH,
+            "qgb_gf_evolve: field mismatch");
+  const Geo g = geo_of(gf);
+  if (gf->prec == QGB_F64) return evolve<double>(g, gf->d, gm->d, step_size, 1);
+  return evolve<float>(g, gf->d, gm->d, step_size, 1);
+}
+
+int qgb_gm_evolve_fg(qgb_field* gm, const qgb_field* gf_init, double beta, double c1, double fg_dt, double dt)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_gm_evolve_fg"));
+  QGB_RC(check_field(gf_init, QGB_KIND_COLOR_MATRIX, "qgb_gm_evolve_fg"));
+  QGB_CHECK(gf_init->mult == 4 && gm->mult == 4 && same_geo(gf_init, gm) && gf_init->prec == gm->prec,
+            QGB_ERR_MISMATCH, "qgb_gm_evolve_fg: field mismatch");
+  const Geo g = geo_of(gf_init);
+  void* tmp = nullptr;
+  QGB_RC(get_scratch(gf_init->bytes, 1, &tmp));
+  ForceArgs a = fargs(gf_init->d, tmp, beta, c1, fg_dt);
+  ForceArgs b = fargs(tmp, gm->d, beta, c1, dt);
+  if (gf_init->prec == QGB_F64) {
+    QGB_RC(force<double>(g, qgb::FORCE_EVOLVE, a));
+    return force<double>(g, qgb::FORCE_UPDATE, b);
+  }
+  QGB_RC(force<float>(g, qgb::FORCE_EVOLVE, a));
+  return force<float>(g, qgb::FORCE_UPDATE, b);
+}
+
+int qgb_unitarize(qgb_field* gf)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_unitarize"));
+  const Geo g = geo_of(gf);
+  Prof p("unitarize");
+  if (gf->prec == QGB_F64) QGB_TRY_CUDA((qgb::launch_unitarize<double, double>(g, gf->mult, gf->d, g_ctx.stream)));
+  else QGB_TRY_CUDA((qgb::launch_unitarize<float, float>(g, gf->mult, gf->d, g_ctx.stream)));
+  return QGB_OK;
+}
+
+int qgb_metropolis_accept(double delta_h, int32_t traj, const uint32_t rs[24], double* accept_prob, int32_t* flag)
+{
+  (void)traj;
+  QGB_CHECK(rs && accept_prob && flag, QGB_ERR_INVALID_ARG, "qgb_metropolis_accept: null argument");
+  // hmc.cpp:77-105.  The reference draws u_rand_gen(rs, 0.0, 1.0), i.e.
+  // upper = 0 and lower = 1, which is 1 - u.
+  if (delta_h <= 0.0) {
+    *accept_prob = 1.0;
+    *flag = 1;
+    return QGB_OK;
+  }
+  uint32_t r[24];
+  memcpy(r, rs, sizeof(r));
+  const double rand_num = qgb::rng_host_u_rand_gen(r, 0.0, 1.0);
+  *accept_prob = exp(-delta_h);
+  *flag = rand_num <= *accept_prob ? 1 : 0;
+  return QGB_OK;
+}
+
+int qgb_run_hmc_evolve(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step, double md_time,
+                       int32_t integrator, double* delta_h)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_run_hmc_evolve"));
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_run_hmc_evolve"));
+  QGB_CHECK(gf->mult == 4 && gm->mult == 4 && same_geo(gf, gm) && gf->prec == gm->prec, QGB_ERR_MISMATCH,
+            "qgb_run_hmc_evolve: field mismatch");
+  QGB_CHECK(n_step >= 1 && delta_h, QGB_ERR_INVALID_ARG, "qgb_run_hmc_evolve: bad argument");
+  const Geo g = geo_of(gf);
+  void* tmp = nullptr;
+  QGB_RC(get_scratch(gf->bytes, 1, &tmp));
+  QGB_RC(hamiltonian_slots(gm, gf, c1, 0));
+  if (gf->prec == QGB_F64)
+    QGB_RC(md_trajectory<double>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, 1, 0));
+  else
+    QGB_RC(md_trajectory<float>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, 1, 0));
+  QGB_RC(qgb_unitarize(gf));
+  QGB_RC(hamiltonian_slots(gm, gf, c1, 3));
+  double r[6];
+  QGB_RC(read_results(0, 6, r));
+  const double e0 = r[0] + gf_hamilton_from(r[1], r[2], beta, c1);
+  *delta_h = r[3] + gf_hamilton_from(r[4], r[5], beta, c1) - e0;
+  if (isnan(*delta_h)) return fail(QGB_ERR_NAN, "qgb_run_hmc_evolve: delta_h is NaN");
+  return QGB_OK;
+}
+
+int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step, double md_time,
+                             int32_t integrator, int32_t reunit_interval, double* delta_h)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_run_hmc_evolve_mixed"));
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_run_hmc_evolve_mixed"));
+  QGB_CHECK(gf->mult == 4 && gm->mult == 4 && same_geo(gf, gm) && gf->prec == QGB_F64 && gm->prec == QGB_F64,
+            QGB_ERR_MISMATCH, "qgb_run_hmc_evolve_mixed: gm and gf must be FP64 fields of one geometry");
+  QGB_CHECK(n_step >= 1 && delta_h, QGB_ERR_INVALID_ARG, "qgb_run_hmc_evolve_mixed: bad argument");
+  const Geo g = geo_of(gf);
+  const size_t b32 = gf->bytes / 2;
+  void *gf32 = nullptr, *gm32 = nullptr, *tmp32 = nullptr;
+  QGB_RC(get_scratch(b32, 11, &gf32));
+  QGB_RC(get_scratch(b32, 12, &gm32));
+  QGB_RC(get_scratch(b32, 13, &tmp32));
+  QGB_RC(hamiltonian_slots(gm, gf, c1, 0));
+  const long n = n_reals(gf);
+  {
+    Prof p("convert", 2);
+    QGB_TRY_CUDA((qgb::launch_convert<double, float>(n, gf->d, gf32, g_ctx.stream)));
+    QGB_TRY_CUDA((qgb::launch_convert<double, float>(n, gm->d, gm32, g_ctx.stream)));
+  }
+  const int unit_each = reunit_interval > 0 ? 0 : 1;
+  QGB_RC(md_trajectory<float>(g, gf32, gm32, tmp32, beta, c1, n_step, md_time, integrator, unit_each,
+                              reunit_interval));
+  {
+    Prof p("convert", 2);
+    QGB_TRY_CUDA((qgb::launch_convert<float, double>(n, gf32, gf->d, g_ctx.stream)));
+    QGB_TRY_CUDA((qgb::launch_convert<float, double>(n, gm32, gm->d, g_ctx.stream)));
+  }
+  QGB_RC(qgb_unitarize(gf));
+  QGB_RC(hamiltonian_slots(gm, gf, c1, 3));
+  double r[6];
+  QGB_RC(read_results(0, 6, r));
+  const double e0 = r[0] + gf_hamilton_from(r[1], r[2], beta, c1);
+  *delta_h = r[3] + gf_hamilton_from(r[4], r[5], beta, c1) - e0;
+  if (isnan(*delta_h)) return fail(QGB_ERR_NAN, "qgb_run_hmc_evolve_mixed: delta_h is NaN");
+  return QGB_OK;
+}
+
+// ---- gradient flow ---------------------------------------------------------
+
+int qgb_set_wilson_flow_z(qgb_field* z, const qgb_field* gf, double c1)
+{
+  return qgb_set_gm_force(z, gf, 3.0, c1);
+}
+
+// One flow step through fused stage kernels: W -> T -> W -> T and a
+// buffer swap, so the field handle ends up owning the result.
+static int flow_step(qgb_field* gf, double eps, double c1, bool rk3)
+{
+  const Geo g = geo_of(gf);
+  void *T = nullptr, *Z = nullptr;
+  QGB_RC(get_scratch(gf->bytes, 21, &T));
+  QGB_RC(get_scratch(gf->bytes, 22, &Z));
+  auto stage = [&](const void* in, void* out, double a, double b, const void* zp, void* zo) -> int {
+    ForceArgs fa = fargs(in, out, 3.0, c1, eps);
+    fa.a = a;
+    fa.b = b;
+    fa.zp = zp;
+    fa.z = zo;
+    if (gf->prec == QGB_F64) return force<double>(g, qgb::FORCE_FLOW, fa);
+    return force<float>(g, qgb::FORCE_FLOW, fa);
+  };
+  if (rk3) {
+    // wilson-flow.cpp:29-50: Z0 = F/4; Z1 = 8/9 F - 17/9 Z0; Z2 = 3/4 F - Z1
+    QGB_RC(stage(gf->d, T, 0.25, 0.0, nullptr, Z));
+    QGB_RC(stage(T, gf->d, 8.0 / 9.0, -17.0 / 9.0, Z, Z));
+    QGB_RC(stage(gf->d, T, 0.75, -1.0, Z, nullptr));
+  } else {
+    QGB_RC(stage(gf->d, T, 1.0, 0.0, nullptr, nullptr));
+  }
+  // the handle takes the result buffer; the old one becomes the scratch
+  auto& v = g_ctx.scratch[std::make_pair(gf->bytes, 21)];
+  v[0] = gf->d;
+  gf->d = T;
+  return QGB_OK;
+}
+
+int qgb_gf_wilson_flow_step(qgb_field* gf, double epsilon, double c1)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_wilson_flow_step"));
+  QGB_CHECK(gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_wilson_flow_step: multiplicity must be 4");
+  return flow_step(gf, epsilon, c1, true);
+}
+
+int qgb_gf_wilson_flow_step_euler(qgb_field* gf, double epsilon, double c1)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_wilson_flow_step_euler"));
+  QGB_CHECK(gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_wilson_flow_step_euler: multiplicity must be 4");
+  return flow_step(gf, epsilon, c1, false);
+}
+
+int qgb_gf_energy_density_field(qgb_field* fd, const qgb_field* gf)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_energy_density_field"));
+  QGB_RC(check_field(fd, QGB_KIND_REAL, "qgb_gf_energy_density_field"));
+  QGB_CHECK(same_geo(fd, gf) && fd->mult == 1 && fd->prec == gf->prec, QGB_ERR_MISMATCH,
+            "qgb_gf_energy_density_field: fd must be a real field of multiplicity 1 in the links' precision");
+  return clover_slot(gf, fd, nullptr, 0);
+}
+
+int qgb_gf_energy_density(const qgb_field* gf, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_energy_density"));
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_gf_energy_density: null output");
+  QGB_RC(clover_slot(gf, nullptr, nullptr, 0));
+  double r;
+  QGB_RC(read_results(0, 1, &r));
+  *out = r / (double)gf->V;
+  return QGB_OK;
+}
+
+int qgb_gf_wilson_flow(qgb_field* gf, double flow_time, int32_t steps, double c1, double* energy_list)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_wilson_flow"));
+  QGB_CHECK(steps >= 1 && energy_list, QGB_ERR_INVALID_ARG, "qgb_gf_wilson_flow: bad argument");
+  const double eps = flow_time / (double)steps;
+  // energies of up to NSLOT-2 consecutive steps are gathered on the device
+  // and read back together
+  const int chunk = Ctx::NSLOT - 2;
+  for (int i0 = 0; i0 < steps; i0 += chunk) {
+    const int n = (steps - i0) < chunk ? (steps - i0) : chunk;
+    for (int i = 0; i < n; ++i) {
+      QGB_RC(flow_step(gf, eps, c1, true));
+      QGB_RC(clover_slot(gf, nullptr, nullptr, i));  // writes slots i, i+1; i+1 is overwritten next step
+    }
+    double r[Ctx::NSLOT];
+    QGB_RC(read_results(0, n, r));
+    for (int i = 0; i < n; ++i) energy_list[i0 + i] = r[i] / (double)gf->V;
+  }
+  return QGB_OK;
+}
+
+int qgb_clf_topology_field(qgb_field* topf, const qgb_field* gf)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_clf_topology_field"));
+  QGB_RC(check_field(topf, QGB_KIND_REAL, "qgb_clf_topology_field"));
+  QGB_CHECK(same_geo(topf, gf) && topf->mult == 1 && topf->prec == gf->prec, QGB_ERR_MISMATCH,
+            "qgb_clf_topology_field: topf must be a real field of multiplicity 1 in the links' precision");
+  return clover_slot(gf, nullptr, topf, 0);
+}
+
+int qgb_gf_topology_clf(const qgb_field* gf, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_topology_clf"));
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_gf_topology_clf: null output");
+  QGB_RC(clover_slot(gf, nullptr, nullptr, 0));
+  double r[2];
+  QGB_RC(read_results(0, 2, r));
+  *out = r[1];
+  return QGB_OK;
+}
+
+// ---- instrumentation -------------------------------------------------------
+
+int qgb_prof_enable(int32_t on)
+{
+  QGB_CTX();
+  g_ctx.prof_on = on != 0;
+  return QGB_OK;
+}
+
+int qgb_prof_reset(void)
+{
+  QGB_CTX();
+  prof_collect();
+  for (auto& kv : g_ctx.prof) {
+    kv.second.total_ms = 0;
+    kv.second.launches = 0;
+  }
+  return QGB_OK;
+}
+
+int qgb_prof_get(const char* name, double* total_ms, int64_t* launches)
+{
+  QGB_CTX();
+  QGB_CHECK(name && total_ms && launches, QGB_ERR_INVALID_ARG, "qgb_prof_get: null argument");
+  prof_collect();
+  auto it = g_ctx.prof.find(name);
+  *total_ms = it == g_ctx.prof.end() ? 0.0 : it->second.total_ms;
+  *launches = it == g_ctx.prof.end() ? 0 : it->second.launches;
+  return QGB_OK;
+}
+
+int qgb_launch_count(int64_t* out)
+{
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_launch_count: null output");
+  *out = g_launches;
+  return QGB_OK;
+}
+
+int qgb_rng_ambiguous_count(int64_t* out)
+{
+  QGB_CTX();
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_rng_ambiguous_count: null output");
+  int v = 0;
+  QGB_TRY_CUDA(cudaMemcpyAsync(&v, g_ctx.ambiguous, sizeof(int), cudaMemcpyDeviceToHost, g_ctx.stream));
+  QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  *out = v;
+  return QGB_OK;
+}
+
+}  // extern "C"

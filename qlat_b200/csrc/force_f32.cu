@@ -1,0 +1,7 @@
+// force_f32.cu -- float instantiation of the gauge force kernels.
+#include "force_impl.cuh"
+
+namespace qgb
+{
+template cudaError_t launch_force<float>(const Geo&, ForceMode, const ForceArgs&, cudaStream_t);
+}  // namespace qgb

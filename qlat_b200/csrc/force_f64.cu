@@ -1,0 +1,7 @@
+// force_f64.cu -- double instantiation of the gauge force kernels.
+#include "force_impl.cuh"
+
+namespace qgb
+{
+template cudaError_t launch_force<double>(const Geo&, ForceMode, const ForceArgs&, cudaStream_t);
+}  // namespace qgb

@@ -1,0 +1,651 @@
+// kernels.cu -- CUDA kernels of the pure-gauge hot path for sm_100a.
+//
+// Memory layout in HBM: a color-matrix field with multiplicity m over V sites
+// is stored structure-of-arrays, element (site, mu, k) of the 3x3 matrix at
+// Cx<R>[(mu * 9 + k) * V + site], sites in the reference's order (x fastest,
+// coordinate.h:182-188).  A warp touches 32 consecutive sites per component,
+// so every load and store is a fully coalesced 512-byte (FP64) or 256-byte
+// (FP32) transaction.  Neighbour links come through L1/L2; the lattice is
+// periodic.
+//
+// Kernels use one thread per link (site, mu) for link-local work and force
+// evaluation, and one thread per site for the site reductions.  Reductions
+// accumulate in FP64 whatever the storage precision, then reduce in a fixed
+// order (warp shuffles, block, then one block over the partials), so results
+// are deterministic run to run.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "gauge_common.cuh"
+#include "kernels.h"
+#include "rng.cuh"
+#include "su3.cuh"
+
+namespace qgb
+{
+
+ShaConst qgb_sha_host;
+
+// ------------------------------------------------------------------------
+// constants
+
+static void sha_const_compute(ShaConst& c)
+{
+  int primes[64];
+  int n = 0;
+  for (int v = 2; n < 64; ++v) {
+    bool p = true;
+    for (int d = 2; d * d <= v; ++d)
+      if (v % d == 0) {
+        p = false;
+        break;
+      }
+    if (p) primes[n++] = v;
+  }
+  // first 32 fractional bits of cube roots (k) and square roots (h0) of primes
+  for (int i = 0; i < 64; ++i) {
+    const unsigned __int128 target = ((unsigned __int128)primes[i]) << 96;
+    uint64_t lo = 0, hi = (uint64_t)1 << 36;
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) / 2;
+      if ((unsigned __int128)mid * mid * mid <= target) lo = mid; else hi = mid;
+    }
+    c.k[i] = (uint32_t)lo;
+  }
+  for (int i = 0; i < 8; ++i) {
+    const unsigned __int128 target = ((unsigned __int128)primes[i]) << 64;
+    uint64_t lo = 0, hi = (uint64_t)1 << 36;
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) / 2;
+      if ((unsigned __int128)mid * mid <= target) lo = mid; else hi = mid;
+    }
+    c.h0[i] = (uint32_t)lo;
+  }
+}
+
+struct HostConstInit {
+  HostConstInit() { sha_const_compute(qgb_sha_host); }
+};
+static HostConstInit host_const_init;
+
+void init_constants()
+{
+  cudaMemcpyToSymbol(qgb_sha_dev, &qgb_sha_host, sizeof(ShaConst));
+  cudaMemcpyToSymbol(qgb_logtab_dev, qgb_logtab_host, sizeof(qgb_logtab_host));
+}
+
+// ------------------------------------------------------------------------
+// gf_evolve: U = unitarize(exp(eps P) U) (hmc.cpp:311-328, matrix-hmc.h:179-188)
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_evolve(Geo g, Cx<R>* U, const Cx<R>* P, double eps, int unit, int taylor)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.V) return;
+  const int mu = blockIdx.y;
+  const WField<R> Uf{U, g.V};
+  const CField<R> Pf{P, g.V};
+  const M3<R> a = scale(R(eps), Pf.ld(s, mu));
+  const M3<R> e = taylor ? exp_taylor(a, 20) : exp_ch(a);
+  M3<R> un = mul(e, Uf.ld(s, mu));
+  if (unit) unitarize(un);
+  Uf.st(s, mu, un);
+}
+
+template <typename R>
+cudaError_t launch_evolve(const Geo& g, void* U, const void* P, double eps, int unitarize, int taylor,
+                          cudaStream_t st)
+{
+  const int bs = 256;
+  dim3 grid((unsigned)((g.V + bs - 1) / bs), 4);
+  k_evolve<R><<<grid, bs, 0, st>>>(g, (Cx<R>*)U, (const Cx<R>*)P, eps, unitarize, taylor);
+  return cudaGetLastError();
+}
+
+template <typename R, typename C>
+__global__ void k_unitarize(long V, int m, Cx<R>* U)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  const WField<R> Uf{U, V};
+  for (int mu = 0; mu < m; ++mu) {
+    M3<R> u = Uf.ld(s, mu);
+    unitarize_as<C, R>(u);
+    Uf.st(s, mu, u);
+  }
+}
+
+template <typename R, typename C>
+cudaError_t launch_unitarize(const Geo& g, int m, void* U, cudaStream_t st)
+{
+  const int bs = 256;
+  k_unitarize<R, C><<<(unsigned)((g.V + bs - 1) / bs), bs, 0, st>>>(g.V, m, (Cx<R>*)U);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// deterministic reductions
+
+static const int RED_BS = 256;
+
+int reduce_blocks(const Geo& g) { return (int)((g.V + RED_BS - 1) / RED_BS); }
+
+// Reduce NV values across the block in a fixed order; thread 0 writes
+// partials[k * gridDim.x + blockIdx.x].
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* partials)
+{
+  __shared__ double sm[NV][RED_BS / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double x = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sm[k][w] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = 0.0;
+      for (int i = 0; i < RED_BS / 32; ++i) t += sm[k][i];
+      partials[(long)k * gridDim.x + blockIdx.x] = t;
+    }
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(RED_BS) k_gm_hamilton(Geo g, const Cx<R>* P, double* partials)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (s < g.V) {
+    const CField<R> Pf{P, g.V};
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) v[0] += neg_half_tr_square(Pf.ld(s, mu));
+  }
+  block_reduce_store<1>(v, partials);
+}
+
+template <typename R>
+cudaError_t launch_gm_hamilton(const Geo& g, const void* P, double* partials, cudaStream_t st)
+{
+  k_gm_hamilton<R><<<reduce_blocks(g), RED_BS, 0, st>>>(g, (const Cx<R>*)P, partials);
+  return cudaGetLastError();
+}
+
+// Sums over the 6 planes mu < nu at x of (Re tr plaq - 3) and, with RECT, of
+// (Re tr rect - 3) for both rectangle orientations (hmc.cpp:9-25,203-252):
+// plaq = A B^+ with A = U_mu(x) U_nu(x+mu), B = U_nu(x) U_mu(x+nu);
+// rect (mu, mu, nu, -mu, -mu, -nu) = A B^+ with A = U_mu(x) U_mu(x+mu) U_nu(x+2mu),
+// B = U_nu(x) U_mu(x+nu) U_mu(x+mu+nu).
+template <typename R, bool RECT>
+__global__ void __launch_bounds__(RED_BS) k_action(Geo g, const Cx<R>* Up, double* partials)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (s < g.V) {
+    const CField<R> U{Up, g.V};
+    const Coord x = coord_of(g, s);
+#pragma unroll 1
+    for (int p = 0; p < 6; ++p) {
+      const int mu = p < 3 ? 0 : (p < 5 ? 1 : 2);
+      const int nu = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
+      {
+        const M3<R> A = mul(U.ld(s, mu), U.ld(site_rt(g, x, mu, 1, nu, 0), nu));
+        const M3<R> B = mul(U.ld(s, nu), U.ld(site_rt(g, x, mu, 0, nu, 1), mu));
+        v[0] += (double)re_tr_mul_adj(A, B) - 3.0;
+      }
+      if (RECT) {
+#pragma unroll 1
+        for (int o = 0; o < 2; ++o) {
+          const int a = o == 0 ? mu : nu, b = o == 0 ? nu : mu;  // long side along a
+          M3<R> A = mul(U.ld(s, a), U.ld(site_rt(g, x, a, 1, b, 0), a));
+          A = mul(A, U.ld(site_rt(g, x, a, 2, b, 0), b));
+          M3<R> B = mul(U.ld(s, b), U.ld(site_rt(g, x, a, 0, b, 1), a));
+          B = mul(B, U.ld(site_rt(g, x, a, 1, b, 1), a));
+          v[1] += (double)re_tr_mul_adj(A, B) - 3.0;
+        }
+      }
+    }
+  }
+  block_reduce_store<2>(v, partials);
+}
+
+template <typename R>
+cudaError_t launch_action(const Geo& g, const void* U, int rect, double* partials, cudaStream_t st)
+{
+  if (rect) k_action<R, true><<<reduce_blocks(g), RED_BS, 0, st>>>(g, (const Cx<R>*)U, partials);
+  else k_action<R, false><<<reduce_blocks(g), RED_BS, 0, st>>>(g, (const Cx<R>*)U, partials);
+  return cudaGetLastError();
+}
+
+// Clover leaf sum C_mu_nu(x) (the 4 leaves of qcd-acc.h:135-150, without the 1/4).
+template <typename R>
+__device__ __forceinline__ M3<R> clover_sum(const CField<R>& U, const Geo& g, const Coord& x, long s, int mu, int nu)
+{
+  // leaf 1: (mu, nu, -mu, -nu) = U_mu(x) U_nu(x+mu) [U_nu(x) U_mu(x+nu)]^+
+  M3<R> C = mul_adj(mul(U.ld(s, mu), U.ld(site_rt(g, x, mu, 1, nu, 0), nu)),
+                    mul(U.ld(s, nu), U.ld(site_rt(g, x, mu, 0, nu, 1), mu)));
+  // leaf 2: (-mu, -nu, mu, nu) = [U_nu(x-mu-nu) U_mu(x-mu)]^+ U_mu(x-mu-nu) U_nu(x-nu)
+  {
+    const M3<R> a = mul(U.ld(site_rt(g, x, mu, -1, nu, -1), nu), U.ld(site_rt(g, x, mu, -1, nu, 0), mu));
+    const M3<R> b = mul(U.ld(site_rt(g, x, mu, -1, nu, -1), mu), U.ld(site_rt(g, x, mu, 0, nu, -1), nu));
+    C = add_adj_mul(C, a, b);
+  }
+  // leaf 3: (nu, -mu, -nu, mu) = U_nu(x) U_mu(x-mu+nu)^+ U_nu(x-mu)^+ U_mu(x-mu)
+  {
+    const M3<R> a = mul_adj(U.ld(s, nu), U.ld(site_rt(g, x, mu, -1, nu, 1), mu));
+    const M3<R> b = adj_mul(U.ld(site_rt(g, x, mu, -1, nu, 0), nu), U.ld(site_rt(g, x, mu, -1, nu, 0), mu));
+    C = add_mul(C, a, b);
+  }
+  // leaf 4: (-nu, mu, nu, -mu) = U_nu(x-nu)^+ U_mu(x-nu) U_nu(x-nu+mu) U_mu(x)^+
+  {
+    const M3<R> a = adj_mul(U.ld(site_rt(g, x, mu, 0, nu, -1), nu), U.ld(site_rt(g, x, mu, 0, nu, -1), mu));
+    const M3<R> b = mul_adj(U.ld(site_rt(g, x, mu, 1, nu, -1), nu), U.ld(s, mu));
+    C = add_mul(C, a, b);
+  }
+  return C;
+}
+
+// (C - C^+)/8 = the anti-Hermitian part of the leaf average C/4.
+template <typename R>
+__device__ __forceinline__ M3<R> leaf_antiherm(const M3<R>& C)
+{
+  M3<R> ah;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      ah.e[3 * r + c] = cx<R>(R(0.125) * (C.e[3 * r + c].re - C.e[3 * c + r].re),
+                             R(0.125) * (C.e[3 * r + c].im + C.e[3 * c + r].im));
+  return ah;
+}
+
+// -tr(G^2) with G = TA(C/4) = Fa - i Im(tr Fa)/3 (matrix-hmc.h:202-213)
+template <typename R>
+__device__ __forceinline__ double energy_of(const M3<R>& Fa)
+{
+  M3<R> G = Fa;
+  const R t = (G.e[0].im + G.e[4].im + G.e[8].im) / R(3);
+  G.e[0].im -= t;
+  G.e[4].im -= t;
+  G.e[8].im -= t;
+  return -(double)re_tr_mul(G, G);
+}
+
+// Energy density E(x) = sum_{mu<nu} -tr(G_mu_nu^2), G = TA(C/4)
+// (wilson-flow.cpp:99-129) and the clover topological charge density
+// -1/(4 pi^2) [-tr(F02 F13) + tr(F03 F12) + tr(F23 F01)], F = (C/4 - C^+/4)/2
+// (qcd.cpp:64-79), sharing the leaves; planes are visited in the pairs the
+// charge needs so that only two plane matrices are live at a time.
+template <typename R>
+__global__ void __launch_bounds__(RED_BS) k_clover(Geo g, const Cx<R>* Up, R* ef, R* qf, double* partials)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (s < g.V) {
+    const CField<R> U{Up, g.V};
+    const Coord x = coord_of(g, s);
+    double e = 0.0, q = 0.0;
+    // plane pairs (02,13) -, (03,12) +, (23,01) +
+#pragma unroll 1
+    for (int p = 0; p < 3; ++p) {
+      const int m1 = p == 2 ? 2 : 0, n1 = p == 0 ? 2 : (p == 1 ? 3 : 3);
+      const int m2 = p == 2 ? 0 : 1, n2 = p == 0 ? 3 : (p == 1 ? 2 : 1);
+      const M3<R> Fa = leaf_antiherm(clover_sum<R>(U, g, x, s, m1, n1));
+      const M3<R> Fb = leaf_antiherm(clover_sum<R>(U, g, x, s, m2, n2));
+      e += energy_of(Fa) + energy_of(Fb);
+      const double t = (double)re_tr_mul(Fa, Fb);
+      q += p == 0 ? -t : t;
+    }
+    q *= -1.0 / (4.0 * 3.141592653589793 * 3.141592653589793);
+    v[0] = e;
+    v[1] = q;
+    if (ef) ef[s] = (R)e;
+    if (qf) qf[s] = (R)q;
+  }
+  block_reduce_store<2>(v, partials);
+}
+
+template <typename R>
+cudaError_t launch_clover(const Geo& g, const void* U, void* e_field, void* q_field, double* partials,
+                          cudaStream_t st)
+{
+  k_clover<R><<<reduce_blocks(g), RED_BS, 0, st>>>(g, (const Cx<R>*)U, (R*)e_field, (R*)q_field, partials);
+  return cudaGetLastError();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(RED_BS) k_qnorm(long n, const R* x, double* partials)
+{
+  double v[1] = {0.0};
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double t = (double)x[i];
+    v[0] += t * t;
+  }
+  block_reduce_store<1>(v, partials);
+}
+
+template <typename R>
+cudaError_t launch_qnorm(long n_reals, const void* x, double* partials, int blocks, cudaStream_t st)
+{
+  k_qnorm<R><<<blocks, RED_BS, 0, st>>>(n_reals, (const R*)x, partials);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(1024) k_finalize(const double* partials, int nv, int blocks, double* results,
+                                                   int slot)
+{
+  __shared__ double sm[32];
+  for (int k = 0; k < nv; ++k) {
+    double t = 0.0;
+    for (int i = threadIdx.x; i < blocks; i += blockDim.x) t += partials[(long)k * blocks + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double r = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sm[i];
+      results[slot + k] = r;
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_finalize(const double* partials, int n_values, int blocks, double* results, int slot,
+                            cudaStream_t st)
+{
+  k_finalize<<<1, 1024, 0, st>>>(partials, n_values, blocks, results, slot);
+  return cudaGetLastError();
+}
+
+__global__ void k_combine(double* r, int out, int a, int b, int c) { r[out] = r[a] + r[b] - r[c]; }
+
+cudaError_t launch_combine(double* results, int out, int a, int b, int c, cudaStream_t st)
+{
+  k_combine<<<1, 1, 0, st>>>(results, out, a, b, c);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// per-site random fields (qcd-utils.cpp:47-92)
+
+struct RngArg {
+  uint32_t v[24];
+};
+
+// set_g_rand_anti_hermitian_matrix_field: per site RngState(rs, gindex),
+// 4 x make_g_rand_anti_hermitian_matrix (matrix-hmc.h:125-142).
+template <typename R>
+__global__ void __launch_bounds__(128) k_rand_momentum(Geo g, RngArg ra, double s_sigma, double inv_sqrt3,
+                                                       Cx<R>* P, int* ambiguous)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.V) return;
+  Rng base, rs;
+  rng_import(base, ra.v);
+  rng_split_long(rs, base, (int64_t)s);
+  int amb = 0;
+  const WField<R> Pf{P, g.V};
+  for (int mu = 0; mu < 4; ++mu) {
+    double b[8];
+    for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
+    const M3<double> m = x_make_anti_hermitian(b, inv_sqrt3);
+    M3<R> mr;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) mr.e[k] = cx<R>((R)m.e[k].re, (R)m.e[k].im);
+    Pf.st(s, mu, mr);
+  }
+  if (amb) atomicAdd(ambiguous, 1);
+}
+
+template <typename R>
+cudaError_t launch_rand_momentum(const Geo& g, void* P, const uint32_t* rs24, double sigma, int* ambiguous,
+                                 cudaStream_t st)
+{
+  RngArg ra;
+  memcpy(ra.v, rs24, sizeof(ra.v));
+  const double s_sigma = sigma / sqrt(2.0);
+  const double inv_sqrt3 = 1.0 / sqrt(3.0);
+  const int bs = 128;
+  k_rand_momentum<R><<<(unsigned)((g.V + bs - 1) / bs), bs, 0, st>>>(g, ra, s_sigma, inv_sqrt3, (Cx<R>*)P,
+                                                                     ambiguous);
+  return cudaGetLastError();
+}
+
+// set_g_rand_color_matrix_field: per link n_step products of
+// unitarize(exp_taylor20(X)) with X from make_g_rand_anti_hermitian_matrix.
+template <typename R>
+__global__ void __launch_bounds__(128) k_hot_start(Geo g, RngArg ra, double s_sigma, double inv_sqrt3, int n_step,
+                                                   Cx<R>* U, int* ambiguous)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.V) return;
+  Rng base, rs;
+  rng_import(base, ra.v);
+  rng_split_long(rs, base, (int64_t)s);
+  int amb = 0;
+  const WField<R> Uf{U, g.V};
+  for (int mu = 0; mu < 4; ++mu) {
+    M3<double> v;
+    const int nk = n_step > 1 ? n_step : 1;  // the reference always draws at least one factor
+    for (int k = 0; k < nk; ++k) {
+      double b[8];
+      for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
+      M3<double> e = x_exp_taylor20(x_make_anti_hermitian(b, inv_sqrt3));
+      x_unitarize(e);
+      v = (k == 0) ? e : xm_mul(v, e);
+    }
+    M3<R> vr;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) vr.e[k] = cx<R>((R)v.e[k].re, (R)v.e[k].im);
+    Uf.st(s, mu, vr);
+  }
+  if (amb) atomicAdd(ambiguous, 1);
+}
+
+template <typename R>
+cudaError_t launch_hot_start(const Geo& g, void* U, const uint32_t* rs24, double sigma, int n_step, int* ambiguous,
+                             cudaStream_t st)
+{
+  RngArg ra;
+  memcpy(ra.v, rs24, sizeof(ra.v));
+  const double s_sigma = sigma / sqrt(2.0);
+  const double inv_sqrt3 = 1.0 / sqrt(3.0);
+  const int bs = 128;
+  k_hot_start<R><<<(unsigned)((g.V + bs - 1) / bs), bs, 0, st>>>(g, ra, s_sigma, inv_sqrt3, n_step, (Cx<R>*)U,
+                                                                 ambiguous);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// elementwise field operations
+
+template <typename R>
+__global__ void k_set_unit(long V, int m, Cx<R>* U)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  const WField<R> Uf{U, V};
+  for (int mu = 0; mu < m; ++mu) Uf.st(s, mu, m3_unit<R>());
+}
+
+template <typename R>
+cudaError_t launch_set_unit(const Geo& g, int m, void* U, cudaStream_t st)
+{
+  k_set_unit<R><<<(unsigned)((g.V + 255) / 256), 256, 0, st>>>(g.V, m, (Cx<R>*)U);
+  return cudaGetLastError();
+}
+
+template <typename R>
+__global__ void k_axpby(long n, R* y, R a, const R* x, R b)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const R xv = x ? x[i] : R(0);
+    y[i] = (b == R(0)) ? a * xv : fma(a, xv, b * y[i]);
+  }
+}
+
+template <typename R>
+cudaError_t launch_axpby(long n, void* y, double a, const void* x, double b, cudaStream_t st)
+{
+  const long blocks = (n + 255) / 256;
+  k_axpby<R><<<(unsigned)(blocks < 148 * 32 ? blocks : 148 * 32), 256, 0, st>>>(n, (R*)y, (R)a, (const R*)x, (R)b);
+  return cudaGetLastError();
+}
+
+// reference image [site][m][k] (doubles) <-> SoA [m][k/2 complex or 1 real][site]
+template <typename R>
+__global__ void k_aos_to_soa(long V, int m, int k_per, const double* __restrict__ aos, R* __restrict__ soa)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over V * m * k_per, SoA order
+  const long n = V * m * k_per;
+  if (i >= n) return;
+  if (k_per == 1) {
+    const long s = i % V, mm = i / V;
+    soa[i] = (R)aos[s * m + mm];
+  } else {
+    // SoA element (mm, c, s, re/im): index ((mm*9 + c)*V + s)*2 + ri
+    const int ri = (int)(i & 1);
+    const long j = i >> 1;
+    const long s = j % V;
+    const long mc = j / V;
+    const long mm = mc / 9, c = mc % 9;
+    soa[i] = (R)aos[((s * m + mm) * 9 + c) * 2 + ri];
+  }
+}
+
+template <typename R>
+__global__ void k_soa_to_aos(long V, int m, int k_per, const R* __restrict__ soa, double* __restrict__ aos)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over AoS order
+  const long n = V * m * k_per;
+  if (i >= n) return;
+  if (k_per == 1) {
+    const long s = i / m, mm = i % m;
+    aos[i] = (double)soa[mm * V + s];
+  } else {
+    const int ri = (int)(i & 1);
+    const long j = i >> 1;  // (s*m + mm)*9 + c
+    const long c = j % 9;
+    const long sm = j / 9;
+    const long mm = sm % m, s = sm / m;
+    aos[i] = (double)soa[((mm * 9 + c) * V + s) * 2 + ri];
+  }
+}
+
+template <typename R>
+cudaError_t launch_aos_to_soa(const Geo& g, int m, int k_per, const double* aos, void* soa, cudaStream_t st)
+{
+  const long n = g.V * m * k_per;
+  k_aos_to_soa<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g.V, m, k_per, aos, (R*)soa);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_soa_to_aos(const Geo& g, int m, int k_per, const void* soa, double* aos, cudaStream_t st)
+{
+  const long n = g.V * m * k_per;
+  k_soa_to_aos<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g.V, m, k_per, (const R*)soa, aos);
+  return cudaGetLastError();
+}
+
+template <typename RI, typename RO>
+__global__ void k_convert(long n, const RI* in, RO* out)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = (RO)in[i];
+}
+
+template <typename RI, typename RO>
+cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st)
+{
+  const long blocks = (n + 255) / 256;
+  k_convert<RI, RO><<<(unsigned)(blocks < 148 * 32 ? blocks : 148 * 32), 256, 0, st>>>(n, (const RI*)in, (RO*)out);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// explicit instantiations
+
+#define QGB_INST(R)                                                                                          \
+  template cudaError_t launch_evolve<R>(const Geo&, void*, const void*, double, int, int, cudaStream_t);    \
+  template cudaError_t launch_gm_hamilton<R>(const Geo&, const void*, double*, cudaStream_t);              \
+  template cudaError_t launch_action<R>(const Geo&, const void*, int, double*, cudaStream_t);              \
+  template cudaError_t launch_clover<R>(const Geo&, const void*, void*, void*, double*, cudaStream_t);     \
+  template cudaError_t launch_qnorm<R>(long, const void*, double*, int, cudaStream_t);                    \
+  template cudaError_t launch_rand_momentum<R>(const Geo&, void*, const uint32_t*, double, int*, cudaStream_t); \
+  template cudaError_t launch_hot_start<R>(const Geo&, void*, const uint32_t*, double, int, int*, cudaStream_t); \
+  template cudaError_t launch_set_unit<R>(const Geo&, int, void*, cudaStream_t);                          \
+  template cudaError_t launch_axpby<R>(long, void*, double, const void*, double, cudaStream_t);           \
+  template cudaError_t launch_aos_to_soa<R>(const Geo&, int, int, const double*, void*, cudaStream_t);    \
+  template cudaError_t launch_soa_to_aos<R>(const Geo&, int, int, const void*, double*, cudaStream_t);
+
+QGB_INST(double)
+QGB_INST(float)
+template cudaError_t launch_unitarize<double, double>(const Geo&, int, void*, cudaStream_t);
+template cudaError_t launch_unitarize<float, float>(const Geo&, int, void*, cudaStream_t);
+template cudaError_t launch_unitarize<float, double>(const Geo&, int, void*, cudaStream_t);
+template cudaError_t launch_convert<double, float>(long, const void*, void*, cudaStream_t);
+template cudaError_t launch_convert<float, double>(long, const void*, void*, cudaStream_t);
+template cudaError_t launch_convert<double, double>(long, const void*, void*, cudaStream_t);
+template cudaError_t launch_convert<float, float>(long, const void*, void*, cudaStream_t);
+
+}  // namespace qgb
+
+namespace qgb
+{
+// ------------------------------------------------------------------------
+// host RngState API
+
+void rng_host_seed(uint32_t out[24], const char* seed)
+{
+  Rng r;
+  memset(&r, 0, sizeof(r));
+  memcpy(r.hash, qgb_sha_host.h0, 32);
+  r.type = RNG_NO_TYPE;
+  Rng o;
+  rng_split_bytes(o, r, (const uint8_t*)seed, (int)strlen(seed));
+  rng_export(out, o);
+}
+
+bool rng_host_split(uint32_t out[24], const uint32_t rs[24], const char* sindex)
+{
+  Rng r, o;
+  rng_import(r, rs);
+  if (!rng_split_bytes(o, r, (const uint8_t*)sindex, (int)strlen(sindex))) return false;
+  rng_export(out, o);
+  return true;
+}
+
+uint64_t rng_host_rand_gen(uint32_t rs[24])
+{
+  Rng r;
+  rng_import(r, rs);
+  const uint64_t v = rng_rand_gen(r);
+  rng_export(rs, r);
+  return v;
+}
+
+double rng_host_u_rand_gen(uint32_t rs[24], double upper, double lower)
+{
+  Rng r;
+  rng_import(r, rs);
+  const double v = rng_u_rand_gen(r, upper, lower);
+  rng_export(rs, r);
+  return v;
+}
+
+double rng_host_g_rand_gen(uint32_t rs[24], double center, double sigma)
+{
+  Rng r;
+  rng_import(r, rs);
+  const double v = rng_g_rand_gen<false>(r, center, sigma, nullptr);
+  rng_export(rs, r);
+  return v;
+}
+}  // namespace qgb

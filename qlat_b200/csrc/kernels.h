@@ -1,0 +1,101 @@
+// kernels.h -- host-side launch interface of the gauge kernels (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace qgb
+{
+
+struct Geo {
+  int d[4];  // X, Y, Z, T
+  long V;
+};
+
+// Force kernel output modes (see kernels.cu).
+enum ForceMode {
+  FORCE_SET = 0,      // out = F
+  FORCE_UPDATE = 1,   // P += dt F
+  FORCE_EVOLVE = 2,   // U_out = unitarize(exp(eps F) U)
+  FORCE_FLOW = 3,     // Z = a F + b Z_prev; U_out = unitarize(exp(eps Z) U)
+};
+
+struct ForceArgs {
+  const void* U;    // links in (SoA)
+  void* out;        // F (SET) / P (UPDATE) / U_out (EVOLVE, FLOW)
+  const void* zp;   // FLOW: Z_prev (may be null when b == 0)
+  void* z;          // FLOW: Z out (may be null)
+  double beta, c1;  // gauge action
+  double dt;        // UPDATE: P += dt F; EVOLVE/FLOW: exp step
+  double a, b;      // FLOW combination
+  int unitarize;    // EVOLVE/FLOW: unitarize after exp
+};
+
+void init_constants();  // SHA-256 and log tables into constant memory (per device)
+
+template <typename R>
+cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st);
+
+// U = exp(eps P) U (optionally unitarized; exp by Cayley-Hamilton series or the
+// reference's order-20 Taylor series).
+template <typename R>
+cudaError_t launch_evolve(const Geo& g, void* U, const void* P, double eps, int unitarize, int taylor,
+                          cudaStream_t st);
+
+// Unitarize all links of a field with multiplicity m; arithmetic in C.
+template <typename R, typename C>
+cudaError_t launch_unitarize(const Geo& g, int m, void* U, cudaStream_t st);
+
+// Reductions write n_values partial sums per block into `partials`
+// (layout [value][block]); finalize sums them into results[slot..].
+int reduce_blocks(const Geo& g);
+template <typename R>
+cudaError_t launch_gm_hamilton(const Geo& g, const void* P, double* partials, cudaStream_t st);
+// values: 0 = sum(ReTr plaq - 3), 1 = sum(ReTr rect - 3) (if rect)
+template <typename R>
+cudaError_t launch_action(const Geo& g, const void* U, int rect, double* partials, cudaStream_t st);
+// values: 0 = energy density sum, 1 = clover topological charge sum; optional fields
+template <typename R>
+cudaError_t launch_clover(const Geo& g, const void* U, void* e_field, void* q_field, double* partials,
+                          cudaStream_t st);
+template <typename R>
+cudaError_t launch_qnorm(long n_reals, const void* x, double* partials, int blocks, cudaStream_t st);
+cudaError_t launch_finalize(const double* partials, int n_values, int blocks, double* results, int slot,
+                            cudaStream_t st);
+// results[out] = results[a] + results[b] - results[c] (delta H bookkeeping on the device)
+cudaError_t launch_combine(double* results, int out, int a, int b, int c, cudaStream_t st);
+
+// Per-site RNG kernels; rs = 24 x u32 serialised RngState.
+template <typename R>
+cudaError_t launch_rand_momentum(const Geo& g, void* P, const uint32_t* rs24, double sigma,
+                                 int* ambiguous, cudaStream_t st);
+template <typename R>
+cudaError_t launch_hot_start(const Geo& g, void* U, const uint32_t* rs24, double sigma, int n_step,
+                             int* ambiguous, cudaStream_t st);
+
+template <typename R>
+cudaError_t launch_set_unit(const Geo& g, int m, void* U, cudaStream_t st);
+// y = a x + b y over n reals
+template <typename R>
+cudaError_t launch_axpby(long n, void* y, double a, const void* x, double b, cudaStream_t st);
+// Layout conversion: reference image (AoS doubles, [site][m][k]) <-> SoA field.
+// k_per = 18 for color matrices, 1 for real fields.
+template <typename R>
+cudaError_t launch_aos_to_soa(const Geo& g, int m, int k_per, const double* aos, void* soa, cudaStream_t st);
+template <typename R>
+cudaError_t launch_soa_to_aos(const Geo& g, int m, int k_per, const void* soa, double* aos, cudaStream_t st);
+template <typename RI, typename RO>
+cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st);
+
+}  // namespace qgb
+
+namespace qgb
+{
+// Host-side RngState operations (same code as the device streams; the
+// Gaussian draw uses the C library's log on the host, like the reference).
+void rng_host_seed(uint32_t out[24], const char* seed);
+bool rng_host_split(uint32_t out[24], const uint32_t rs[24], const char* sindex);
+uint64_t rng_host_rand_gen(uint32_t rs[24]);
+double rng_host_u_rand_gen(uint32_t rs[24], double upper, double lower);
+double rng_host_g_rand_gen(uint32_t rs[24], double center, double sigma);
+}  // namespace qgb

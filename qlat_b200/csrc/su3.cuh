@@ -1,0 +1,493 @@
+// su3.cuh -- 3x3 complex matrix algebra for the gauge kernels (FP64 / FP32).
+//
+// Conventions follow Qlattice's ColorMatrix (qlat-utils mat-vec.h:115,
+// matrix.h:45-260): row-major, element (i, j) at e[3*i + j].  The functions
+// here are written for registers: everything is unrolled and products use
+// fused multiply-adds.  Algorithms that change the order of floating-point
+// operations relative to the reference are noted where they occur; all agree
+// with the reference to rounding level (checked against the oracle).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define QGB_HD __host__ __device__ __forceinline__
+#else
+#define QGB_HD inline
+#endif
+
+namespace qgb
+{
+
+template <typename R>
+struct alignas(2 * sizeof(R)) Cx {
+  R re, im;
+};
+
+template <typename R>
+struct M3 {
+  Cx<R> e[9];
+};
+
+template <typename R>
+QGB_HD Cx<R> cx(R re, R im)
+{
+  Cx<R> c;
+  c.re = re;
+  c.im = im;
+  return c;
+}
+
+template <typename R>
+QGB_HD M3<R> m3_zero()
+{
+  M3<R> m;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) m.e[i] = cx<R>(0, 0);
+  return m;
+}
+
+template <typename R>
+QGB_HD M3<R> m3_unit()
+{
+  M3<R> m = m3_zero<R>();
+  m.e[0].re = m.e[4].re = m.e[8].re = R(1);
+  return m;
+}
+
+// c = a * b
+template <typename R>
+QGB_HD M3<R> mul(const M3<R>& a, const M3<R>& b)
+{
+  M3<R> c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = a.e[3 * i].re * b.e[j].re;
+      R im = a.e[3 * i].re * b.e[j].im;
+      re = fma(-a.e[3 * i].im, b.e[j].im, re);
+      im = fma(a.e[3 * i].im, b.e[j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; ++k) {
+        re = fma(a.e[3 * i + k].re, b.e[3 * k + j].re, re);
+        re = fma(-a.e[3 * i + k].im, b.e[3 * k + j].im, re);
+        im = fma(a.e[3 * i + k].re, b.e[3 * k + j].im, im);
+        im = fma(a.e[3 * i + k].im, b.e[3 * k + j].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// c = a * b^dagger : c_ij = sum_k a_ik conj(b_jk)
+template <typename R>
+QGB_HD M3<R> mul_adj(const M3<R>& a, const M3<R>& b)
+{
+  M3<R> c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = a.e[3 * i].re * b.e[3 * j].re;
+      R im = -a.e[3 * i].re * b.e[3 * j].im;
+      re = fma(a.e[3 * i].im, b.e[3 * j].im, re);
+      im = fma(a.e[3 * i].im, b.e[3 * j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; ++k) {
+        re = fma(a.e[3 * i + k].re, b.e[3 * j + k].re, re);
+        re = fma(a.e[3 * i + k].im, b.e[3 * j + k].im, re);
+        im = fma(-a.e[3 * i + k].re, b.e[3 * j + k].im, im);
+        im = fma(a.e[3 * i + k].im, b.e[3 * j + k].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// c = a^dagger * b : c_ij = sum_k conj(a_ki) b_kj
+template <typename R>
+QGB_HD M3<R> adj_mul(const M3<R>& a, const M3<R>& b)
+{
+  M3<R> c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = a.e[i].re * b.e[j].re;
+      R im = a.e[i].re * b.e[j].im;
+      re = fma(a.e[i].im, b.e[j].im, re);
+      im = fma(-a.e[i].im, b.e[j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; ++k) {
+        re = fma(a.e[3 * k + i].re, b.e[3 * k + j].re, re);
+        re = fma(a.e[3 * k + i].im, b.e[3 * k + j].im, re);
+        im = fma(a.e[3 * k + i].re, b.e[3 * k + j].im, im);
+        im = fma(-a.e[3 * k + i].im, b.e[3 * k + j].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// s + a * b
+template <typename R>
+QGB_HD M3<R> add_mul(const M3<R>& s, const M3<R>& a, const M3<R>& b)
+{
+  M3<R> c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = s.e[3 * i + j].re, im = s.e[3 * i + j].im;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        re = fma(a.e[3 * i + k].re, b.e[3 * k + j].re, re);
+        re = fma(-a.e[3 * i + k].im, b.e[3 * k + j].im, re);
+        im = fma(a.e[3 * i + k].re, b.e[3 * k + j].im, im);
+        im = fma(a.e[3 * i + k].im, b.e[3 * k + j].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// s + a * b^dagger
+template <typename R>
+QGB_HD M3<R> add_mul_adj(const M3<R>& s, const M3<R>& a, const M3<R>& b)
+{
+  M3<R> c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = s.e[3 * i + j].re, im = s.e[3 * i + j].im;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        re = fma(a.e[3 * i + k].re, b.e[3 * j + k].re, re);
+        re = fma(a.e[3 * i + k].im, b.e[3 * j + k].im, re);
+        im = fma(-a.e[3 * i + k].re, b.e[3 * j + k].im, im);
+        im = fma(a.e[3 * i + k].im, b.e[3 * j + k].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// s + a^dagger * b
+template <typename R>
+QGB_HD M3<R> add_adj_mul(const M3<R>& s, const M3<R>& a, const M3<R>& b)
+{
+  M3<R> c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = s.e[3 * i + j].re, im = s.e[3 * i + j].im;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        re = fma(a.e[3 * k + i].re, b.e[3 * k + j].re, re);
+        re = fma(a.e[3 * k + i].im, b.e[3 * k + j].im, re);
+        im = fma(a.e[3 * k + i].re, b.e[3 * k + j].im, im);
+        im = fma(-a.e[3 * k + i].im, b.e[3 * k + j].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+template <typename R>
+QGB_HD M3<R> adj(const M3<R>& a)
+{
+  M3<R> c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) c.e[3 * i + j] = cx<R>(a.e[3 * j + i].re, -a.e[3 * j + i].im);
+  return c;
+}
+
+// a += s * b
+template <typename R>
+QGB_HD void axpy(M3<R>& a, R s, const M3<R>& b)
+{
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    a.e[i].re = fma(s, b.e[i].re, a.e[i].re);
+    a.e[i].im = fma(s, b.e[i].im, a.e[i].im);
+  }
+}
+
+template <typename R>
+QGB_HD void add_to(M3<R>& a, const M3<R>& b)
+{
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    a.e[i].re += b.e[i].re;
+    a.e[i].im += b.e[i].im;
+  }
+}
+
+template <typename R>
+QGB_HD M3<R> scale(R s, const M3<R>& b)
+{
+  M3<R> a;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) a.e[i] = cx<R>(s * b.e[i].re, s * b.e[i].im);
+  return a;
+}
+
+// Re tr(a b^dagger) = sum_ij Re(a_ij conj(b_ij))
+template <typename R>
+QGB_HD R re_tr_mul_adj(const M3<R>& a, const M3<R>& b)
+{
+  R s = a.e[0].re * b.e[0].re;
+  s = fma(a.e[0].im, b.e[0].im, s);
+#pragma unroll
+  for (int i = 1; i < 9; ++i) {
+    s = fma(a.e[i].re, b.e[i].re, s);
+    s = fma(a.e[i].im, b.e[i].im, s);
+  }
+  return s;
+}
+
+// Re tr(a b) = sum_ij Re(a_ij b_ji)
+template <typename R>
+QGB_HD R re_tr_mul(const M3<R>& a, const M3<R>& b)
+{
+  R s = R(0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      s = fma(a.e[3 * i + j].re, b.e[3 * j + i].re, s);
+      s = fma(-a.e[3 * i + j].im, b.e[3 * j + i].im, s);
+    }
+  return s;
+}
+
+template <typename R>
+QGB_HD R re_tr(const M3<R>& a)
+{
+  return a.e[0].re + a.e[4].re + a.e[8].re;
+}
+
+// Traceless anti-Hermitian part (m - m^dagger)/2 - tr(m - m^dagger)/6
+// (matrix-hmc.h:202-213).  The diagonal of (m - m^dagger)/2 is i Im(m_ii).
+template <typename R>
+QGB_HD M3<R> traceless_antiherm(const M3<R>& m)
+{
+  M3<R> r;
+  const R c = (m.e[0].im + m.e[4].im + m.e[8].im) / R(3);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.e[4 * i] = cx<R>(R(0), m.e[4 * i].im - c);
+#pragma unroll
+    for (int j = i + 1; j < 3; ++j) {
+      const R re = R(0.5) * (m.e[3 * i + j].re - m.e[3 * j + i].re);
+      const R im = R(0.5) * (m.e[3 * i + j].im + m.e[3 * j + i].im);
+      r.e[3 * i + j] = cx<R>(re, im);
+      r.e[3 * j + i] = cx<R>(-re, im);
+    }
+  }
+  return r;
+}
+
+// -1/2 tr(m^2) for anti-Hermitian m in the su(3) basis with tr(T_a T_b) = -2 delta_ab:
+// sum of the squared basis coefficients (matrix-hmc.h:144-152).
+template <typename R>
+QGB_HD double neg_half_tr_square(const M3<R>& m)
+{
+  const double p1 = m.e[0].im, p9 = m.e[4].im, p17 = m.e[8].im;
+  const double p2 = m.e[1].re, p3 = m.e[1].im, p4 = m.e[2].re, p5 = m.e[2].im;
+  const double p10 = m.e[5].re, p11 = m.e[5].im;
+  return p3 * p3 + p2 * p2 + (p1 - p9) * (p1 - p9) * 0.25 + p5 * p5 + p4 * p4 + p11 * p11 + p10 * p10 +
+         p17 * p17 * 0.75;
+}
+
+// Gram-Schmidt projection onto SU(3) (matrix-hmc.h:11-74): normalise row 1,
+// orthogonalise and normalise row 2, row 3 = conj(row1 x row2).  The
+// arithmetic type C may be wider than the storage type (FP64 arithmetic on
+// FP32 links).
+template <typename C, typename R>
+QGB_HD void unitarize_as(M3<R>& m)
+{
+  C r1[6], r2[6];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    r1[2 * k] = C(m.e[k].re);
+    r1[2 * k + 1] = C(m.e[k].im);
+    r2[2 * k] = C(m.e[3 + k].re);
+    r2[2 * k + 1] = C(m.e[3 + k].im);
+  }
+  C n1 = C(0);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) n1 = fma(r1[k], r1[k], n1);
+  if (!(n1 == C(1))) {
+    const C inv = C(1) / sqrt(n1);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) r1[k] *= inv;
+  }
+  // c = sum_k conj(r1_k) r2_k
+  C cre = C(0), cim = C(0);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    cre = fma(r1[2 * k], r2[2 * k], cre);
+    cre = fma(r1[2 * k + 1], r2[2 * k + 1], cre);
+    cim = fma(r1[2 * k], r2[2 * k + 1], cim);
+    cim = fma(-r1[2 * k + 1], r2[2 * k], cim);
+  }
+  if (!(cre == C(0) && cim == C(0))) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const C are = r1[2 * k], aim = r1[2 * k + 1];
+      r2[2 * k] -= cre * are - cim * aim;
+      r2[2 * k + 1] -= cre * aim + cim * are;
+    }
+  }
+  C n2 = C(0);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) n2 = fma(r2[k], r2[k], n2);
+  if (!(n2 == C(1))) {
+    const C inv = C(1) / sqrt(n2);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) r2[k] *= inv;
+  }
+  // row 3 = conj(r1 x r2)
+  const C a0r = r1[0], a0i = r1[1], a1r = r1[2], a1i = r1[3], a2r = r1[4], a2i = r1[5];
+  const C b0r = r2[0], b0i = r2[1], b1r = r2[2], b1i = r2[3], b2r = r2[4], b2i = r2[5];
+  const C x0r = (a1r * b2r - a1i * b2i) - (a2r * b1r - a2i * b1i);
+  const C x0i = (a1r * b2i + a1i * b2r) - (a2r * b1i + a2i * b1r);
+  const C x1r = (a2r * b0r - a2i * b0i) - (a0r * b2r - a0i * b2i);
+  const C x1i = (a2r * b0i + a2i * b0r) - (a0r * b2i + a0i * b2r);
+  const C x2r = (a0r * b1r - a0i * b1i) - (a1r * b0r - a1i * b0i);
+  const C x2i = (a0r * b1i + a0i * b1r) - (a1r * b0i + a1i * b0r);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    m.e[k] = cx<R>(R(r1[2 * k]), R(r1[2 * k + 1]));
+    m.e[3 + k] = cx<R>(R(r2[2 * k]), R(r2[2 * k + 1]));
+  }
+  m.e[6] = cx<R>(R(x0r), R(-x0i));
+  m.e[7] = cx<R>(R(x1r), R(-x1i));
+  m.e[8] = cx<R>(R(x2r), R(-x2i));
+}
+
+template <typename R>
+QGB_HD void unitarize(M3<R>& m)
+{
+  unitarize_as<R, R>(m);
+}
+
+// exp(a) by the order-N Taylor series in Horner form, exactly the
+// reference's make_matrix_exp (matrix-hmc.h:155-167).  Used where the
+// reference's own truncation must be reproduced (the hot start).
+template <typename R>
+QGB_HD M3<R> exp_taylor(const M3<R>& a, int max_order = 20)
+{
+  M3<R> t2 = a;
+  M3<R> t3;
+  for (int j = max_order; j > 1; --j) {
+    t3 = scale(R(1) / R(j), t2);
+    t3.e[0].re += R(1);
+    t3.e[4].re += R(1);
+    t3.e[8].re += R(1);
+    t2 = mul(a, t3);
+  }
+  t3 = t2;
+  t3.e[0].re += R(1);
+  t3.e[4].re += R(1);
+  t3.e[8].re += R(1);
+  return t3;
+}
+
+// Complex helpers for the Cayley-Hamilton exponential.
+template <typename R>
+QGB_HD Cx<R> cmul(Cx<R> a, Cx<R> b)
+{
+  return cx<R>(fma(a.re, b.re, -a.im * b.im), fma(a.re, b.im, a.im * b.re));
+}
+
+// exp(a) for a 3x3 matrix through the Cayley-Hamilton theorem: with
+// t = tr a, s = (t^2 - tr a^2)/2, d = det a, every power a^n equals
+// x_n 1 + y_n a + z_n a^2 with (x, y, z)_{n+1} = (z_n d, x_n - z_n s, y_n + z_n t).
+// exp(a) = f0 1 + f1 a + f2 a^2 with f = sum_n (x, y, z)_n / n!, summed until
+// the terms fall below the working precision.  For |a| > 1 the argument is
+// halved k times first and the result squared k times.  Cost: ~3 matrix
+// products instead of the 19 of the order-20 Taylor series, and no
+// truncation at order 20; the two agree to rounding for the step sizes of
+// HMC and gradient flow.
+template <typename R>
+QGB_HD M3<R> exp_ch(const M3<R>& a_in)
+{
+  // Frobenius norm bound for the scaling step
+  R n2 = R(0);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) n2 = fma(a_in.e[i].re, a_in.e[i].re, fma(a_in.e[i].im, a_in.e[i].im, n2));
+  int k = 0;
+  R sc = R(1);
+  while (n2 > R(1) && k < 30) {
+    n2 *= R(0.25);
+    sc *= R(0.5);
+    ++k;
+  }
+  const M3<R> a = (k > 0) ? scale(sc, a_in) : a_in;
+  const M3<R> a2 = mul(a, a);
+  const Cx<R> t = cx<R>(a.e[0].re + a.e[4].re + a.e[8].re, a.e[0].im + a.e[4].im + a.e[8].im);
+  const Cx<R> t2 = cx<R>(a2.e[0].re + a2.e[4].re + a2.e[8].re, a2.e[0].im + a2.e[4].im + a2.e[8].im);
+  const Cx<R> tt = cmul(t, t);
+  const Cx<R> s = cx<R>(R(0.5) * (tt.re - t2.re), R(0.5) * (tt.im - t2.im));
+  // det a by cofactor expansion along row 0
+  const Cx<R> m0 = cx<R>(cmul(a.e[4], a.e[8]).re - cmul(a.e[5], a.e[7]).re,
+                         cmul(a.e[4], a.e[8]).im - cmul(a.e[5], a.e[7]).im);
+  const Cx<R> m1 = cx<R>(cmul(a.e[5], a.e[6]).re - cmul(a.e[3], a.e[8]).re,
+                         cmul(a.e[5], a.e[6]).im - cmul(a.e[3], a.e[8]).im);
+  const Cx<R> m2 = cx<R>(cmul(a.e[3], a.e[7]).re - cmul(a.e[4], a.e[6]).re,
+                         cmul(a.e[3], a.e[7]).im - cmul(a.e[4], a.e[6]).im);
+  const Cx<R> d0 = cmul(a.e[0], m0), d1 = cmul(a.e[1], m1), d2 = cmul(a.e[2], m2);
+  const Cx<R> d = cx<R>(d0.re + d1.re + d2.re, d0.im + d1.im + d2.im);
+  // series
+  Cx<R> x = cx<R>(R(1), R(0)), y = cx<R>(R(0), R(0)), z = cx<R>(R(0), R(0));
+  Cx<R> f0 = x, f1 = y, f2 = z;
+  const int nmax = sizeof(R) == 8 ? 22 : 13;
+#pragma unroll 4
+  for (int n = 1; n <= nmax; ++n) {
+    const R inv = R(1) / R(n);
+    const Cx<R> zd = cmul(z, d), zs = cmul(z, s), zt = cmul(z, t);
+    const Cx<R> xn = cx<R>(zd.re * inv, zd.im * inv);
+    const Cx<R> yn = cx<R>((x.re - zs.re) * inv, (x.im - zs.im) * inv);
+    const Cx<R> zn = cx<R>((y.re + zt.re) * inv, (y.im + zt.im) * inv);
+    x = xn;
+    y = yn;
+    z = zn;
+    f0.re += x.re;
+    f0.im += x.im;
+    f1.re += y.re;
+    f1.im += y.im;
+    f2.re += z.re;
+    f2.im += z.im;
+  }
+  M3<R> r;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const Cx<R> p = cmul(f1, a.e[i]);
+    const Cx<R> q = cmul(f2, a2.e[i]);
+    r.e[i] = cx<R>(p.re + q.re, p.im + q.im);
+  }
+  r.e[0].re += f0.re;
+  r.e[0].im += f0.im;
+  r.e[4].re += f0.re;
+  r.e[4].im += f0.im;
+  r.e[8].re += f0.re;
+  r.e[8].im += f0.im;
+  for (int i = 0; i < k; ++i) r = mul(r, r);
+  return r;
+}
+
+}  // namespace qgb

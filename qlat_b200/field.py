@@ -1,0 +1,305 @@
+"""Lattice geometry, RngState and GPU-resident fields, mirroring qlat's
+``Geometry``, ``RngState``, ``GaugeField`` (qcd.pyx:45-88), ``GaugeMomentum``
+(hmc.pyx:39-53), ``FieldRealD`` and ``GaugeAction`` (gauge_action.pyx:18-36).
+
+A field lives in GPU memory behind a C ABI handle (include/qlat_b200.h).
+``np.asarray(field)`` downloads it in the reference memory image
+(shape ``(V, multiplicity, 3, 3)`` complex128 for color matrices,
+``(V, multiplicity)`` float64 for real fields, sites x-fastest);
+``field.from_numpy(arr)`` uploads.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import call
+
+F64 = 64
+F32 = 32
+KIND_COLOR_MATRIX = 0
+KIND_REAL = 1
+
+
+class Coordinate(tuple):
+    """Minimal stand-in for qlat.Coordinate (a 4-tuple of ints)."""
+
+    def __new__(cls, x=(0, 0, 0, 0)):
+        v = tuple(int(a) for a in x)
+        assert len(v) == 4
+        return super().__new__(cls, v)
+
+    def to_list(self):
+        return list(self)
+
+    def volume(self):
+        return int(np.prod(self))
+
+
+class Geometry:
+    """qlat.Geometry(total_site) for one node (core.h:92-359)."""
+
+    def __init__(self, total_site=None):
+        self.total_site = Coordinate(total_site if total_site is not None else (1, 1, 1, 1))
+
+    @property
+    def total_volume(self) -> int:
+        return self.total_site.volume()
+
+    @property
+    def local_volume(self) -> int:
+        return self.total_volume
+
+    def __eq__(self, other):
+        return isinstance(other, Geometry) and self.total_site == other.total_site
+
+    def __repr__(self):
+        return f"Geometry({list(self.total_site)})"
+
+    def show(self):
+        return repr(self)
+
+
+class RngState:
+    """qlat.RngState (rng-state.h:38-99): a SHA-256 counter RNG; the state is
+    the 24 x uint32 serialised form of the reference (rng-state.cpp:61-81)."""
+
+    def __init__(self, seed: str | int | None = None):
+        self._v = (ctypes.c_uint32 * 24)()
+        if seed is None:
+            # reset(rs) (rng-state.cpp:150-164): initial SHA-256 hash (first 32
+            # fractional bits of the square roots of the first 8 primes), no
+            # bytes hashed, type = ULONG_MAX
+            h0 = [math.isqrt(p << 64) & 0xFFFFFFFF for p in (2, 3, 5, 7, 11, 13, 17, 19)]
+            v = [0, 0] + h0 + [0xFFFFFFFF, 0xFFFFFFFF] + [0] * 12
+            for i in range(24):
+                self._v[i] = v[i]
+        else:
+            call("qgb_rng_seed", self._v, str(seed).encode())
+
+    @classmethod
+    def _from(cls, arr) -> "RngState":
+        r = cls.__new__(cls)
+        r._v = (ctypes.c_uint32 * 24)(*list(arr))
+        return r
+
+    def copy(self) -> "RngState":
+        return RngState._from(list(self._v))
+
+    def split(self, sindex) -> "RngState":
+        out = (ctypes.c_uint32 * 24)()
+        call("qgb_rng_split", out, self._v, str(sindex).encode())
+        return RngState._from(list(out))
+
+    def rand_gen(self) -> int:
+        o = ctypes.c_uint64()
+        call("qgb_rng_rand_gen", self._v, ctypes.byref(o))
+        return int(o.value)
+
+    def u_rand_gen(self, upper: float = 1.0, lower: float = 0.0) -> float:
+        o = ctypes.c_double()
+        call("qgb_rng_u_rand_gen", self._v, upper, lower, ctypes.byref(o))
+        return o.value
+
+    def g_rand_gen(self, center: float = 0.0, sigma: float = 1.0) -> float:
+        o = ctypes.c_double()
+        call("qgb_rng_g_rand_gen", self._v, center, sigma, ctypes.byref(o))
+        return o.value
+
+    def export(self) -> np.ndarray:
+        return np.array(list(self._v), dtype=np.uint32)
+
+    @property
+    def c(self):
+        return self._v
+
+
+class GaugeAction:
+    """qlat.GaugeAction(beta, c1) (gauge-action.h:8-28): Wilson c1 = 0,
+    Iwasaki c1 = -0.331, DBW2 c1 = -1.4008."""
+
+    def __init__(self, beta: float = 5.5, c1: float = 0.0):
+        self._beta = float(beta)
+        self._c1 = float(c1)
+
+    def beta(self) -> float:
+        return self._beta
+
+    def c1(self) -> float:
+        return self._c1
+
+    def __repr__(self):
+        return f"GaugeAction(beta={self._beta}, c1={self._c1})"
+
+
+class Field:
+    """A lattice field in GPU memory (Field<M>, core.h:753-969)."""
+
+    _kind = KIND_COLOR_MATRIX
+
+    def __init__(self, geo: Geometry | None = None, multiplicity: int = 1, *, precision: int = F64,
+                 kind: int | None = None):
+        self._h = None
+        self.geo = geo
+        self.multiplicity = int(multiplicity)
+        self.precision = int(precision)
+        self.kind = self._kind if kind is None else int(kind)
+        if geo is not None:
+            self._create()
+
+    def _create(self):
+        h = ctypes.c_void_p()
+        call("qgb_field_create", ctypes.byref(h), _lib.i32x4(*self.geo.total_site), self.multiplicity,
+             self.kind, self.precision)
+        self._h = h
+
+    def init(self, geo: Geometry, multiplicity: int | None = None):
+        self._free()
+        self.geo = geo
+        if multiplicity is not None:
+            self.multiplicity = int(multiplicity)
+        self._create()
+
+    def _free(self):
+        if self._h is not None and self._h.value:
+            try:
+                _lib.load().qgb_field_destroy(self._h)
+            except Exception:
+                pass
+        self._h = None
+
+    def __del__(self):
+        self._free()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._h is None:
+            raise RuntimeError("field is not initialised (no geometry)")
+        return self._h
+
+    def _like(self) -> "Field":
+        f = self.__class__.__new__(self.__class__)
+        Field.__init__(f, self.geo, self.multiplicity, precision=self.precision, kind=self.kind)
+        return f
+
+    def copy(self, precision: int | None = None) -> "Field":
+        f = self._like()
+        if precision is not None and precision != self.precision:
+            f._free()
+            f.precision = precision
+            f._create()
+        call("qgb_field_copy", f.handle, self.handle)
+        return f
+
+    def __imatmul__(self, other: "Field"):
+        """f @= g: copy (with precision conversion), qlat's field assignment."""
+        if self._h is None:
+            self.geo = other.geo
+            self.multiplicity = other.multiplicity
+            self._create()
+        call("qgb_field_copy", self.handle, other.handle)
+        return self
+
+    def __imul__(self, s: float):
+        call("qgb_field_axpby", self.handle, 0.0, None, float(s))
+        return self
+
+    def __iadd__(self, other: "Field"):
+        call("qgb_field_axpby", self.handle, 1.0, other.handle, 1.0)
+        return self
+
+    def __isub__(self, other: "Field"):
+        call("qgb_field_axpby", self.handle, -1.0, other.handle, 1.0)
+        return self
+
+    def set_zero(self):
+        call("qgb_field_set_zero", self.handle)
+
+    def qnorm(self) -> float:
+        o = ctypes.c_double()
+        call("qgb_field_qnorm", self.handle, ctypes.byref(o))
+        return o.value
+
+    def _shape(self):
+        V = self.geo.total_volume
+        if self.kind == KIND_COLOR_MATRIX:
+            return (V, self.multiplicity, 3, 3), np.complex128
+        return (V, self.multiplicity), np.float64
+
+    def to_numpy(self) -> np.ndarray:
+        shape, dt = self._shape()
+        a = np.empty(shape, dtype=dt)
+        call("qgb_field_download", self.handle, a.ctypes.data_as(_lib.c_dbl_p))
+        return a
+
+    def __array__(self, dtype=None, copy=None):
+        a = self.to_numpy()
+        return a if dtype is None else a.astype(dtype)
+
+    def from_numpy(self, arr) -> "Field":
+        shape, dt = self._shape()
+        a = np.ascontiguousarray(np.asarray(arr, dtype=dt).reshape(shape))
+        call("qgb_field_upload", self.handle, a.ctypes.data_as(_lib.c_dbl_p))
+        return self
+
+    def upload_device(self, ptr: int) -> None:
+        """Copy from a device buffer (e.g. a torch CUDA tensor's data_ptr) in
+        the reference memory image."""
+        call("qgb_field_upload_device", self.handle, ctypes.c_void_p(ptr))
+
+    def download_device(self, ptr: int) -> None:
+        call("qgb_field_download_device", self.handle, ctypes.c_void_p(ptr))
+
+
+class FieldColorMatrix(Field):
+    _kind = KIND_COLOR_MATRIX
+
+
+class FieldRealD(Field):
+    _kind = KIND_REAL
+
+    def glb_sum(self) -> np.ndarray:
+        return self.to_numpy().sum(axis=0, keepdims=True)
+
+
+class GaugeField(FieldColorMatrix):
+    """qlat.GaugeField (qcd.pyx:45-88)."""
+
+    def __init__(self, geo: Geometry | None = None, multiplicity: int = 4, *, precision: int = F64):
+        assert multiplicity == 4
+        super().__init__(geo, 4, precision=precision)
+
+    def set_rand(self, rng: RngState, sigma: float = 0.5, n_step: int = 1):
+        call("qgb_gf_set_rand", self.handle, rng.c, float(sigma), int(n_step))
+
+    def set_unit(self):
+        call("qgb_set_unit", self.handle)
+
+    def unitarize(self):
+        call("qgb_unitarize", self.handle)
+
+    def plaq(self) -> float:
+        from .hmc import gf_avg_plaq
+        return gf_avg_plaq(self)
+
+
+class GaugeMomentum(FieldColorMatrix):
+    """qlat.GaugeMomentum (hmc.pyx:39-53)."""
+
+    def __init__(self, geo: Geometry | None = None, multiplicity: int = 4, *, precision: int = F64):
+        assert multiplicity == 4
+        super().__init__(geo, 4, precision=precision)
+
+    def set_rand(self, rng: RngState, sigma: float = 1.0):
+        call("qgb_set_rand_gauge_momentum", self.handle, float(sigma), rng.c)
+
+
+def set_unit(gf: Field, coef: float = 1.0):
+    """field.h set_unit (everything.pxd:187) for color-matrix fields."""
+    call("qgb_set_unit", gf.handle)
+    if coef != 1.0:
+        gf *= coef

@@ -1,0 +1,66 @@
+#!/usr/bin/env python3
+"""Extract the golden values that pin the pure-gauge path from the
+reference's own test logs into reference_goldens.json.
+
+Run in a checkout that has the reference source tree (default
+/root/reference, or pass its path).  Sources:
+  examples-cpp/hmc/log                        C++ force-gradient HMC, plaq per trajectory
+  examples-py/hmc-pure-gauge.log.json         Python HMC, plaq and delta_h per trajectory
+  examples-py/hmc-pure-gauge-test.log.json    Python HMC from a unit start, plaq per trajectory
+  examples-py/flow-and-smear.log.json         Wilson flow steps and energies
+  examples-py/gf-utils.log.json               hot-start plaquette and clover charge along the flow
+"""
+
+import json
+import os
+import re
+import sys
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    out = {}
+    # C++ HMC log
+    lines = open(os.path.join(ref, "examples-cpp/hmc/log")).read().splitlines()
+    cpp = []
+    for ln in lines:
+        m = re.match(r"CHECK: test_hmc: traj=(\d+) ; plaq_avg=\s*(\S+) ; plaq_sum=\s*(\S+)\.", ln)
+        if m:
+            cpp.append([int(m.group(1)), float(m.group(2)), float(m.group(3))])
+    out["cpp_hmc"] = {"source": "examples-cpp/hmc/log", "rows": cpp, "printed_digits": 13}
+
+    def load(name):
+        d = json.load(open(os.path.join(ref, "examples-py", name)))
+        return {e[0]: [e[1], e[2]] for e in d if len(e) == 3}
+
+    g = load("hmc-pure-gauge.log.json")
+    out["py_hmc"] = {"source": "examples-py/hmc-pure-gauge.log.json",
+                     "plaq": [g[f"run_hmc: {t} plaq"][0] for t in range(1, 9)],
+                     "delta_h": [g[f"run_hmc: {t} delta_h"][0] for t in range(1, 9)],
+                     "eps_plaq": 1e-10, "eps_delta_h": 1e-4}
+    g = load("hmc-pure-gauge-test.log.json")
+    out["py_hmc_test"] = {"source": "examples-py/hmc-pure-gauge-test.log.json",
+                          "iwasaki_plaq": [g[f"beta=2.13_c1=-0.331 traj={t} plaq"][0] for t in range(1, 5)],
+                          "wilson_plaq": [g[f"beta=5.5_c1=0.0 traj={t} plaq"][0] for t in range(1, 5)],
+                          "eps": 1e-10}
+    g = load("flow-and-smear.log.json")
+    out["flow"] = {"source": "examples-py/flow-and-smear.log.json",
+                   "rk3_plaq": g["gf_wilson_flow_step runge-kutta plaq"][0],
+                   "euler_plaq": g["gf_wilson_flow_step euler plaq"][0],
+                   "c1_plaq": {str(c1): g[f"gf_wilson_flow_step c1={c1} plaq"][0] for c1 in (0.0, -0.331, -1.4008)},
+                   "flow3_energy": g["gf_wilson_flow energy_list"][0]["value"],
+                   "flow3_plaq": g["gf_wilson_flow final plaq"][0],
+                   "eps": 1e-10}
+    g = load("gf-utils.log.json")
+    out["gf_utils"] = {"source": "examples-py/gf-utils.log.json",
+                       "hot_plaq": g["gf_ape_list[0] plaq"][0],
+                       "topo_clf": {str(t): g[f"t={t} topo_clf"][0] for t in ("0", "1.0", "2.0", "3.0", "4.0", "5.0")},
+                       "eps_topo": 1e-9}
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "reference_goldens.json"), "w") as f:
+        json.dump(out, f, indent=1)
+        f.write("\n")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,177 @@
+"""Parity of each CUDA kernel with the CPU oracle, through the C ABI.
+
+FP64 bar: bit-exact for the random fields (hot start, momenta) against the
+oracle run with a correctly rounded log; 1e-13 normwise for force, evolve and
+flow fields; 1e-12 relative for the reductions.  FP32 storage: 2e-6 normwise.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GEOS = [(4, 4, 4, 8), (3, 4, 5, 6)]
+ACTIONS = [(5.5, 0.0), (2.13, -0.331), (0.9, -1.4008)]
+
+
+def nrel(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def hot_start(q, oracle, ts, seed="gpu-kernels", sigma=0.5, n_step=3):
+    rs = q.RngState(seed).split("gf-init")
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(rs, sigma, n_step)
+    ref = oracle.new_field(ts)
+    oracle.set_log_mode(1)
+    oracle.gf_set_rand(ref, ts, oracle.RngState(seed).split("gf-init"), sigma, n_step)
+    oracle.set_log_mode(0)
+    return gf, ref
+
+
+@pytest.mark.parametrize("ts", GEOS)
+def test_hot_start_bit_exact(q, oracle, ts):
+    gf, ref = hot_start(q, oracle, ts)
+    got = np.asarray(gf)
+    assert got.shape == ref.shape
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+    # against the C library's log: identical except where glibc's log is not
+    # correctly rounded, and then only in the last bits
+    ref_libm = oracle.new_field(ts)
+    oracle.gf_set_rand(ref_libm, ts, oracle.RngState("gpu-kernels").split("gf-init"), 0.5, 3)
+    assert nrel(got, ref_libm) < 1e-14
+    assert q.rng_ambiguous_count() == 0
+
+
+@pytest.mark.parametrize("ts", GEOS)
+def test_momentum_bit_exact(q, oracle, ts):
+    rs = q.RngState("traj-7").split("set_rand_gauge_momentum")
+    gm = q.GaugeMomentum(q.Geometry(ts))
+    gm.set_rand(rs, 1.0)
+    ref = oracle.new_field(ts)
+    oracle.set_log_mode(1)
+    oracle.set_rand_gauge_momentum(ref, ts, oracle.RngState("traj-7").split("set_rand_gauge_momentum"), 1.0)
+    oracle.set_log_mode(0)
+    got = np.asarray(gm)
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+    ref_libm = oracle.new_field(ts)
+    oracle.set_rand_gauge_momentum(ref_libm, ts, oracle.RngState("traj-7").split("set_rand_gauge_momentum"), 1.0)
+    diff = got != ref_libm
+    assert diff.mean() < 0.01
+    assert nrel(got, ref_libm) < 1e-15
+    # gm_hamilton_node on the same momenta
+    h = q.gm_hamilton_node(gm)
+    assert abs(h - oracle.gm_hamilton_node(ref, ts)) <= 1e-12 * abs(h)
+
+
+@pytest.mark.parametrize("ts", GEOS)
+@pytest.mark.parametrize("beta,c1", ACTIONS)
+def test_set_gm_force(q, oracle, ts, beta, c1):
+    gf, ref = hot_start(q, oracle, ts)
+    F = q.GaugeMomentum(gf.geo)
+    q.set_gm_force(F, gf, q.GaugeAction(beta, c1))
+    Fr = oracle.new_field(ts)
+    oracle.set_gm_force(Fr, ref, ts, beta, c1)
+    assert nrel(np.asarray(F), Fr) < 1e-13
+
+
+@pytest.mark.parametrize("ts", GEOS)
+@pytest.mark.parametrize("beta,c1", ACTIONS)
+def test_hamiltonians_and_plaquette(q, oracle, ts, beta, c1):
+    gf, ref = hot_start(q, oracle, ts)
+    ga = q.GaugeAction(beta, c1)
+    h = q.gf_hamilton_node(gf, ga)
+    hr = oracle.gf_hamilton_node(ref, ts, beta, c1)
+    assert abs(h - hr) <= 1e-12 * abs(hr)
+    sp = q.gf_sum_re_tr_plaq_node_no_comm(gf)
+    assert abs(sp - oracle.gf_sum_re_tr_plaq(ref, ts)) <= 1e-12 * abs(sp)
+    sr = q.gf_sum_re_tr_rect_node_no_comm(gf)
+    assert abs(sr - oracle.gf_sum_re_tr_rect(ref, ts)) <= 1e-12 * abs(sr)
+    p = q.gf_avg_plaq(gf)
+    assert abs(p - oracle.gf_avg_plaq(ref, ts)) <= 1e-13
+
+
+@pytest.mark.parametrize("ts", GEOS)
+@pytest.mark.parametrize("step", [0.1, -0.37, 0.9])
+def test_gf_evolve(q, oracle, ts, step):
+    gf, ref = hot_start(q, oracle, ts)
+    gm = q.GaugeMomentum(gf.geo)
+    gm.set_rand(q.RngState("mom"), 1.0)
+    gmr = np.asarray(gm)
+    q.gf_evolve(gf, gm, step)
+    oracle.gf_evolve(ref, np.ascontiguousarray(gmr), ts, step)
+    assert nrel(np.asarray(gf), ref) < 1e-13
+
+
+def test_unitarize(q, oracle):
+    ts = (4, 4, 4, 4)
+    gf, ref = hot_start(q, oracle, ts)
+    rng = np.random.default_rng(3)
+    noisy = ref + 1e-3 * (rng.standard_normal(ref.shape) + 1j * rng.standard_normal(ref.shape))
+    gf.from_numpy(noisy)
+    gf.unitarize()
+    r = np.ascontiguousarray(noisy)
+    oracle.unitarize(r, ts)
+    assert nrel(np.asarray(gf), r) < 1e-14
+
+
+@pytest.mark.parametrize("ts", GEOS)
+@pytest.mark.parametrize("c1", [0.0, -0.331])
+@pytest.mark.parametrize("integ", ["runge-kutta", "euler"])
+def test_flow_step(q, oracle, ts, c1, integ):
+    gf, ref = hot_start(q, oracle, ts)
+    q.gf_wilson_flow_step(gf, 0.05, c1=c1, wilson_flow_integrator_type=integ)
+    oracle.gf_wilson_flow_step(ref, ts, 0.05, c1, integ)
+    assert nrel(np.asarray(gf), ref) < 1e-13
+
+
+@pytest.mark.parametrize("ts", GEOS)
+def test_energy_density_and_topology(q, oracle, ts):
+    gf, ref = hot_start(q, oracle, ts)
+    e = q.gf_energy_density(gf)
+    assert abs(e - oracle.gf_energy_density(ref, ts)) <= 1e-12 * abs(e)
+    ef = q.gf_energy_density_field(gf)
+    assert nrel(np.asarray(ef)[:, 0], oracle.gf_energy_density_field(ref, ts)) < 1e-13
+    qt = q.gf_topology_clf(gf)
+    assert abs(qt - oracle.gf_topology_clf(ref, ts)) <= 1e-12 * max(1.0, abs(qt))
+    tf = q.gf_topology_field_clf(gf)
+    assert nrel(np.asarray(tf)[:, 0], oracle.clf_topology_field(ref, ts)) < 1e-12
+
+
+def test_fp32_storage(q, oracle):
+    ts = (4, 4, 4, 8)
+    gf, ref = hot_start(q, oracle, ts)
+    g32 = gf.copy(precision=q.F32)
+    F = q.GaugeMomentum(gf.geo, precision=q.F32)
+    q.set_gm_force(F, g32, q.GaugeAction(2.13, -0.331))
+    Fr = oracle.new_field(ts)
+    oracle.set_gm_force(Fr, ref, ts, 2.13, -0.331)
+    assert nrel(np.asarray(F), Fr) < 2e-6
+    assert abs(q.gf_avg_plaq(g32) - oracle.gf_avg_plaq(ref, ts)) < 1e-6
+
+
+def test_field_algebra(q):
+    ts = (4, 4, 4, 4)
+    geo = q.Geometry(ts)
+    a = q.GaugeMomentum(geo)
+    a.set_rand(q.RngState("a"), 1.0)
+    b = q.GaugeMomentum(geo)
+    b.set_rand(q.RngState("b"), 1.0)
+    A, B = np.asarray(a), np.asarray(b)
+    c = a.copy()
+    c *= 0.25
+    c += b
+    c -= a
+    assert np.allclose(np.asarray(c), 0.25 * A + B - A, rtol=0, atol=1e-14)
+    assert abs(a.qnorm() - float(np.sum(np.abs(A) ** 2))) < 1e-10 * a.qnorm()
+
+
+def test_errors_are_reported(q):
+    geo = q.Geometry((4, 4, 4, 4))
+    gf = q.GaugeField(geo)
+    gm = q.GaugeMomentum(q.Geometry((4, 4, 4, 8)))
+    with pytest.raises(q.QlatB200Error) as e:
+        q.gf_evolve(gf, gm, 0.1)
+    assert e.value.code == 7
+    with pytest.raises(q.QlatB200Error):
+        q.set_gm_force(gf, gf, q.GaugeAction(1.0, 0.0))
