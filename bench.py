@@ -280,7 +280,7 @@ def our_arm(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for i in range(n_e2e):
-            q._lib.call("qgb_field_upload", gf.handle, q._lib.ctypes.cast(host.data_ptr(), q._lib.c_dbl_p))
+            gf.upload_host(host.data_ptr())
             dh, fl = trajectory(traj + 1 + i, "mixed")
             _ = q.gf_avg_plaq(gf)
         e1.record(stream)

@@ -246,6 +246,11 @@ class Field:
         call("qgb_field_upload", self.handle, a.ctypes.data_as(_lib.c_dbl_p))
         return self
 
+    def upload_host(self, ptr: int) -> None:
+        """Copy from host memory at address `ptr` (e.g. a pinned torch tensor)
+        in the reference memory image."""
+        call("qgb_field_upload", self.handle, ctypes.cast(ctypes.c_void_p(ptr), _lib.c_dbl_p))
+
     def upload_device(self, ptr: int) -> None:
         """Copy from a device buffer (e.g. a torch CUDA tensor's data_ptr) in
         the reference memory image."""
