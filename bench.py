@@ -198,6 +198,7 @@ def our_arm(args):
     gm = q.GaugeMomentum(geo)
 
     def trajectory(traj, precision):
+        nonlocal gf, gf0
         r = rs.split(f"{traj}")
         gf0 @= gf
         gm.set_rand(r.split("set_rand_gauge_momentum"), 1.0)

@@ -414,50 +414,37 @@ QGB_HD Cx<R> cmul(Cx<R> a, Cx<R> b)
   return cx<R>(fma(a.re, b.re, -a.im * b.im), fma(a.re, b.im, a.im * b.re));
 }
 
-// exp(a) for a 3x3 matrix through the Cayley-Hamilton theorem: with
+// The reference's exponential, sum_{n=0}^{20} a^n / n! (the order-20 Taylor
+// polynomial that make_matrix_exp evaluates in Horner form,
+// matrix-hmc.h:155-167), evaluated through the Cayley-Hamilton theorem: with
 // t = tr a, s = (t^2 - tr a^2)/2, d = det a, every power a^n equals
-// x_n 1 + y_n a + z_n a^2 with (x, y, z)_{n+1} = (z_n d, x_n - z_n s, y_n + z_n t).
-// exp(a) = f0 1 + f1 a + f2 a^2 with f = sum_n (x, y, z)_n / n!, summed until
-// the terms fall below the working precision.  For |a| > 1 the argument is
-// halved k times first and the result squared k times.  Cost: ~3 matrix
-// products instead of the 19 of the order-20 Taylor series, and no
-// truncation at order 20; the two agree to rounding for the step sizes of
-// HMC and gradient flow.
+// x_n 1 + y_n a + z_n a^2 with (x, y, z)_{n+1} = (z_n d, x_n - z_n s, y_n + z_n t),
+// so the polynomial is f0 1 + f1 a + f2 a^2 with f = sum_{n<=20} (x, y, z)_n / n!.
+// Cost: one matrix product (a^2) plus a 20-step scalar recursion, instead of
+// the 19 matrix products of the Horner form.  It is the same polynomial, so it
+// keeps the reference's truncation (which matters when |a| reaches ~3, as in
+// gradient flow of rough fields with large steps) and differs from it only by
+// rounding.
 template <typename R>
-QGB_HD M3<R> exp_ch(const M3<R>& a_in)
+QGB_HD M3<R> exp_ch(const M3<R>& a)
 {
-  // Frobenius norm bound for the scaling step
-  R n2 = R(0);
-#pragma unroll
-  for (int i = 0; i < 9; ++i) n2 = fma(a_in.e[i].re, a_in.e[i].re, fma(a_in.e[i].im, a_in.e[i].im, n2));
-  int k = 0;
-  R sc = R(1);
-  while (n2 > R(1) && k < 30) {
-    n2 *= R(0.25);
-    sc *= R(0.5);
-    ++k;
-  }
-  const M3<R> a = (k > 0) ? scale(sc, a_in) : a_in;
   const M3<R> a2 = mul(a, a);
   const Cx<R> t = cx<R>(a.e[0].re + a.e[4].re + a.e[8].re, a.e[0].im + a.e[4].im + a.e[8].im);
   const Cx<R> t2 = cx<R>(a2.e[0].re + a2.e[4].re + a2.e[8].re, a2.e[0].im + a2.e[4].im + a2.e[8].im);
   const Cx<R> tt = cmul(t, t);
   const Cx<R> s = cx<R>(R(0.5) * (tt.re - t2.re), R(0.5) * (tt.im - t2.im));
   // det a by cofactor expansion along row 0
-  const Cx<R> m0 = cx<R>(cmul(a.e[4], a.e[8]).re - cmul(a.e[5], a.e[7]).re,
-                         cmul(a.e[4], a.e[8]).im - cmul(a.e[5], a.e[7]).im);
-  const Cx<R> m1 = cx<R>(cmul(a.e[5], a.e[6]).re - cmul(a.e[3], a.e[8]).re,
-                         cmul(a.e[5], a.e[6]).im - cmul(a.e[3], a.e[8]).im);
-  const Cx<R> m2 = cx<R>(cmul(a.e[3], a.e[7]).re - cmul(a.e[4], a.e[6]).re,
-                         cmul(a.e[3], a.e[7]).im - cmul(a.e[4], a.e[6]).im);
-  const Cx<R> d0 = cmul(a.e[0], m0), d1 = cmul(a.e[1], m1), d2 = cmul(a.e[2], m2);
+  const Cx<R> p48 = cmul(a.e[4], a.e[8]), p57 = cmul(a.e[5], a.e[7]);
+  const Cx<R> p56 = cmul(a.e[5], a.e[6]), p38 = cmul(a.e[3], a.e[8]);
+  const Cx<R> p37 = cmul(a.e[3], a.e[7]), p46 = cmul(a.e[4], a.e[6]);
+  const Cx<R> d0 = cmul(a.e[0], cx<R>(p48.re - p57.re, p48.im - p57.im));
+  const Cx<R> d1 = cmul(a.e[1], cx<R>(p56.re - p38.re, p56.im - p38.im));
+  const Cx<R> d2 = cmul(a.e[2], cx<R>(p37.re - p46.re, p37.im - p46.im));
   const Cx<R> d = cx<R>(d0.re + d1.re + d2.re, d0.im + d1.im + d2.im);
-  // series
   Cx<R> x = cx<R>(R(1), R(0)), y = cx<R>(R(0), R(0)), z = cx<R>(R(0), R(0));
   Cx<R> f0 = x, f1 = y, f2 = z;
-  const int nmax = sizeof(R) == 8 ? 22 : 13;
 #pragma unroll 4
-  for (int n = 1; n <= nmax; ++n) {
+  for (int n = 1; n <= 20; ++n) {
     const R inv = R(1) / R(n);
     const Cx<R> zd = cmul(z, d), zs = cmul(z, s), zt = cmul(z, t);
     const Cx<R> xn = cx<R>(zd.re * inv, zd.im * inv);
@@ -486,7 +473,6 @@ QGB_HD M3<R> exp_ch(const M3<R>& a_in)
   r.e[4].im += f0.im;
   r.e[8].re += f0.re;
   r.e[8].im += f0.im;
-  for (int i = 0; i < k; ++i) r = mul(r, r);
   return r;
 }
 
