@@ -182,6 +182,25 @@ int qgb_prof_reset(void);
 /* name: "force", "force_update", "force_evolve", "evolve", "reduce", "rng",
  * "unitarize", "convert", "clover", "flow_stage"; totals since the last reset. */
 int qgb_prof_get(const char* name, double* total_ms, int64_t* launches);
+/* ---- force-kernel autotuner (no counterpart in the reference) ---------- */
+
+/* The force kernels (set_gm_force and its fused HMC / flow consumers) exist
+ * in several launch shapes: threads per block, a register cap through the
+ * minimum resident blocks per SM, one or two threads per link, and packed
+ * FP32 FMAs.  The shape is chosen per (precision, rect): by hand, or by timing
+ * them all on a given gauge field. */
+int qgb_force_variant_count(int32_t* n);
+int qgb_force_variant_info(int32_t variant, int32_t* block_size, int32_t* min_blocks, int32_t* threads_per_link,
+                           int32_t* packed_fp32);
+int qgb_force_set_variant(int32_t precision, int32_t rect, int32_t variant);
+int qgb_force_get_variant(int32_t precision, int32_t rect, int32_t* variant);
+/* Time every variant (force + momentum update, `reps` launches each) on gf
+ * with action coefficient c1, select the fastest for gf's precision and
+ * (c1 != 0); returns it and its time per launch. */
+int qgb_autotune_force(const qgb_field* gf, double c1, int32_t reps, int32_t* best, double* best_ms);
+/* Time one variant without selecting it. */
+int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int32_t reps, double* ms_per_launch);
+
 /* Number of kernels this library has launched since it was loaded. */
 int qgb_launch_count(int64_t* out);
 /* Number of Gaussian draws whose logarithm could not be proven correctly

@@ -71,6 +71,46 @@ def set_device(device: int):
     call("qgb_set_device", int(device))
 
 
+def force_variants():
+    """The force-kernel launch shapes: list of dicts (block_size, min_blocks,
+    threads_per_link, packed_fp32)."""
+    import ctypes
+    from ._lib import call
+    n = ctypes.c_int32()
+    call("qgb_force_variant_count", ctypes.byref(n))
+    out = []
+    for v in range(n.value):
+        a = [ctypes.c_int32() for _ in range(4)]
+        call("qgb_force_variant_info", v, *[ctypes.byref(x) for x in a])
+        out.append(dict(block_size=a[0].value, min_blocks=a[1].value, threads_per_link=a[2].value,
+                        packed_fp32=a[3].value))
+    return out
+
+
+def force_set_variant(precision: int, rect: bool, variant: int):
+    from ._lib import call
+    call("qgb_force_set_variant", int(precision), int(bool(rect)), int(variant))
+
+
+def autotune_force(gf, c1: float, reps: int = 3):
+    """Time every force-kernel variant on gf (its precision) and keep the
+    fastest for (precision, c1 != 0).  Returns (variant, ms per launch)."""
+    import ctypes
+    from ._lib import call
+    b = ctypes.c_int32()
+    t = ctypes.c_double()
+    call("qgb_autotune_force", gf.handle, float(c1), int(reps), ctypes.byref(b), ctypes.byref(t))
+    return b.value, t.value
+
+
+def force_time_variant(gf, c1: float, variant: int, reps: int = 3) -> float:
+    import ctypes
+    from ._lib import call
+    t = ctypes.c_double()
+    call("qgb_force_time_variant", gf.handle, float(c1), int(variant), int(reps), ctypes.byref(t))
+    return t.value
+
+
 def synchronize():
     from ._lib import call
     call("qgb_synchronize")

@@ -83,6 +83,8 @@ struct Ctx {
 
 Ctx g_ctx;
 int64_t g_launches = 0;  // kernels launched by this library
+// force-kernel launch variant per [precision: 0 = FP64, 1 = FP32][rect]
+int g_force_variant[2][2] = {{0, 0}, {0, 0}};
 
 int ensure_ctx()
 {
@@ -294,8 +296,9 @@ template <typename R>
 int force(const Geo& g, qgb::ForceMode mode, const ForceArgs& a)
 {
   static const char* names[] = {"force", "force_update", "force_evolve", "flow_stage"};
+  const int v = g_force_variant[sizeof(R) == 8 ? 0 : 1][a.c1 != 0.0 ? 1 : 0];
   Prof p(names[mode]);
-  QGB_TRY_CUDA(qgb::launch_force<R>(g, mode, a, g_ctx.stream));
+  QGB_TRY_CUDA(qgb::launch_force<R>(g, mode, a, v, g_ctx.stream));
   return QGB_OK;
 }
 
@@ -1029,6 +1032,116 @@ int qgb_prof_get(const char* name, double* total_ms, int64_t* launches)
   auto it = g_ctx.prof.find(name);
   *total_ms = it == g_ctx.prof.end() ? 0.0 : it->second.total_ms;
   *launches = it == g_ctx.prof.end() ? 0 : it->second.launches;
+  return QGB_OK;
+}
+
+int qgb_force_variant_count(int32_t* n)
+{
+  QGB_CHECK(n, QGB_ERR_INVALID_ARG, "qgb_force_variant_count: null output");
+  *n = qgb::force_variant_count();
+  return QGB_OK;
+}
+
+int qgb_force_variant_info(int32_t variant, int32_t* block_size, int32_t* min_blocks, int32_t* threads_per_link,
+                           int32_t* packed_fp32)
+{
+  int bs, mb, sp, pk;
+  QGB_CHECK(qgb::force_variant_info_c(variant, &bs, &mb, &sp, &pk), QGB_ERR_INVALID_ARG,
+            "qgb_force_variant_info: no such variant");
+  if (block_size) *block_size = bs;
+  if (min_blocks) *min_blocks = mb;
+  if (threads_per_link) *threads_per_link = sp;
+  if (packed_fp32) *packed_fp32 = pk;
+  return QGB_OK;
+}
+
+int qgb_force_set_variant(int32_t precision, int32_t rect, int32_t variant)
+{
+  std::lock_guard<std::recursive_mutex> lock(g_mu);
+  QGB_CHECK(precision == QGB_F64 || precision == QGB_F32, QGB_ERR_INVALID_ARG, "qgb_force_set_variant: precision");
+  QGB_CHECK(variant >= 0 && variant < qgb::force_variant_count(), QGB_ERR_INVALID_ARG,
+            "qgb_force_set_variant: no such variant");
+  g_force_variant[precision == QGB_F64 ? 0 : 1][rect ? 1 : 0] = variant;
+  return QGB_OK;
+}
+
+int qgb_force_get_variant(int32_t precision, int32_t rect, int32_t* variant)
+{
+  QGB_CHECK(variant && (precision == QGB_F64 || precision == QGB_F32), QGB_ERR_INVALID_ARG,
+            "qgb_force_get_variant: bad argument");
+  *variant = g_force_variant[precision == QGB_F64 ? 0 : 1][rect ? 1 : 0];
+  return QGB_OK;
+}
+
+int qgb_autotune_force(const qgb_field* gf, double c1, int32_t reps, int32_t* best, double* best_ms)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_autotune_force"));
+  QGB_CHECK(gf->mult == 4 && reps >= 1, QGB_ERR_INVALID_ARG, "qgb_autotune_force: bad argument");
+  const Geo g = geo_of(gf);
+  void* P = nullptr;
+  QGB_RC(get_scratch(gf->bytes, 31, &P));
+  QGB_TRY_CUDA(cudaMemsetAsync(P, 0, gf->bytes, g_ctx.stream));
+  cudaEvent_t e0 = get_event(), e1 = get_event();
+  int best_v = 0;
+  float best_t = 1e30f;
+  const int nv = qgb::force_variant_count();
+  for (int v = 0; v < nv; ++v) {
+    ForceArgs a = fargs(gf->d, P, 3.0, c1, 1e-3);
+    auto launch = [&]() {
+      return gf->prec == QGB_F64 ? qgb::launch_force<double>(g, qgb::FORCE_UPDATE, a, v, g_ctx.stream)
+                                 : qgb::launch_force<float>(g, qgb::FORCE_UPDATE, a, v, g_ctx.stream);
+    };
+    QGB_TRY_CUDA(launch());
+    QGB_TRY_CUDA(cudaEventRecord(e0, g_ctx.stream));
+    for (int r = 0; r < reps; ++r) QGB_TRY_CUDA(launch());
+    QGB_TRY_CUDA(cudaEventRecord(e1, g_ctx.stream));
+    QGB_TRY_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= reps;
+    g_launches += reps + 1;
+    if (ms < best_t) {
+      best_t = ms;
+      best_v = v;
+    }
+  }
+  g_ctx.event_pool.push_back(e0);
+  g_ctx.event_pool.push_back(e1);
+  g_force_variant[gf->prec == QGB_F64 ? 0 : 1][c1 != 0.0 ? 1 : 0] = best_v;
+  if (best) *best = best_v;
+  if (best_ms) *best_ms = best_t;
+  return QGB_OK;
+}
+
+int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int32_t reps, double* ms_per_launch)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_force_time_variant"));
+  QGB_CHECK(gf->mult == 4 && reps >= 1 && ms_per_launch, QGB_ERR_INVALID_ARG, "qgb_force_time_variant: bad argument");
+  QGB_CHECK(variant >= 0 && variant < qgb::force_variant_count(), QGB_ERR_INVALID_ARG,
+            "qgb_force_time_variant: no such variant");
+  const Geo g = geo_of(gf);
+  void* P = nullptr;
+  QGB_RC(get_scratch(gf->bytes, 31, &P));
+  QGB_TRY_CUDA(cudaMemsetAsync(P, 0, gf->bytes, g_ctx.stream));
+  cudaEvent_t e0 = get_event(), e1 = get_event();
+  ForceArgs a = fargs(gf->d, P, 3.0, c1, 1e-3);
+  auto launch = [&]() {
+    return gf->prec == QGB_F64 ? qgb::launch_force<double>(g, qgb::FORCE_UPDATE, a, variant, g_ctx.stream)
+                               : qgb::launch_force<float>(g, qgb::FORCE_UPDATE, a, variant, g_ctx.stream);
+  };
+  QGB_TRY_CUDA(launch());
+  QGB_TRY_CUDA(cudaEventRecord(e0, g_ctx.stream));
+  for (int r = 0; r < reps; ++r) QGB_TRY_CUDA(launch());
+  QGB_TRY_CUDA(cudaEventRecord(e1, g_ctx.stream));
+  QGB_TRY_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  g_ctx.event_pool.push_back(e0);
+  g_ctx.event_pool.push_back(e1);
+  g_launches += reps + 1;
+  *ms_per_launch = ms / reps;
   return QGB_OK;
 }
 

@@ -3,5 +3,5 @@
 
 namespace qgb
 {
-template cudaError_t launch_force<float>(const Geo&, ForceMode, const ForceArgs&, cudaStream_t);
+template cudaError_t launch_force<float>(const Geo&, ForceMode, const ForceArgs&, int, cudaStream_t);
 }  // namespace qgb

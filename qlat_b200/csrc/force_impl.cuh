@@ -31,69 +31,71 @@ namespace qgb
 // at most five 3x3 matrices are live (accumulator, B or T, chain product,
 // loaded link, product being formed): ~180 registers in FP64, ~90 in FP32.
 
-// hop(y) for the signed direction: sgn = +1: U_nu(y); sgn = -1: U_nu(y - nu)^+.
-// `where` is the site of the stored link (y or y - nu); the caller picks
-// mul / adj_mul / mul_adj accordingly.
+// Positions are x + a mu + b e with e = s nu (s = +1 or -1).  The link from
+// such a point along +e ("hop") is U_nu(y) for s = +1 and U_nu(y - nu)^+ for
+// s = -1; the link along -e ("back") is U_nu(y - nu)^+ for s = +1 and U_nu(y)
+// for s = -1.  Both signs therefore run the same code: only the stored site
+// and a warp-uniform conjugate-transpose differ, which keeps the loop body
+// small enough for the instruction cache.
 
-template <typename R, bool RECT>
-__device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g, const Coord& x, int mu, R cp, R cr)
+template <typename R>
+struct SignedDir {
+  const CField<R>& U;
+  const Geo& g;
+  const Coord& x;
+  int mu, nu, s;
+  __device__ __forceinline__ M3<R> umu(int a, int b) const { return U.ld(site_rt(g, x, mu, a, nu, b * s), mu); }
+  __device__ __forceinline__ M3<R> hop(int a, int b) const
+  {
+    M3<R> m = U.ld(site_rt(g, x, mu, a, nu, b * s + (s < 0 ? -1 : 0)), nu);
+    return s < 0 ? adj(m) : m;
+  }
+  __device__ __forceinline__ M3<R> back(int a, int b) const
+  {
+    M3<R> m = U.ld(site_rt(g, x, mu, a, nu, b * s + (s < 0 ? 0 : -1)), nu);
+    return s < 0 ? m : adj(m);
+  }
+};
+
+template <typename R, bool RECT, bool PACKED>
+__device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g, const Coord& x, int mu, R cp, R cr,
+                                               int k0, int k1)
 {
+  using O = Ops<R, PACKED>;
   M3<R> S = m3_zero<R>();
 #pragma unroll 1
-  for (int k = 0; k < 6; ++k) {
-    const int nu = (mu + 1 + (k >> 1)) & 3;  // the three directions != mu
-    const int s = (k & 1) ? -1 : 1;          // sign of e
-    // B = A U_mu(x+e)
-    M3<R> B;
-    if (s > 0) B = mul(U.ld(site_rt(g, x, mu, 0, nu, 0), nu), U.ld(site_rt(g, x, mu, 0, nu, 1), mu));
-    else B = adj_mul(U.ld(site_rt(g, x, mu, 0, nu, -1), nu), U.ld(site_rt(g, x, mu, 0, nu, -1), mu));
+  for (int k = k0; k < k1; ++k) {
+    const SignedDir<R> d{U, g, x, mu, (mu + 1 + (k >> 1)) & 3, (k & 1) ? -1 : 1};
+    // B = hop(x) U_mu(x+e)
+    const M3<R> B = O::mul(d.hop(0, 0), d.umu(0, 1));
     if (!RECT) {
-      // S += B Hb
-      if (s > 0) S = add_mul_adj(S, B, U.ld(site_rt(g, x, mu, 1, nu, 0), nu));
-      else S = add_mul(S, B, U.ld(site_rt(g, x, mu, 1, nu, -1), nu));
+      S = O::add_mul(S, B, d.back(1, 1));
       continue;
     }
-    // rect2: S += c1 B U_mu(x+e+mu) hop_back(x+e+2mu) U_mu(x+mu)^+
+    // rect2: S += c1 B U_mu(x+e+mu) back(x+e+2mu) U_mu(x+mu)^+
     {
-      M3<R> C = mul(B, U.ld(site_rt(g, x, mu, 1, nu, s), mu));
-      if (s > 0) C = mul_adj(C, U.ld(site_rt(g, x, mu, 2, nu, 0), nu));
-      else C = mul(C, U.ld(site_rt(g, x, mu, 2, nu, -1), nu));
-      C = mul_adj(C, U.ld(site_rt(g, x, mu, 1, nu, 0), mu));
+      M3<R> C = O::mul(B, d.umu(1, 1));
+      C = O::mul(C, d.back(2, 1));
+      C = O::mul_adj(C, d.umu(1, 0));
       axpy(S, cr, C);
     }
     M3<R> T = scale(cp, B);
-    // rect1: C1 = A hop(x+e) U_mu(x+2e) hop_back(x+2e+mu)
+    // rect1: C1 = hop(x) hop(x+e) U_mu(x+2e) back(x+2e+mu)
     {
-      M3<R> C;
-      if (s > 0) {
-        C = mul(U.ld(site_rt(g, x, mu, 0, nu, 0), nu), U.ld(site_rt(g, x, mu, 0, nu, 1), nu));
-        C = mul(C, U.ld(site_rt(g, x, mu, 0, nu, 2), mu));
-        C = mul_adj(C, U.ld(site_rt(g, x, mu, 1, nu, 1), nu));
-      } else {
-        // A hop(x-nu) = [U_nu(x-2nu) U_nu(x-nu)]^+
-        C = mul(U.ld(site_rt(g, x, mu, 0, nu, -2), nu), U.ld(site_rt(g, x, mu, 0, nu, -1), nu));
-        C = adj_mul(C, U.ld(site_rt(g, x, mu, 0, nu, -2), mu));
-        C = mul(C, U.ld(site_rt(g, x, mu, 1, nu, -2), nu));
-      }
+      M3<R> C = O::mul(d.hop(0, 0), d.hop(0, 1));
+      C = O::mul(C, d.umu(0, 2));
+      C = O::mul(C, d.back(1, 2));
       axpy(T, cr, C);
     }
     // rect3: C3 = U_mu(x-mu)^+ hop(x-mu) U_mu(x-mu+e) U_mu(x+e)
     {
-      M3<R> C;
-      if (s > 0) {
-        C = adj_mul(U.ld(site_rt(g, x, mu, -1, nu, 0), mu), U.ld(site_rt(g, x, mu, -1, nu, 0), nu));
-      } else {
-        // U_mu(x-mu)^+ U_nu(x-mu-nu)^+ = [U_nu(x-mu-nu) U_mu(x-mu)]^+
-        C = mul(U.ld(site_rt(g, x, mu, -1, nu, -1), nu), U.ld(site_rt(g, x, mu, -1, nu, 0), mu));
-        C = adj(C);
-      }
-      C = mul(C, U.ld(site_rt(g, x, mu, -1, nu, s), mu));
-      C = mul(C, U.ld(site_rt(g, x, mu, 0, nu, s), mu));
+      M3<R> C = O::adj_mul(d.umu(-1, 0), d.hop(-1, 0));
+      C = O::mul(C, d.umu(-1, 1));
+      C = O::mul(C, d.umu(0, 1));
       axpy(T, cr, C);
     }
-    // S += T Hb
-    if (s > 0) S = add_mul_adj(S, T, U.ld(site_rt(g, x, mu, 1, nu, 0), nu));
-    else S = add_mul(S, T, U.ld(site_rt(g, x, mu, 1, nu, -1), nu));
+    // S += T back(x+e+mu)
+    S = O::add_mul(S, T, d.back(1, 1));
   }
   if (!RECT) S = scale(cp, S);
   return S;
@@ -102,16 +104,48 @@ __device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g,
 // ------------------------------------------------------------------------
 // force: F = TA(-beta/3 U_mu(x) S^+) (hmc.cpp:64-75) and its fused consumers
 
-template <typename R, int MODE, bool RECT>
-__global__ void __launch_bounds__(128) k_force(Geo g, ForceArgs a)
+// Launch variants for the autotuner: threads per block, minimum resident
+// blocks per SM (caps registers), threads per link (SPLIT = 2 gives each link
+// to a lane pair, each doing 3 of the 6 signed directions, combined by a
+// shuffle), and packed FP32 FMAs.
+struct ForceVariant {
+  int bs, minb, split, packed;
+};
+#define QGB_FORCE_VARIANTS(X) \
+  X(0, 128, 1, 1, 0)          \
+  X(1, 128, 2, 1, 0)          \
+  X(2, 256, 1, 1, 0)          \
+  X(3, 64, 1, 1, 0)           \
+  X(4, 128, 1, 2, 0)          \
+  X(5, 128, 2, 2, 0)          \
+  X(6, 128, 1, 1, 1)          \
+  X(7, 128, 2, 1, 1)          \
+  X(8, 128, 1, 2, 1)          \
+  X(9, 64, 1, 2, 1)
+static const int N_FORCE_VARIANTS = 10;
+
+template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, bool PACKED>
+__global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 {
-  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= g.V) return;
+  const long t = (long)blockIdx.x * BS + threadIdx.x;
+  const long s0 = t / SPLIT;
+  const int h = (int)(t % SPLIT);
+  if (SPLIT == 1 && s0 >= g.V) return;
+  const bool valid = s0 < g.V;  // lane pairs stay together for the shuffle
+  const long s = valid ? s0 : g.V - 1;
   const int mu = blockIdx.y;
   const CField<R> U{(const Cx<R>*)a.U, g.V};
   const Coord x = coord_of(g, s);
   const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
-  const M3<R> S = staple_sum_rt<R, RECT>(U, g, x, mu, cp, cr);
+  M3<R> S = staple_sum_rt<R, RECT, PACKED>(U, g, x, mu, cp, cr, h * (6 / SPLIT), (h + 1) * (6 / SPLIT));
+  if (SPLIT == 2) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      S.e[i].re += __shfl_xor_sync(0xffffffffu, S.e[i].re, 1);
+      S.e[i].im += __shfl_xor_sync(0xffffffffu, S.e[i].im, 1);
+    }
+    if (!valid || h != 0) return;
+  }
   const M3<R> u = U.ld(s, mu);
   M3<R> F = traceless_antiherm(mul_adj(u, S));
   F = scale(R(-a.beta / 3.0), F);
@@ -135,15 +169,14 @@ __global__ void __launch_bounds__(128) k_force(Geo g, ForceArgs a)
   }
 }
 
-template <typename R>
-cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st)
+template <typename R, int BS, int MINB, int SPLIT, bool PACKED>
+cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
-  const int bs = 128;
-  dim3 grid((unsigned)((g.V + bs - 1) / bs), 4);
+  dim3 grid((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
   const bool rect = a.c1 != 0.0;
-#define QGB_LAUNCH(M)                                       \
-  if (rect) k_force<R, M, true><<<grid, bs, 0, st>>>(g, a); \
-  else k_force<R, M, false><<<grid, bs, 0, st>>>(g, a);
+#define QGB_LAUNCH(M)                                                               \
+  if (rect) k_force<R, M, true, BS, MINB, SPLIT, PACKED><<<grid, BS, 0, st>>>(g, a); \
+  else k_force<R, M, false, BS, MINB, SPLIT, PACKED><<<grid, BS, 0, st>>>(g, a);
   switch (mode) {
     case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
     case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;
@@ -152,6 +185,29 @@ cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, cudaS
   }
 #undef QGB_LAUNCH
   return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, int variant, cudaStream_t st)
+{
+  switch (variant) {
+#define QGB_V(ID, BS, MINB, SPLIT, PACKED) \
+  case ID: return launch_force_v<R, BS, MINB, SPLIT, (PACKED != 0)>(g, mode, a, st);
+    QGB_FORCE_VARIANTS(QGB_V)
+#undef QGB_V
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* packed)
+{
+  switch (variant) {
+#define QGB_V(ID, BS, MINB, SPLIT, PACKED) \
+  case ID: *bs = BS; *minb = MINB; *split = SPLIT; *packed = PACKED; return 1;
+    QGB_FORCE_VARIANTS(QGB_V)
+#undef QGB_V
+    default: return 0;
+  }
 }
 
 }  // namespace qgb

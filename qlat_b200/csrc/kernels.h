@@ -33,8 +33,11 @@ struct ForceArgs {
 
 void init_constants();  // SHA-256 and log tables into constant memory (per device)
 
+// `variant` indexes the autotuner's table of launch shapes (force_impl.cuh).
 template <typename R>
-cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st);
+cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, int variant, cudaStream_t st);
+int force_variant_count();
+int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed);
 
 // U = exp(eps P) U (optionally unitarized; exp by Cayley-Hamilton series or the
 // reference's order-20 Taylor series).

@@ -175,3 +175,27 @@ def test_errors_are_reported(q):
     assert e.value.code == 7
     with pytest.raises(q.QlatB200Error):
         q.set_gm_force(gf, gf, q.GaugeAction(1.0, 0.0))
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_every_force_variant(q, oracle, prec):
+    """All launch shapes of the autotuner compute the same force."""
+    ts = (3, 4, 5, 6)
+    gf, ref = hot_start(q, oracle, ts)
+    g = gf if prec == "f64" else gf.copy(precision=q.F32)
+    tol = 1e-13 if prec == "f64" else 2e-6
+    Fr = {}
+    for c1 in (0.0, -0.331):
+        Fr[c1] = oracle.new_field(ts)
+        oracle.set_gm_force(Fr[c1], ref, ts, 2.0, c1)
+    P = q.F64 if prec == "f64" else q.F32
+    try:
+        for v in range(len(q.force_variants())):
+            for c1 in (0.0, -0.331):
+                q.force_set_variant(P, c1 != 0.0, v)
+                F = q.GaugeMomentum(gf.geo, precision=P)
+                q.set_gm_force(F, g, q.GaugeAction(2.0, c1))
+                assert nrel(np.asarray(F), Fr[c1]) < tol, (v, c1)
+    finally:
+        q.force_set_variant(P, False, 0)
+        q.force_set_variant(P, True, 0)
