@@ -1043,15 +1043,16 @@ int qgb_force_variant_count(int32_t* n)
 }
 
 int qgb_force_variant_info(int32_t variant, int32_t* block_size, int32_t* min_blocks, int32_t* threads_per_link,
-                           int32_t* packed_fp32)
+                           int32_t* packed_fp32, int32_t* site_map)
 {
-  int bs, mb, sp, pk;
-  QGB_CHECK(qgb::force_variant_info_c(variant, &bs, &mb, &sp, &pk), QGB_ERR_INVALID_ARG,
+  int bs, mb, sp, pk, mp;
+  QGB_CHECK(qgb::force_variant_info_c(variant, &bs, &mb, &sp, &pk, &mp), QGB_ERR_INVALID_ARG,
             "qgb_force_variant_info: no such variant");
   if (block_size) *block_size = bs;
   if (min_blocks) *min_blocks = mb;
   if (threads_per_link) *threads_per_link = sp;
   if (packed_fp32) *packed_fp32 = pk;
+  if (site_map) *site_map = mp;
   return QGB_OK;
 }
 

@@ -107,33 +107,69 @@ __device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g,
 // Launch variants for the autotuner: threads per block, minimum resident
 // blocks per SM (caps registers), threads per link (SPLIT = 2 gives each link
 // to a lane pair, each doing 3 of the 6 signed directions, combined by a
-// shuffle), and packed FP32 FMAs.
+// shuffle), packed FP32 FMAs, and the site mapping: MAP 0 runs blocks of
+// consecutive sites with mu = blockIdx.y; MAP 1 gives each block the four
+// links of a compact tile of BS/4 sites (4 x 2 x 2 x 2 for 128 threads,
+// 4 x 4 x 2 x 2 for 256), one warp-group per mu, so the four directions share
+// the tile's neighbourhood in L1.  MAP 1 needs the lattice extents to be
+// multiples of the tile; otherwise the launcher uses MAP 0.
 struct ForceVariant {
-  int bs, minb, split, packed;
+  int bs, minb, split, packed, map;
 };
 #define QGB_FORCE_VARIANTS(X) \
-  X(0, 128, 1, 1, 0)          \
-  X(1, 128, 2, 1, 0)          \
-  X(2, 256, 1, 1, 0)          \
-  X(3, 64, 1, 1, 0)           \
-  X(4, 128, 1, 2, 0)          \
-  X(5, 128, 2, 2, 0)          \
-  X(6, 128, 1, 1, 1)          \
-  X(7, 128, 2, 1, 1)          \
-  X(8, 128, 1, 2, 1)          \
-  X(9, 64, 1, 2, 1)
-static const int N_FORCE_VARIANTS = 10;
+  X(0, 128, 1, 1, 0, 0)       \
+  X(1, 256, 1, 1, 0, 0)       \
+  X(2, 128, 3, 1, 0, 0)       \
+  X(3, 128, 4, 1, 0, 0)       \
+  X(4, 128, 5, 1, 0, 0)       \
+  X(5, 128, 1, 2, 0, 0)       \
+  X(6, 128, 1, 1, 1, 0)       \
+  X(7, 128, 1, 1, 0, 1)       \
+  X(8, 128, 3, 1, 0, 1)       \
+  X(9, 128, 4, 1, 0, 1)       \
+  X(10, 256, 1, 1, 0, 1)      \
+  X(11, 256, 2, 1, 0, 1)
+static const int N_FORCE_VARIANTS = 12;
 
-template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, bool PACKED>
+template <int BS>
+struct Tile {
+  static const int tx = 4, ty = BS >= 256 ? 4 : 2, tz = 2, tt = BS >= 256 ? 2 : (BS >= 128 ? 2 : 1);
+  static const int sites = tx * ty * tz * tt;
+};
+
+template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, bool PACKED, int MAP>
 __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 {
-  const long t = (long)blockIdx.x * BS + threadIdx.x;
-  const long s0 = t / SPLIT;
-  const int h = (int)(t % SPLIT);
+  long s0;
+  int h, mu;
+  if (MAP == 0) {
+    const long t = (long)blockIdx.x * BS + threadIdx.x;
+    s0 = t / SPLIT;
+    h = (int)(t % SPLIT);
+    mu = blockIdx.y;
+  } else {
+    // tile of Tile<BS>::sites sites; thread = mu * sites + site-in-tile
+    using TL = Tile<BS>;
+    const int in = threadIdx.x % TL::sites;
+    mu = threadIdx.x / TL::sites;
+    h = 0;
+    long b = blockIdx.x;
+    const int nx = g.d[0] / TL::tx, ny = g.d[1] / TL::ty, nz = g.d[2] / TL::tz;
+    const int bx = (int)(b % nx);
+    b /= nx;
+    const int by = (int)(b % ny);
+    b /= ny;
+    const int bz = (int)(b % nz);
+    const int bt = (int)(b / nz);
+    const int x0 = bx * TL::tx + in % TL::tx;
+    const int x1 = by * TL::ty + (in / TL::tx) % TL::ty;
+    const int x2 = bz * TL::tz + (in / (TL::tx * TL::ty)) % TL::tz;
+    const int x3 = bt * TL::tt + in / (TL::tx * TL::ty * TL::tz);
+    s0 = (long)x0 + (long)g.d[0] * ((long)x1 + (long)g.d[1] * ((long)x2 + (long)g.d[2] * (long)x3));
+  }
   if (SPLIT == 1 && s0 >= g.V) return;
   const bool valid = s0 < g.V;  // lane pairs stay together for the shuffle
   const long s = valid ? s0 : g.V - 1;
-  const int mu = blockIdx.y;
   const CField<R> U{(const Cx<R>*)a.U, g.V};
   const Coord x = coord_of(g, s);
   const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
@@ -169,14 +205,18 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
   }
 }
 
-template <typename R, int BS, int MINB, int SPLIT, bool PACKED>
+template <typename R, int BS, int MINB, int SPLIT, bool PACKED, int MAP>
 cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
-  dim3 grid((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
+  using TL = Tile<BS>;
+  const bool tiled = MAP == 1 && SPLIT == 1 && g.d[0] % TL::tx == 0 && g.d[1] % TL::ty == 0 &&
+                     g.d[2] % TL::tz == 0 && g.d[3] % TL::tt == 0;
+  if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
+  dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
   const bool rect = a.c1 != 0.0;
-#define QGB_LAUNCH(M)                                                               \
-  if (rect) k_force<R, M, true, BS, MINB, SPLIT, PACKED><<<grid, BS, 0, st>>>(g, a); \
-  else k_force<R, M, false, BS, MINB, SPLIT, PACKED><<<grid, BS, 0, st>>>(g, a);
+#define QGB_LAUNCH(M)                                                                                  \
+  if (rect) k_force<R, M, true, BS, MINB, SPLIT, PACKED, (MAP == 1 ? 1 : 0)><<<grid, BS, 0, st>>>(g, a); \
+  else k_force<R, M, false, BS, MINB, SPLIT, PACKED, (MAP == 1 ? 1 : 0)><<<grid, BS, 0, st>>>(g, a);
   switch (mode) {
     case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
     case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;
@@ -191,19 +231,19 @@ template <typename R>
 cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, int variant, cudaStream_t st)
 {
   switch (variant) {
-#define QGB_V(ID, BS, MINB, SPLIT, PACKED) \
-  case ID: return launch_force_v<R, BS, MINB, SPLIT, (PACKED != 0)>(g, mode, a, st);
+#define QGB_V(ID, BS, MINB, SPLIT, PACKED, MAP) \
+  case ID: return launch_force_v<R, BS, MINB, SPLIT, (PACKED != 0), MAP>(g, mode, a, st);
     QGB_FORCE_VARIANTS(QGB_V)
 #undef QGB_V
     default: return cudaErrorInvalidValue;
   }
 }
 
-inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* packed)
+inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* packed, int* map)
 {
   switch (variant) {
-#define QGB_V(ID, BS, MINB, SPLIT, PACKED) \
-  case ID: *bs = BS; *minb = MINB; *split = SPLIT; *packed = PACKED; return 1;
+#define QGB_V(ID, BS, MINB, SPLIT, PACKED, MAP) \
+  case ID: *bs = BS; *minb = MINB; *split = SPLIT; *packed = PACKED; *map = MAP; return 1;
     QGB_FORCE_VARIANTS(QGB_V)
 #undef QGB_V
     default: return 0;

@@ -4,8 +4,8 @@
 namespace qgb
 {
 int force_variant_count() { return N_FORCE_VARIANTS; }
-int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed)
+int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed, int* map)
 {
-  return force_variant_info(variant, bs, minb, split, packed);
+  return force_variant_info(variant, bs, minb, split, packed, map);
 }
 }  // namespace qgb

@@ -37,7 +37,7 @@ void init_constants();  // SHA-256 and log tables into constant memory (per devi
 template <typename R>
 cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, int variant, cudaStream_t st);
 int force_variant_count();
-int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed);
+int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed, int* map);
 
 // U = exp(eps P) U (optionally unitarized; exp by Cayley-Hamilton series or the
 // reference's order-20 Taylor series).
