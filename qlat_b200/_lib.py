@@ -78,6 +78,7 @@ SIGNATURES = {
     "qgb_force_get_variant": [ctypes.c_int32, ctypes.c_int32, c_i32_p],
     "qgb_autotune_force": [c_field, ctypes.c_double, ctypes.c_int32, c_i32_p, c_dbl_p],
     "qgb_force_time_variant": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+    "qgb_gf_action_sums_noalloc": [ctypes.c_void_p, i32x4, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p],
     "qgb_launch_count": [c_i64_p],
     "qgb_rng_ambiguous_count": [c_i64_p],
 }

@@ -383,6 +383,12 @@ int hamiltonian_slots(const qgb_field* gm, const qgb_field* gf, double c1, int s
 
 }  // namespace
 
+namespace qgb
+{
+// Lets the allocation-free entry point (noalloc.cu) report through qgb_last_error.
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace qgb
+
 // ========================================================================
 // C ABI
 
