@@ -54,6 +54,7 @@ extern "C" {
 #define QGB_INTEGRATOR_LEAPFROG 1
 
 typedef struct qgb_field_s qgb_field;
+typedef struct qgb_batch_s qgb_batch;
 
 /* ---- library state ---------------------------------------------------- */
 
@@ -182,6 +183,38 @@ int qgb_prof_reset(void);
 /* name: "force", "force_update", "force_evolve", "evolve", "reduce", "rng",
  * "unitarize", "convert", "clover", "flow_stage"; totals since the last reset. */
 int qgb_prof_get(const char* name, double* total_ms, int64_t* launches);
+/* ---- batches of independent chains (no counterpart in the reference) ---- */
+
+/* Many independent pure-gauge HMC chains of different lattice sizes, betas and
+ * c1 advanced together: every phase of a trajectory is one launch over all
+ * chains, and the trajectory is recorded once as a CUDA graph per
+ * (n_step, md_time, integrator, precision) and replayed.  Chain c has lattice
+ * total_sites[4c .. 4c+3], beta[c], c1[c]; RngStates are 24 x uint32 per chain,
+ * concatenated.  Each chain follows run_hmc_evolve_pure_gauge (hmc.pyx:169-188)
+ * with the per-site RngState(rs_c, gindex) momenta of set_rand_gauge_momentum
+ * (hmc.cpp:107-119); accept/reject is the caller's (qgb_batch_accept). */
+int qgb_batch_create(qgb_batch** out, int32_t n_chains, const int32_t* total_sites, const double* beta,
+                     const double* c1);
+int qgb_batch_destroy(qgb_batch* b);
+int qgb_batch_info(const qgb_batch* b, int32_t* n_chains, int64_t* total_site_count);
+/* Hot start of every chain: GaugeField.set_rand(rs_c, sigma, n_step) (qcd-utils.cpp:71-92). */
+int qgb_batch_set_rand(qgb_batch* b, const uint32_t* rs, double sigma, int32_t n_step);
+/* One trajectory of every chain from its current state: momenta from rs_momentum
+ * (sigma 1), molecular dynamics in FP64 (mixed = 0) or FP32 (mixed = 1, FP64
+ * re-unitarisation every reunit_interval steps), FP64 Hamiltonians; writes the
+ * n_chains values of delta_h and keeps the proposals until qgb_batch_accept.
+ * use_graph != 0 records / replays the trajectory as a CUDA graph. */
+int qgb_batch_trajectory(qgb_batch* b, const uint32_t* rs_momentum, int32_t n_step, double md_time,
+                         int32_t integrator, int32_t mixed, int32_t reunit_interval, int32_t use_graph,
+                         double* delta_h);
+/* Replace the state of every chain whose flag is non-zero by its proposal. */
+int qgb_batch_accept(qgb_batch* b, const int32_t* flags);
+/* gf_avg_plaq of every chain. */
+int qgb_batch_plaq(qgb_batch* b, double* plaq);
+/* One chain's links in the reference memory image. */
+int qgb_batch_download_chain(qgb_batch* b, int32_t chain, double* host);
+int qgb_batch_upload_chain(qgb_batch* b, int32_t chain, const double* host);
+
 /* ---- force-kernel autotuner (no counterpart in the reference) ---------- */
 
 /* The force kernels (set_gm_force and its fused HMC / flow consumers) exist

@@ -16,6 +16,7 @@ from .hmc import (gf_avg_plaq, gf_evolve, gf_hamilton, gf_hamilton_node, gf_sum_
                   gf_sum_re_tr_rect_node_no_comm, glb_sum_double, gm_evolve_fg_pure_gauge, gm_hamilton_node,
                   metropolis_accept, metropolis_accept_cpp, run_hmc_evolve_pure_gauge, run_hmc_pure_gauge,
                   set_gm_force, set_rand_gauge_momentum, unitarize)
+from .batch import ChainBatch
 from .wilson_flow import (gf_energy_density, gf_energy_density_field, gf_energy_derivative_density_field,
                           gf_topology_clf, gf_topology_field_clf, gf_wilson_flow, gf_wilson_flow_force,
                           gf_wilson_flow_step)

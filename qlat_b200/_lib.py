@@ -79,6 +79,16 @@ SIGNATURES = {
     "qgb_autotune_force": [c_field, ctypes.c_double, ctypes.c_int32, c_i32_p, c_dbl_p],
     "qgb_force_time_variant": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, c_dbl_p],
     "qgb_gf_action_sums_noalloc": [ctypes.c_void_p, i32x4, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p],
+    "qgb_batch_create": [c_field_p, ctypes.c_int32, c_i32_p, c_dbl_p, c_dbl_p],
+    "qgb_batch_destroy": [c_field],
+    "qgb_batch_info": [c_field, c_i32_p, c_i64_p],
+    "qgb_batch_set_rand": [c_field, c_u32_p, ctypes.c_double, ctypes.c_int32],
+    "qgb_batch_trajectory": [c_field, c_u32_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                             ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+    "qgb_batch_accept": [c_field, c_i32_p],
+    "qgb_batch_plaq": [c_field, c_dbl_p],
+    "qgb_batch_download_chain": [c_field, ctypes.c_int32, c_dbl_p],
+    "qgb_batch_upload_chain": [c_field, ctypes.c_int32, c_dbl_p],
     "qgb_launch_count": [c_i64_p],
     "qgb_rng_ambiguous_count": [c_i64_p],
 }

@@ -1,0 +1,408 @@
+// batch.cu -- many independent pure-gauge HMC chains advanced together.
+//
+// The chains (each with its own lattice, beta and c1) are concatenated into
+// one structure-of-arrays field of Vtot sites; every phase of a trajectory --
+// momentum refresh, Hamiltonians, forces, exponentials -- is one launch over
+// all chains.  The whole trajectory is recorded once as a CUDA graph per
+// (n_step, md_time, integrator, precision) and replayed, so a trajectory of
+// the batch costs one graph launch plus one read of the per-chain Hamiltonian
+// sums.  Every buffer is allocated when the batch is created: the captured
+// graph never allocates.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/qlat_b200.h"
+#include "kernels.h"
+
+namespace qgb
+{
+void set_last_error(const std::string& msg);
+}
+
+struct qgb_batch_s {
+  int n = 0;
+  long Vtot = 0;
+  bool rect = false;
+  std::vector<qgb::ChainInfo> chains;
+  long* d_offs = nullptr;
+  qgb::ChainInfo* d_chains = nullptr;
+  uint32_t* d_rs = nullptr;
+  uint32_t* h_rs = nullptr;
+  int* d_flags = nullptr;
+  int* h_flags = nullptr;
+  double* gf = nullptr;   // chain states (FP64)
+  double* gf0 = nullptr;  // trajectory copy (FP64)
+  double* gm = nullptr;   // momenta (FP64)
+  double* tmp = nullptr;  // FP64 link scratch
+  float* gf32 = nullptr;
+  float* gm32 = nullptr;
+  float* tmp32 = nullptr;
+  double* d_vals = nullptr;  // per-site values (2 Vtot)
+  double* d_sums = nullptr;  // per-chain sums (8 n)
+  double* h_sums = nullptr;  // pinned mirror
+  int* d_ambiguous = nullptr;
+  double* d_chain_tmp = nullptr;  // one chain's field for download / upload (2 x max chain)
+  long max_chain_reals = 0;
+  cudaStream_t stream = nullptr;
+  std::map<std::tuple<int, double, int, int, int>, cudaGraphExec_t> graphs;
+};
+
+namespace
+{
+
+int bfail(int code, const std::string& m)
+{
+  qgb::set_last_error(m);
+  return code;
+}
+
+#define QB_CUDA(expr)                                                                               \
+  do {                                                                                              \
+    cudaError_t e_ = (expr);                                                                        \
+    if (e_ != cudaSuccess) return bfail(QGB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define QB_RC(expr)              \
+  do {                           \
+    int r_ = (expr);             \
+    if (r_ != QGB_OK) return r_; \
+  } while (0)
+
+qgb::ForceArgs bargs(const void* U, void* out, double dt, int unit)
+{
+  qgb::ForceArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U = U;
+  a.out = out;
+  a.dt = dt;
+  a.unitarize = unit;
+  return a;
+}
+
+template <typename R>
+int batch_force(qgb_batch_s* b, qgb::ForceMode mode, const qgb::ForceArgs& a)
+{
+  QB_CUDA(qgb::launch_force_batch<R>(b->Vtot, b->n, b->d_offs, b->d_chains, b->rect, mode, a, b->stream));
+  return QGB_OK;
+}
+
+template <typename R>
+int batch_evolve(qgb_batch_s* b, void* U, const void* P, double eps, int unit)
+{
+  qgb::Geo g;
+  g.d[0] = g.d[1] = g.d[2] = g.d[3] = 1;
+  g.V = b->Vtot;
+  QB_CUDA(qgb::launch_evolve<R>(g, U, P, eps, unit, 0, b->stream));
+  return QGB_OK;
+}
+
+// Molecular dynamics of all chains (same integrator as the single-lattice
+// trajectory: hmc.pyx:169-188 / examples-py/hmc-pure-gauge-fgf.py:57-69).
+template <typename R>
+int batch_md(qgb_batch_s* b, void* gf, void* gm, void* tmp, int n_step, double md_time, int integrator, int unit_each,
+             int reunit_every)
+{
+  const double dt = md_time / n_step;
+  qgb::Geo g;
+  g.d[0] = g.d[1] = g.d[2] = g.d[3] = 1;
+  g.V = b->Vtot;
+  if (integrator == QGB_INTEGRATOR_FORCE_GRADIENT) {
+    const double lam = 0.5 * (1.0 - 1.0 / sqrt(3.0));
+    const double theta = (2.0 - sqrt(3.0)) / 48.0;
+    const double ttheta = theta * dt * dt * dt;
+    const double fg_dt = 4.0 * ttheta / dt;
+    QB_RC(batch_evolve<R>(b, gf, gm, lam * dt, unit_each));
+    for (int i = 0; i < n_step; ++i) {
+      for (int half = 0; half < 2; ++half) {
+        QB_RC(batch_force<R>(b, qgb::FORCE_EVOLVE, bargs(gf, tmp, fg_dt, unit_each)));
+        QB_RC(batch_force<R>(b, qgb::FORCE_UPDATE, bargs(tmp, gm, 0.5 * dt, 1)));
+        if (half == 0) QB_RC(batch_evolve<R>(b, gf, gm, (1.0 - 2.0 * lam) * dt, unit_each));
+      }
+      QB_RC(batch_evolve<R>(b, gf, gm, (i < n_step - 1 ? 2.0 * lam : lam) * dt, unit_each));
+      if (reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step)
+        QB_CUDA((qgb::launch_unitarize<R, double>(g, 4, gf, b->stream)));
+    }
+  } else if (integrator == QGB_INTEGRATOR_LEAPFROG) {
+    for (int i = 0; i < n_step; ++i) {
+      QB_RC(batch_evolve<R>(b, gf, gm, 0.5 * dt, unit_each));
+      QB_RC(batch_force<R>(b, qgb::FORCE_UPDATE, bargs(gf, gm, dt, 1)));
+      QB_RC(batch_evolve<R>(b, gf, gm, 0.5 * dt, unit_each));
+      if (reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step)
+        QB_CUDA((qgb::launch_unitarize<R, double>(g, 4, gf, b->stream)));
+    }
+  } else {
+    return bfail(QGB_ERR_INVALID_ARG, "unknown integrator");
+  }
+  return QGB_OK;
+}
+
+// Per-chain Hamiltonian pieces of (gm, gf0) into d_sums[slot * n ...]: gm, plaq, rect.
+int batch_hamiltonian(qgb_batch_s* b, int slot)
+{
+  QB_CUDA(qgb::launch_site_values_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, 0, 0, b->gm, b->d_vals,
+                                                b->stream));
+  QB_CUDA(qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals, b->d_sums + (long)slot * b->n, b->stream));
+  QB_CUDA(qgb::launch_site_values_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, 1, b->rect ? 1 : 0, b->gf0,
+                                                b->d_vals, b->stream));
+  QB_CUDA(qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals, b->d_sums + (long)(slot + 1) * b->n, b->stream));
+  if (b->rect)
+    QB_CUDA(qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals + b->Vtot, b->d_sums + (long)(slot + 2) * b->n,
+                                    b->stream));
+  else
+    QB_CUDA(cudaMemsetAsync(b->d_sums + (long)(slot + 2) * b->n, 0, b->n * sizeof(double), b->stream));
+  return QGB_OK;
+}
+
+// One trajectory of every chain, enqueued on b->stream (recordable as a graph).
+int enqueue_trajectory(qgb_batch_s* b, int n_step, double md_time, int integrator, int mixed, int reunit)
+{
+  const size_t bytes64 = (size_t)b->Vtot * 72 * sizeof(double);
+  const long n = b->Vtot * 72;
+  qgb::Geo g;
+  g.d[0] = g.d[1] = g.d[2] = g.d[3] = 1;
+  g.V = b->Vtot;
+  QB_CUDA(cudaMemcpyAsync(b->gf0, b->gf, bytes64, cudaMemcpyDeviceToDevice, b->stream));
+  QB_CUDA(qgb::launch_rand_momentum_batch<double>(b->Vtot, b->n, b->d_offs, b->d_rs, 1.0, b->gm, b->d_ambiguous,
+                                                  b->stream));
+  QB_RC(batch_hamiltonian(b, 0));
+  if (mixed) {
+    QB_CUDA((qgb::launch_convert<double, float>(n, b->gf0, b->gf32, b->stream)));
+    QB_CUDA((qgb::launch_convert<double, float>(n, b->gm, b->gm32, b->stream)));
+    QB_RC(batch_md<float>(b, b->gf32, b->gm32, b->tmp32, n_step, md_time, integrator, reunit > 0 ? 0 : 1, reunit));
+    QB_CUDA((qgb::launch_convert<float, double>(n, b->gf32, b->gf0, b->stream)));
+    QB_CUDA((qgb::launch_convert<float, double>(n, b->gm32, b->gm, b->stream)));
+  } else {
+    QB_RC(batch_md<double>(b, b->gf0, b->gm, b->tmp, n_step, md_time, integrator, 1, 0));
+  }
+  QB_CUDA((qgb::launch_unitarize<double, double>(g, 4, b->gf0, b->stream)));
+  QB_RC(batch_hamiltonian(b, 3));
+  QB_CUDA(cudaMemcpyAsync(b->h_sums, b->d_sums, 6 * b->n * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  return QGB_OK;
+}
+
+double chain_action(const qgb::ChainInfo& c, double sp, double sr)
+{
+  return -c.beta / 3.0 * ((1.0 - 8.0 * c.c1) * sp + c.c1 * (c.c1 == 0.0 ? 0.0 : sr));
+}
+
+}  // namespace
+
+extern "C" {
+
+int qgb_batch_create(qgb_batch** out, int32_t n_chains, const int32_t* total_sites, const double* beta,
+                     const double* c1)
+{
+  if (!out || !total_sites || !beta || !c1 || n_chains < 1)
+    return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_create: bad argument");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bfail(QGB_ERR_NO_DEVICE, "no CUDA device");
+  qgb_batch_s* b = new qgb_batch_s;
+  b->n = n_chains;
+  std::vector<long> offs(n_chains + 1, 0);
+  long max_v = 0;
+  for (int c = 0; c < n_chains; ++c) {
+    qgb::ChainInfo ci;
+    long V = 1;
+    for (int i = 0; i < 4; ++i) {
+      if (total_sites[4 * c + i] < 1 || total_sites[4 * c + i] > (1 << 20)) {
+        delete b;
+        return bfail(QGB_ERR_BAD_GEOMETRY, "qgb_batch_create: each lattice extent must be in [1, 2^20]");
+      }
+      ci.d[i] = total_sites[4 * c + i];
+      V *= ci.d[i];
+    }
+    ci.V = V;
+    ci.off = offs[c];
+    ci.beta = beta[c];
+    ci.c1 = c1[c];
+    if (c1[c] != 0.0) b->rect = true;
+    offs[c + 1] = offs[c] + V;
+    if (V > max_v) max_v = V;
+    b->chains.push_back(ci);
+  }
+  b->Vtot = offs[n_chains];
+  b->max_chain_reals = max_v * 72;
+  const size_t b64 = (size_t)b->Vtot * 72 * sizeof(double), b32 = b64 / 2;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  A((void**)&b->d_offs, (n_chains + 1) * sizeof(long));
+  A((void**)&b->d_chains, n_chains * sizeof(qgb::ChainInfo));
+  A((void**)&b->d_rs, (size_t)n_chains * 24 * sizeof(uint32_t));
+  A((void**)&b->d_flags, n_chains * sizeof(int));
+  A((void**)&b->gf, b64);
+  A((void**)&b->gf0, b64);
+  A((void**)&b->gm, b64);
+  A((void**)&b->tmp, b64);
+  A((void**)&b->gf32, b32);
+  A((void**)&b->gm32, b32);
+  A((void**)&b->tmp32, b32);
+  A((void**)&b->d_vals, 2 * b->Vtot * sizeof(double));
+  A((void**)&b->d_sums, 8 * (size_t)n_chains * sizeof(double));
+  A((void**)&b->d_ambiguous, sizeof(int));
+  A((void**)&b->d_chain_tmp, 2 * b->max_chain_reals * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_rs, (size_t)n_chains * 24 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_flags, n_chains * sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_sums, 8 * (size_t)n_chains * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_offs, offs.data(), (n_chains + 1) * sizeof(long), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_chains, b->chains.data(), n_chains * sizeof(qgb::ChainInfo), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(b->d_ambiguous, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->gf, 0, b64);
+  if (e != cudaSuccess) {
+    qgb_batch_destroy(b);
+    cudaGetLastError();
+    return bfail(QGB_ERR_ALLOC, std::string("qgb_batch_create: ") + cudaGetErrorString(e));
+  }
+  qgb::init_constants();
+  *out = b;
+  return QGB_OK;
+}
+
+int qgb_batch_destroy(qgb_batch* b)
+{
+  if (!b) return QGB_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  void* dev[] = {b->d_offs, b->d_chains, b->d_rs, b->d_flags, b->gf,     b->gf0,         b->gm,
+                 b->tmp,    b->gf32,     b->gm32, b->tmp32,   b->d_vals, b->d_sums,      b->d_ambiguous,
+                 b->d_chain_tmp};
+  for (void* p : dev)
+    if (p) cudaFree(p);
+  if (b->h_rs) cudaFreeHost(b->h_rs);
+  if (b->h_flags) cudaFreeHost(b->h_flags);
+  if (b->h_sums) cudaFreeHost(b->h_sums);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return QGB_OK;
+}
+
+int qgb_batch_info(const qgb_batch* b, int32_t* n_chains, int64_t* total_site_count)
+{
+  if (!b) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_info: null batch");
+  if (n_chains) *n_chains = b->n;
+  if (total_site_count) *total_site_count = b->Vtot;
+  return QGB_OK;
+}
+
+int qgb_batch_set_rand(qgb_batch* b, const uint32_t* rs, double sigma, int32_t n_step)
+{
+  if (!b || !rs) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_set_rand: null argument");
+  memcpy(b->h_rs, rs, (size_t)b->n * 24 * sizeof(uint32_t));
+  QB_CUDA(cudaMemcpyAsync(b->d_rs, b->h_rs, (size_t)b->n * 24 * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+  QB_CUDA(qgb::launch_hot_start_batch<double>(b->Vtot, b->n, b->d_offs, b->d_rs, sigma, n_step, b->gf,
+                                              b->d_ambiguous, b->stream));
+  QB_CUDA(cudaStreamSynchronize(b->stream));
+  return QGB_OK;
+}
+
+int qgb_batch_trajectory(qgb_batch* b, const uint32_t* rs_momentum, int32_t n_step, double md_time,
+                         int32_t integrator, int32_t mixed, int32_t reunit_interval, int32_t use_graph,
+                         double* delta_h)
+{
+  if (!b || !rs_momentum || !delta_h || n_step < 1) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_trajectory: bad argument");
+  memcpy(b->h_rs, rs_momentum, (size_t)b->n * 24 * sizeof(uint32_t));
+  QB_CUDA(cudaMemcpyAsync(b->d_rs, b->h_rs, (size_t)b->n * 24 * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+  const int reunit = mixed ? reunit_interval : 0;
+  if (use_graph) {
+    auto key = std::make_tuple((int)n_step, md_time, (int)integrator, (int)(mixed != 0), reunit);
+    auto it = b->graphs.find(key);
+    if (it == b->graphs.end()) {
+      cudaGraph_t graph = nullptr;
+      QB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      const int rc = enqueue_trajectory(b, n_step, md_time, integrator, mixed, reunit);
+      cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+      if (rc != QGB_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (e != cudaSuccess) return bfail(QGB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+      cudaGraphExec_t exec = nullptr;
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return bfail(QGB_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      it = b->graphs.emplace(key, exec).first;
+    }
+    QB_CUDA(cudaGraphLaunch(it->second, b->stream));
+  } else {
+    QB_RC(enqueue_trajectory(b, n_step, md_time, integrator, mixed, reunit));
+  }
+  QB_CUDA(cudaStreamSynchronize(b->stream));
+  const int n = b->n;
+  for (int c = 0; c < n; ++c) {
+    const qgb::ChainInfo& ci = b->chains[c];
+    const double h0 = b->h_sums[c] + chain_action(ci, b->h_sums[n + c], b->h_sums[2 * n + c]);
+    const double h1 = b->h_sums[3 * n + c] + chain_action(ci, b->h_sums[4 * n + c], b->h_sums[5 * n + c]);
+    delta_h[c] = h1 - h0;
+  }
+  return QGB_OK;
+}
+
+int qgb_batch_accept(qgb_batch* b, const int32_t* flags)
+{
+  if (!b || !flags) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_accept: null argument");
+  for (int c = 0; c < b->n; ++c) b->h_flags[c] = flags[c] ? 1 : 0;
+  QB_CUDA(cudaMemcpyAsync(b->d_flags, b->h_flags, b->n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  QB_CUDA(qgb::launch_accept_batch<double>(b->Vtot, b->n, b->d_offs, b->d_flags, b->gf, b->gf0, b->stream));
+  QB_CUDA(cudaStreamSynchronize(b->stream));
+  return QGB_OK;
+}
+
+int qgb_batch_plaq(qgb_batch* b, double* plaq)
+{
+  if (!b || !plaq) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_plaq: null argument");
+  QB_CUDA(qgb::launch_site_values_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, 1, 0, b->gf, b->d_vals,
+                                                b->stream));
+  QB_CUDA(qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals, b->d_sums + 6L * b->n, b->stream));
+  QB_CUDA(cudaMemcpyAsync(b->h_sums + 6L * b->n, b->d_sums + 6L * b->n, b->n * sizeof(double), cudaMemcpyDeviceToHost,
+                          b->stream));
+  QB_CUDA(cudaStreamSynchronize(b->stream));
+  for (int c = 0; c < b->n; ++c) plaq[c] = 1.0 + b->h_sums[6L * b->n + c] / (18.0 * (double)b->chains[c].V);
+  return QGB_OK;
+}
+
+// Chain c's links <-> host buffer in the reference memory image.
+int qgb_batch_download_chain(qgb_batch* b, int32_t chain, double* host)
+{
+  if (!b || !host || chain < 0 || chain >= b->n) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_download_chain: bad argument");
+  const qgb::ChainInfo& ci = b->chains[chain];
+  double* soa = b->d_chain_tmp;
+  double* aos = b->d_chain_tmp + b->max_chain_reals;
+  // 36 components of 16-byte complex numbers: [mu*9 + k][site] with pitch Vtot -> pitch V
+  QB_CUDA(cudaMemcpy2DAsync(soa, ci.V * 16, b->gf + ci.off * 2, b->Vtot * 16, ci.V * 16, 36, cudaMemcpyDeviceToDevice,
+                            b->stream));
+  qgb::Geo g;
+  for (int i = 0; i < 4; ++i) g.d[i] = ci.d[i];
+  g.V = ci.V;
+  QB_CUDA(qgb::launch_soa_to_aos<double>(g, 4, 18, soa, aos, b->stream));
+  QB_CUDA(cudaMemcpyAsync(host, aos, ci.V * 72 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  QB_CUDA(cudaStreamSynchronize(b->stream));
+  return QGB_OK;
+}
+
+int qgb_batch_upload_chain(qgb_batch* b, int32_t chain, const double* host)
+{
+  if (!b || !host || chain < 0 || chain >= b->n) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_upload_chain: bad argument");
+  const qgb::ChainInfo& ci = b->chains[chain];
+  double* soa = b->d_chain_tmp;
+  double* aos = b->d_chain_tmp + b->max_chain_reals;
+  QB_CUDA(cudaMemcpyAsync(aos, host, ci.V * 72 * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+  qgb::Geo g;
+  for (int i = 0; i < 4; ++i) g.d[i] = ci.d[i];
+  g.V = ci.V;
+  QB_CUDA(qgb::launch_aos_to_soa<double>(g, 4, 18, aos, soa, b->stream));
+  QB_CUDA(cudaMemcpy2DAsync(b->gf + ci.off * 2, b->Vtot * 16, soa, ci.V * 16, ci.V * 16, 36, cudaMemcpyDeviceToDevice,
+                            b->stream));
+  QB_CUDA(cudaStreamSynchronize(b->stream));
+  return QGB_OK;
+}
+
+}  // extern "C"

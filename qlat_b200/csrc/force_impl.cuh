@@ -104,6 +104,36 @@ __device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g,
 // ------------------------------------------------------------------------
 // force: F = TA(-beta/3 U_mu(x) S^+) (hmc.cpp:64-75) and its fused consumers
 
+// F = TA(-beta/3 U_mu(x) S^+) (hmc.cpp:64-75) at global site s of a field with
+// `stride` sites, then the mode's consumer: store F, P += dt F, or
+// U_out = unitarize(exp(eps Z) U) with Z = F or the flow combination a F + b Z'.
+template <typename R, int MODE>
+__device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<R>& U, long stride, long s, int mu,
+                                               const M3<R>& S, double beta)
+{
+  const M3<R> u = U.ld(s, mu);
+  M3<R> F = traceless_antiherm(mul_adj(u, S));
+  F = scale(R(-beta / 3.0), F);
+  if (MODE == FORCE_SET) {
+    WField<R>{(Cx<R>*)a.out, stride}.st(s, mu, F);
+  } else if (MODE == FORCE_UPDATE) {
+    const WField<R> P{(Cx<R>*)a.out, stride};
+    M3<R> p = P.ld(s, mu);
+    axpy(p, R(a.dt), F);
+    P.st(s, mu, p);
+  } else {
+    M3<R> Z = F;
+    if (MODE == FORCE_FLOW) {
+      Z = scale(R(a.a), F);
+      if (a.zp != nullptr && a.b != 0.0) axpy(Z, R(a.b), CField<R>{(const Cx<R>*)a.zp, stride}.ld(s, mu));
+      if (a.z != nullptr) WField<R>{(Cx<R>*)a.z, stride}.st(s, mu, Z);
+    }
+    M3<R> un = mul(exp_ch(scale(R(a.dt), Z)), u);
+    if (a.unitarize) unitarize(un);
+    WField<R>{(Cx<R>*)a.out, stride}.st(s, mu, un);
+  }
+}
+
 // Launch variants for the autotuner: threads per block, minimum resident
 // blocks per SM (caps registers), threads per link (SPLIT = 2 gives each link
 // to a lane pair, each doing 3 of the 6 signed directions, combined by a
@@ -182,27 +212,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
     }
     if (!valid || h != 0) return;
   }
-  const M3<R> u = U.ld(s, mu);
-  M3<R> F = traceless_antiherm(mul_adj(u, S));
-  F = scale(R(-a.beta / 3.0), F);
-  if (MODE == FORCE_SET) {
-    WField<R>{(Cx<R>*)a.out, g.V}.st(s, mu, F);
-  } else if (MODE == FORCE_UPDATE) {
-    const WField<R> P{(Cx<R>*)a.out, g.V};
-    M3<R> p = P.ld(s, mu);
-    axpy(p, R(a.dt), F);
-    P.st(s, mu, p);
-  } else {
-    M3<R> Z = F;
-    if (MODE == FORCE_FLOW) {
-      Z = scale(R(a.a), F);
-      if (a.zp != nullptr && a.b != 0.0) axpy(Z, R(a.b), CField<R>{(const Cx<R>*)a.zp, g.V}.ld(s, mu));
-      if (a.z != nullptr) WField<R>{(Cx<R>*)a.z, g.V}.st(s, mu, Z);
-    }
-    M3<R> un = mul(exp_ch(scale(R(a.dt), Z)), u);
-    if (a.unitarize) unitarize(un);
-    WField<R>{(Cx<R>*)a.out, g.V}.st(s, mu, un);
-  }
+  force_epilogue<R, MODE>(a, U, g.V, s, mu, S, a.beta);
 }
 
 template <typename R, int BS, int MINB, int SPLIT, bool PACKED, int MAP>
@@ -248,6 +258,46 @@ inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* 
 #undef QGB_V
     default: return 0;
   }
+}
+
+// Batched force: every chain of a batch in one launch, one thread per link of
+// the concatenated field (Vtot sites, mu = blockIdx.y).  Each thread finds its
+// chain by binary search over the chain offsets and uses that chain's lattice,
+// beta and c1.  RECT is set when any chain has c1 != 0 (Wilson chains then add
+// rectangle terms with weight 0).
+template <typename R, int MODE, bool RECT>
+__global__ void __launch_bounds__(128) k_force_batch(long Vtot, int nchain, const long* __restrict__ offs,
+                                                     const ChainInfo* __restrict__ chains, ForceArgs a)
+{
+  const long sg = (long)blockIdx.x * 128 + threadIdx.x;
+  if (sg >= Vtot) return;
+  const int c = chain_of(offs, nchain, sg);
+  const ChainInfo ci = chains[c];
+  const Geo g = chain_geo(ci);
+  const int mu = blockIdx.y;
+  const CField<R> U{(const Cx<R>*)a.U, Vtot};
+  const Coord x = coord_of(g, sg - ci.off);
+  const R cp = R(1.0 - 8.0 * ci.c1), cr = R(ci.c1);
+  const M3<R> S = staple_sum_rt<R, RECT, false>(U, g, x, mu, cp, cr, 0, 6);
+  force_epilogue<R, MODE>(a, U, Vtot, sg, mu, S, ci.beta);
+}
+
+template <typename R>
+cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
+                               ForceMode mode, const ForceArgs& a, cudaStream_t st)
+{
+  dim3 grid((unsigned)((Vtot + 127) / 128), 4);
+#define QGB_LAUNCH(M)                                                                      \
+  if (rect) k_force_batch<R, M, true><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a); \
+  else k_force_batch<R, M, false><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);
+  switch (mode) {
+    case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
+    case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;
+    case FORCE_EVOLVE: QGB_LAUNCH(FORCE_EVOLVE) break;
+    case FORCE_FLOW: QGB_LAUNCH(FORCE_FLOW) break;
+  }
+#undef QGB_LAUNCH
+  return cudaGetLastError();
 }
 
 }  // namespace qgb

@@ -99,7 +99,7 @@ __device__ __forceinline__ long site_at(const Geo& g, const Coord& x, int a, int
   int y[4] = {x.c[0], x.c[1], x.c[2], x.c[3]};
   y[MU] = wrap(y[MU] + a, g.d[MU]);
   if (b != 0) y[NU] = wrap(y[NU] + b, g.d[NU]);
-  return (long)y[0] + (long)g.d[0] * ((long)y[1] + (long)g.d[1] * ((long)y[2] + (long)g.d[2] * (long)y[3]));
+  return g.off + (long)y[0] + (long)g.d[0] * ((long)y[1] + (long)g.d[1] * ((long)y[2] + (long)g.d[2] * (long)y[3]));
 }
 
 // Same with run-time directions mu != nu (no local-memory arrays: each
@@ -113,7 +113,30 @@ __device__ __forceinline__ long site_rt(const Geo& g, const Coord& x, int mu, in
     const int y = wrap(x.c[k] + off, g.d[k]);
     idx = (k == 3) ? (long)y : idx * (long)g.d[k] + y;
   }
-  return idx;
+  return g.off + idx;
+}
+
+// Chain of global site sg: the largest i with offs[i] <= sg (offs ascending, offs[0] = 0).
+__device__ __forceinline__ int chain_of(const long* __restrict__ offs, int n, long sg)
+{
+  int lo = 0, hi = n;  // invariant: offs[lo] <= sg < offs[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(offs + mid) <= sg) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ Geo chain_geo(const ChainInfo& c)
+{
+  Geo g;
+  g.d[0] = c.d[0];
+  g.d[1] = c.d[1];
+  g.d[2] = c.d[2];
+  g.d[3] = c.d[3];
+  g.V = c.V;
+  g.off = c.off;
+  return g;
 }
 
 }  // namespace qgb

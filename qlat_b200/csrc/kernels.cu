@@ -463,6 +463,198 @@ cudaError_t launch_hot_start(const Geo& g, void* U, const uint32_t* rs24, double
 }
 
 // ------------------------------------------------------------------------
+// batches of independent chains (all chains in one launch)
+
+// Per-site random momenta of every chain: chain c uses RngState rs24[24 c ..]
+// split by the site's index within its chain.
+template <typename R>
+__global__ void __launch_bounds__(128) k_rand_momentum_batch(long Vtot, int nchain, const long* __restrict__ offs,
+                                                             const uint32_t* __restrict__ rs24, double s_sigma,
+                                                             double inv_sqrt3, Cx<R>* P, int* ambiguous)
+{
+  const long sg = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= Vtot) return;
+  const int c = chain_of(offs, nchain, sg);
+  Rng base, rs;
+  rng_import(base, rs24 + 24 * c);
+  rng_split_long(rs, base, (int64_t)(sg - offs[c]));
+  int amb = 0;
+  const WField<R> Pf{P, Vtot};
+  for (int mu = 0; mu < 4; ++mu) {
+    double b[8];
+    for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
+    const M3<double> m = x_make_anti_hermitian(b, inv_sqrt3);
+    M3<R> mr;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) mr.e[k] = cx<R>((R)m.e[k].re, (R)m.e[k].im);
+    Pf.st(sg, mu, mr);
+  }
+  if (amb) atomicAdd(ambiguous, 1);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_hot_start_batch(long Vtot, int nchain, const long* __restrict__ offs,
+                                                         const uint32_t* __restrict__ rs24, double s_sigma,
+                                                         double inv_sqrt3, int n_step, Cx<R>* U, int* ambiguous)
+{
+  const long sg = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= Vtot) return;
+  const int c = chain_of(offs, nchain, sg);
+  Rng base, rs;
+  rng_import(base, rs24 + 24 * c);
+  rng_split_long(rs, base, (int64_t)(sg - offs[c]));
+  int amb = 0;
+  const WField<R> Uf{U, Vtot};
+  for (int mu = 0; mu < 4; ++mu) {
+    M3<double> v;
+    const int nk = n_step > 1 ? n_step : 1;
+    for (int k = 0; k < nk; ++k) {
+      double b[8];
+      for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
+      M3<double> e = x_exp_taylor20(x_make_anti_hermitian(b, inv_sqrt3));
+      x_unitarize(e);
+      v = (k == 0) ? e : xm_mul(v, e);
+    }
+    M3<R> vr;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) vr.e[k] = cx<R>((R)v.e[k].re, (R)v.e[k].im);
+    Uf.st(sg, mu, vr);
+  }
+  if (amb) atomicAdd(ambiguous, 1);
+}
+
+// Site values for the per-chain Hamiltonians: what = 0: sum_mu -tr(P^2)/2 from
+// P into vals[sg]; what = 1: plaquette sum (vals[sg]) and, if rect, rectangle
+// sum (vals[Vtot + sg]) from U.
+template <typename R>
+__global__ void __launch_bounds__(128) k_site_values_batch(long Vtot, int nchain, const long* __restrict__ offs,
+                                                           const ChainInfo* __restrict__ chains, int what, int rect,
+                                                           const Cx<R>* F, double* vals)
+{
+  const long sg = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= Vtot) return;
+  const CField<R> Ff{F, Vtot};
+  if (what == 0) {
+    double v = 0.0;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) v += neg_half_tr_square(Ff.ld(sg, mu));
+    vals[sg] = v;
+    return;
+  }
+  const int c = chain_of(offs, nchain, sg);
+  const Geo g = chain_geo(chains[c]);
+  const Coord x = coord_of(g, sg - g.off);
+  double sp = 0.0, sr = 0.0;
+#pragma unroll 1
+  for (int p = 0; p < 6; ++p) {
+    const int mu = p < 3 ? 0 : (p < 5 ? 1 : 2);
+    const int nu = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
+    const M3<R> A = mul(Ff.ld(sg, mu), Ff.ld(site_rt(g, x, mu, 1, nu, 0), nu));
+    const M3<R> B = mul(Ff.ld(sg, nu), Ff.ld(site_rt(g, x, mu, 0, nu, 1), mu));
+    sp += (double)re_tr_mul_adj(A, B) - 3.0;
+    if (rect) {
+#pragma unroll 1
+      for (int o = 0; o < 2; ++o) {
+        const int a = o == 0 ? mu : nu, b = o == 0 ? nu : mu;
+        M3<R> A2 = mul(Ff.ld(sg, a), Ff.ld(site_rt(g, x, a, 1, b, 0), a));
+        A2 = mul(A2, Ff.ld(site_rt(g, x, a, 2, b, 0), b));
+        M3<R> B2 = mul(Ff.ld(sg, b), Ff.ld(site_rt(g, x, a, 0, b, 1), a));
+        B2 = mul(B2, Ff.ld(site_rt(g, x, a, 1, b, 1), a));
+        sr += (double)re_tr_mul_adj(A2, B2) - 3.0;
+      }
+    }
+  }
+  vals[sg] = sp;
+  if (rect) vals[Vtot + sg] = sr;
+}
+
+// out[c] = sum of vals over chain c's sites, one block per chain, fixed order.
+__global__ void __launch_bounds__(256) k_segment_sum(int nchain, const long* __restrict__ offs,
+                                                     const double* __restrict__ vals, double* out)
+{
+  const int c = blockIdx.x;
+  const long a = offs[c], b = offs[c + 1];
+  double t = 0.0;
+  for (long i = a + threadIdx.x; i < b; i += blockDim.x) t += vals[i];
+  __shared__ double sm[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int i = 0; i < 8; ++i) r += sm[i];
+    out[c] = r;
+  }
+}
+
+// dst = src on the sites of chains whose flag is set (4 links per site).
+template <typename R>
+__global__ void k_accept_batch(long Vtot, int nchain, const long* __restrict__ offs, const int* __restrict__ flags,
+                               Cx<R>* dst, const Cx<R>* src)
+{
+  const long sg = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= Vtot) return;
+  const int c = chain_of(offs, nchain, sg);
+  if (!flags[c]) return;
+  const CField<R> S{src, Vtot};
+  const WField<R> D{dst, Vtot};
+  for (int mu = 0; mu < 4; ++mu) D.st(sg, mu, S.ld(sg, mu));
+}
+
+template <typename R>
+cudaError_t launch_rand_momentum_batch(long Vtot, int nchain, const long* offs, const uint32_t* rs24, double sigma,
+                                       void* P, int* ambiguous, cudaStream_t st)
+{
+  k_rand_momentum_batch<R><<<(unsigned)((Vtot + 127) / 128), 128, 0, st>>>(Vtot, nchain, offs, rs24, sigma / sqrt(2.0),
+                                                                          1.0 / sqrt(3.0), (Cx<R>*)P, ambiguous);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_hot_start_batch(long Vtot, int nchain, const long* offs, const uint32_t* rs24, double sigma,
+                                   int n_step, void* U, int* ambiguous, cudaStream_t st)
+{
+  k_hot_start_batch<R><<<(unsigned)((Vtot + 127) / 128), 128, 0, st>>>(Vtot, nchain, offs, rs24, sigma / sqrt(2.0),
+                                                                      1.0 / sqrt(3.0), n_step, (Cx<R>*)U, ambiguous);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_site_values_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, int what,
+                                     int rect, const void* F, double* vals, cudaStream_t st)
+{
+  k_site_values_batch<R><<<(unsigned)((Vtot + 127) / 128), 128, 0, st>>>(Vtot, nchain, offs, chains, what, rect,
+                                                                        (const Cx<R>*)F, vals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_segment_sum(int nchain, const long* offs, const double* vals, double* out, cudaStream_t st)
+{
+  k_segment_sum<<<nchain, 256, 0, st>>>(nchain, offs, vals, out);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_accept_batch(long Vtot, int nchain, const long* offs, const int* flags, void* dst, const void* src,
+                                cudaStream_t st)
+{
+  k_accept_batch<R><<<(unsigned)((Vtot + 127) / 128), 128, 0, st>>>(Vtot, nchain, offs, flags, (Cx<R>*)dst,
+                                                                    (const Cx<R>*)src);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_rand_momentum_batch<double>(long, int, const long*, const uint32_t*, double, void*, int*,
+                                                        cudaStream_t);
+template cudaError_t launch_hot_start_batch<double>(long, int, const long*, const uint32_t*, double, int, void*, int*,
+                                                    cudaStream_t);
+template cudaError_t launch_site_values_batch<double>(long, int, const long*, const ChainInfo*, int, int, const void*,
+                                                      double*, cudaStream_t);
+template cudaError_t launch_site_values_batch<float>(long, int, const long*, const ChainInfo*, int, int, const void*,
+                                                     double*, cudaStream_t);
+template cudaError_t launch_accept_batch<double>(long, int, const long*, const int*, void*, const void*, cudaStream_t);
+
+// ------------------------------------------------------------------------
 // elementwise field operations
 
 template <typename R>

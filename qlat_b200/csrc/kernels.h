@@ -8,8 +8,17 @@ namespace qgb
 {
 
 struct Geo {
-  int d[4];  // X, Y, Z, T
+  int d[4];      // X, Y, Z, T
+  long V;        // sites of this lattice
+  long off = 0;  // index of its first site in a field holding several lattices
+};
+
+// One chain of a batch: its lattice, offset in the concatenated field and action.
+struct ChainInfo {
+  int d[4];
   long V;
+  long off;
+  double beta, c1;
 };
 
 // Force kernel output modes (see kernels.cu).
@@ -37,6 +46,10 @@ void init_constants();  // SHA-256 and log tables into constant memory (per devi
 template <typename R>
 cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, int variant, cudaStream_t st);
 int force_variant_count();
+// All chains of a batch in one launch (offs: nchain + 1 ascending offsets on the device).
+template <typename R>
+cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
+                               ForceMode mode, const ForceArgs& a, cudaStream_t st);
 int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed, int* map);
 
 // U = exp(eps P) U (optionally unitarized; exp by Cayley-Hamilton series or the
@@ -78,6 +91,21 @@ cudaError_t launch_hot_start(const Geo& g, void* U, const uint32_t* rs24, double
 
 template <typename R>
 cudaError_t launch_set_unit(const Geo& g, int m, void* U, cudaStream_t st);
+
+// Batches of chains concatenated in one field (offs: nchain + 1 offsets, device).
+template <typename R>
+cudaError_t launch_rand_momentum_batch(long Vtot, int nchain, const long* offs, const uint32_t* rs24, double sigma,
+                                       void* P, int* ambiguous, cudaStream_t st);
+template <typename R>
+cudaError_t launch_hot_start_batch(long Vtot, int nchain, const long* offs, const uint32_t* rs24, double sigma,
+                                   int n_step, void* U, int* ambiguous, cudaStream_t st);
+template <typename R>
+cudaError_t launch_site_values_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, int what,
+                                     int rect, const void* F, double* vals, cudaStream_t st);
+cudaError_t launch_segment_sum(int nchain, const long* offs, const double* vals, double* out, cudaStream_t st);
+template <typename R>
+cudaError_t launch_accept_batch(long Vtot, int nchain, const long* offs, const int* flags, void* dst, const void* src,
+                                cudaStream_t st);
 // y = a x + b y over n reals
 template <typename R>
 cudaError_t launch_axpby(long n, void* y, double a, const void* x, double b, cudaStream_t st);

@@ -1,0 +1,178 @@
+"""Kernel-level benchmarks and profiling drivers for the GPU library.
+
+    python -m qlat_b200.kernel_bench force-variants [--lattice 24,24,24,64]
+        time every force-kernel launch variant (FP64 / FP32, Wilson / Iwasaki)
+    python -m qlat_b200.kernel_bench force-profile --variants 0,7 [--lattice 24,24,24,48]
+        one set_gm_force launch per variant and precision (Iwasaki), for ncu -k regex:k_force
+    python -m qlat_b200.kernel_bench flow [--lattice 32,32,32,32] [--steps 80] [--every 4]
+        gradient flow (RK3, eps = 0.05) with t^2 E(t) and the clover charge Q measured every
+        `every` steps, FP64 and FP32 storage; prints timings and the FP32 errors
+    python -m qlat_b200.kernel_bench batch [--per-size 64] [--trajs 10]
+        256 independent chains of 4^4 ... 12^4 advanced together (CUDA graph per trajectory)
+
+Each command prints one JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+
+def _lattice(s):
+    return tuple(int(v) for v in s.split(","))
+
+
+def force_variants(args):
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    ts = _lattice(args.lattice)
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("kernel-bench").split("gf-init"), 0.3, 1)
+    g32 = gf.copy(precision=q.F32)
+    res = {"lattice": list(ts), "variants": q.force_variants()}
+    for name, g in (("fp64", gf), ("fp32", g32)):
+        for c1 in (0.0, -0.331):
+            res[f"{name} c1={c1} ms"] = [round(q.force_time_variant(g, c1, v, reps=args.reps), 4)
+                                         for v in range(len(res["variants"]))]
+    print(json.dumps(res))
+
+
+def force_profile(args):
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    ts = _lattice(args.lattice)
+    variants = [int(v) for v in args.variants.split(",")]
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("kernel-bench").split("gf-init"), 0.3, 1)
+    g32 = gf.copy(precision=q.F32)
+    ga = q.GaugeAction(2.13, -0.331)
+    for prec, g in ((q.F32, g32), (q.F64, gf)):
+        F = q.GaugeMomentum(gf.geo, precision=prec)
+        for v in variants:
+            q.force_set_variant(prec, True, v)
+            q.set_gm_force(F, g, ga)
+    q.synchronize()
+    print(json.dumps({"lattice": list(ts), "variants": variants, "launches": 2 * len(variants)}))
+
+
+def flow(args):
+    """Gradient flow of a hot start: RK3 steps of eps, t^2 E and clover Q every
+    `every` steps, in FP64 and with FP32 links (FP64 reductions)."""
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    ts = _lattice(args.lattice)
+    geo = q.Geometry(ts)
+    gf = q.GaugeField(geo)
+    gf.set_rand(q.RngState("b200-c3-flow").split("gf-init"), args.sigma, args.n_step)
+    stream = torch.cuda.current_stream()
+    q.set_stream(stream.cuda_stream)
+    out = {"lattice": list(ts), "eps": args.eps, "steps": args.steps, "every": args.every,
+           "hot_start": {"sigma": args.sigma, "n_step": args.n_step}}
+    series = {}
+    for name, prec in (("fp64", q.F64), ("fp32", q.F32)):
+        g = gf.copy(precision=prec)
+        # warm-up: one step on a scratch copy
+        w = g.copy()
+        q.gf_wilson_flow_step(w, args.eps, c1=args.c1)
+        del w
+        torch.cuda.synchronize()
+        t2e, topo, times = [], [], []
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            q.gf_wilson_flow_step(g, args.eps, c1=args.c1)
+            if (i + 1) % args.every == 0:
+                t = (i + 1) * args.eps
+                t2e.append(t * t * q.gf_energy_density(g))
+                topo.append(q.gf_topology_clf(g))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        series[name] = (t2e, topo)
+        out[name] = {"ms_total": ms, "ms_per_step": ms / args.steps, "t2E_final": t2e[-1], "Q_final": topo[-1],
+                     "plaq_final": g.plaq()}
+    d_t2e = max(abs(a - b) for a, b in zip(series["fp32"][0], series["fp64"][0]))
+    d_q = max(abs(a - b) for a, b in zip(series["fp32"][1], series["fp64"][1]))
+    rel_t2e = max(abs(a - b) / abs(b) for a, b in zip(series["fp32"][0], series["fp64"][0]) if b != 0)
+    out["fp32_vs_fp64"] = {"max_abs_t2E": d_t2e, "max_rel_t2E": rel_t2e, "max_abs_Q": d_q}
+    out["t2E_fp64"] = series["fp64"][0]
+    out["Q_fp64"] = series["fp64"][1]
+    out["fp32_over_fp64_speed"] = out["fp64"]["ms_total"] / out["fp32"]["ms_total"]
+    print(json.dumps(out))
+
+
+def batch(args):
+    """256 independent Wilson chains: 64 each of 4^4, 6^4, 8^4, 12^4, betas evenly
+    spaced in [5.6, 6.2], hot starts at scale 1, leapfrog with 10 steps of total
+    length 1, one CUDA graph per trajectory.  Reports aggregate link updates/s
+    for the mixed and FP64 forms and the per-chain plaquette difference between
+    them after the same trajectories."""
+    import numpy as np
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    sizes = [(L, L, L, L) for L in (4, 6, 8, 12) for _ in range(args.per_size)]
+    n = len(sizes)
+    betas = list(np.linspace(5.6, 6.2, n))
+    rs = [q.RngState("b200-c5-batch").split(f"chain-{c}") for c in range(n)]
+    out = {"chains": n, "sites": int(sum(np.prod(s) for s in sizes)), "n_step": args.n_step}
+    plaqs = {}
+    for prec in ("mixed", "fp64"):
+        b = q.ChainBatch(sizes, betas)
+        b.set_rand([r.split("gf-init") for r in rs], 1.0, 1)
+        for t in range(1, args.warmup + 1):
+            b.run_hmc(t, rs, args.n_step, precision=prec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        acc = 0
+        for t in range(args.warmup + 1, args.warmup + 1 + args.trajs):
+            flags, dh = b.run_hmc(t, rs, args.n_step, precision=prec)
+            acc += sum(flags)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        link_updates = 4 * out["sites"] * args.n_step * args.trajs
+        out[prec] = {"s_per_traj": dt / args.trajs, "link_updates_per_s": link_updates / dt,
+                     "accept_rate": acc / (n * args.trajs)}
+        plaqs[prec] = b.plaq()
+        del b
+    d = np.abs(plaqs["mixed"] - plaqs["fp64"])
+    out["plaq_mixed_minus_fp64"] = {"max": float(d.max()), "mean": float(d.mean())}
+    out["plaq_fp64_by_size"] = {str(L): float(plaqs["fp64"][i * args.per_size:(i + 1) * args.per_size].mean())
+                                for i, L in enumerate((4, 6, 8, 12))}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    a = sub.add_parser("force-variants")
+    a.add_argument("--lattice", default="24,24,24,64")
+    a.add_argument("--reps", type=int, default=5)
+    b = sub.add_parser("force-profile")
+    b.add_argument("--lattice", default="24,24,24,48")
+    b.add_argument("--variants", default="0")
+    c = sub.add_parser("flow")
+    c.add_argument("--lattice", default="32,32,32,32")
+    c.add_argument("--steps", type=int, default=80)
+    c.add_argument("--every", type=int, default=4)
+    c.add_argument("--eps", type=float, default=0.05)
+    c.add_argument("--c1", type=float, default=0.0)
+    c.add_argument("--sigma", type=float, default=0.5)
+    c.add_argument("--n-step", type=int, default=1)
+    d = sub.add_parser("batch")
+    d.add_argument("--per-size", type=int, default=64)
+    d.add_argument("--n-step", type=int, default=10)
+    d.add_argument("--trajs", type=int, default=10)
+    d.add_argument("--warmup", type=int, default=3)
+    args = ap.parse_args()
+    {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch}[args.cmd](args)
+
+
+if __name__ == "__main__":
+    main()
