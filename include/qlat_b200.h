@@ -207,6 +207,14 @@ int qgb_batch_set_rand(qgb_batch* b, const uint32_t* rs, double sigma, int32_t n
 int qgb_batch_trajectory(qgb_batch* b, const uint32_t* rs_momentum, int32_t n_step, double md_time,
                          int32_t integrator, int32_t mixed, int32_t reunit_interval, int32_t use_graph,
                          double* delta_h);
+/* run_hmc_pure_gauge (hmc.pyx:190-216) for every chain at once: rs holds each
+ * chain's RngState, split by `traj`, by "set_rand_gauge_momentum" for the
+ * momenta and by "metropolis_accept" for the Metropolis draw (Python-API
+ * semantics, hmc.pyx:139-155); writes delta_h and the accept flags, and
+ * updates every accepted chain (every chain if always_accept). */
+int qgb_batch_run_hmc(qgb_batch* b, const uint32_t* rs, int32_t traj, int32_t n_step, double md_time,
+                      int32_t integrator, int32_t mixed, int32_t reunit_interval, int32_t always_accept,
+                      double* delta_h, int32_t* flags);
 /* Replace the state of every chain whose flag is non-zero by its proposal. */
 int qgb_batch_accept(qgb_batch* b, const int32_t* flags);
 /* gf_avg_plaq of every chain. */

@@ -85,6 +85,8 @@ SIGNATURES = {
     "qgb_batch_set_rand": [c_field, c_u32_p, ctypes.c_double, ctypes.c_int32],
     "qgb_batch_trajectory": [c_field, c_u32_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
                              ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+    "qgb_batch_run_hmc": [c_field, c_u32_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_dbl_p, c_i32_p],
     "qgb_batch_accept": [c_field, c_i32_p],
     "qgb_batch_plaq": [c_field, c_dbl_p],
     "qgb_batch_download_chain": [c_field, ctypes.c_int32, c_dbl_p],

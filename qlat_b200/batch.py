@@ -72,20 +72,17 @@ class ChainBatch:
         call("qgb_batch_accept", self._h, f)
 
     def run_hmc(self, traj, rs_list, n_step, md_time=1.0, *, integrator="leapfrog", precision="fp64",
-                reunit_interval=4, use_graph=True, is_always_accept=False):
+                reunit_interval=4, is_always_accept=False):
         """One trajectory of every chain with run_hmc_pure_gauge's RNG splits and
-        Metropolis (hmc.pyx:139-155, 190-216).  Returns (flags, delta_h)."""
-        from .hmc import metropolis_accept
-        rs_t = [r.split(f"{traj}") for r in rs_list]
-        dh = self.trajectory([r.split("set_rand_gauge_momentum") for r in rs_t], n_step, md_time,
-                             integrator=integrator, precision=precision, reunit_interval=reunit_interval,
-                             use_graph=use_graph)
-        flags = []
-        for c in range(self.n):
-            flag, _ = metropolis_accept(float(dh[c]), traj, rs_t[c].split("metropolis_accept"))
-            flags.append(flag or is_always_accept)
-        self.accept(flags)
-        return flags, dh
+        Metropolis (hmc.pyx:139-155, 190-216), all in the library.
+        Returns (flags, delta_h)."""
+        dh = np.zeros(self.n, dtype=np.float64)
+        flags = np.zeros(self.n, dtype=np.int32)
+        call("qgb_batch_run_hmc", self._h, self._rs_array(rs_list), int(traj), int(n_step), float(md_time),
+             INTEGRATORS[integrator], 1 if precision == "mixed" else 0, int(reunit_interval),
+             int(bool(is_always_accept)), dh.ctypes.data_as(_lib.c_dbl_p),
+             flags.ctypes.data_as(_lib.c_i32_p))
+        return [bool(f) for f in flags], dh
 
     def plaq(self) -> np.ndarray:
         out = np.zeros(self.n, dtype=np.float64)

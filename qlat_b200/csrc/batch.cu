@@ -13,6 +13,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <stdio.h>
+
 #include <map>
 #include <string>
 #include <tuple>
@@ -343,6 +345,43 @@ int qgb_batch_trajectory(qgb_batch* b, const uint32_t* rs_momentum, int32_t n_st
     const double h1 = b->h_sums[3 * n + c] + chain_action(ci, b->h_sums[4 * n + c], b->h_sums[5 * n + c]);
     delta_h[c] = h1 - h0;
   }
+  return QGB_OK;
+}
+
+int qgb_batch_run_hmc(qgb_batch* b, const uint32_t* rs, int32_t traj, int32_t n_step, double md_time,
+                      int32_t integrator, int32_t mixed, int32_t reunit_interval, int32_t always_accept,
+                      double* delta_h, int32_t* flags)
+{
+  if (!b || !rs || !delta_h || !flags) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_run_hmc: null argument");
+  // run_hmc_pure_gauge (hmc.pyx:190-216) for every chain: rs_c.split(traj), its
+  // "set_rand_gauge_momentum" split for the momenta, its "metropolis_accept"
+  // split for the Python-API Metropolis draw (hmc.pyx:139-155).
+  const int n = b->n;
+  std::vector<uint32_t> rs_t(24 * (size_t)n), rs_m(24 * (size_t)n);
+  char tbuf[32];
+  snprintf(tbuf, sizeof(tbuf), "%d", (int)traj);
+  for (int c = 0; c < n; ++c) {
+    if (!qgb::rng_host_split(&rs_t[24 * c], rs + 24 * c, tbuf) ||
+        !qgb::rng_host_split(&rs_m[24 * c], &rs_t[24 * c], "set_rand_gauge_momentum"))
+      return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_run_hmc: RngState split failed");
+  }
+  QB_RC(qgb_batch_trajectory(b, rs_m.data(), n_step, md_time, integrator, mixed, reunit_interval, 1, delta_h));
+  for (int c = 0; c < n; ++c) {
+    int flag = 0;
+    if (delta_h[c] <= 0.0) {
+      flag = 1;
+    } else {
+      uint32_t ra[24];
+      qgb::rng_host_split(ra, &rs_t[24 * c], "metropolis_accept");
+      const double u = qgb::rng_host_u_rand_gen(ra, 1.0, 0.0);
+      flag = u <= exp(-delta_h[c]) ? 1 : 0;
+    }
+    flags[c] = flag;
+    b->h_flags[c] = (flag || always_accept) ? 1 : 0;
+  }
+  QB_CUDA(cudaMemcpyAsync(b->d_flags, b->h_flags, b->n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  QB_CUDA(qgb::launch_accept_batch<double>(b->Vtot, b->n, b->d_offs, b->d_flags, b->gf, b->gf0, b->stream));
+  QB_CUDA(cudaStreamSynchronize(b->stream));
   return QGB_OK;
 }
 

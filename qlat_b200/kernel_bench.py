@@ -126,8 +126,10 @@ def batch(args):
     for prec in ("mixed", "fp64"):
         b = q.ChainBatch(sizes, betas)
         b.set_rand([r.split("gf-init") for r in rs], 1.0, 1)
+        # warm-up trajectories are always accepted (the reference's scripts do the
+        # same for their first trajectories, examples-py/hmc-pure-gauge.py)
         for t in range(1, args.warmup + 1):
-            b.run_hmc(t, rs, args.n_step, precision=prec)
+            b.run_hmc(t, rs, args.n_step, precision=prec, is_always_accept=True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         acc = 0
@@ -169,7 +171,7 @@ def main():
     d.add_argument("--per-size", type=int, default=64)
     d.add_argument("--n-step", type=int, default=10)
     d.add_argument("--trajs", type=int, default=10)
-    d.add_argument("--warmup", type=int, default=3)
+    d.add_argument("--warmup", type=int, default=10)
     args = ap.parse_args()
     {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch}[args.cmd](args)
 
