@@ -168,6 +168,31 @@ int qgb_gf_energy_density(const qgb_field* gf, double* out);
  * energy_list receives `steps` energy densities. */
 int qgb_gf_wilson_flow(qgb_field* gf, double flow_time, int32_t steps, double c1, double* energy_list);
 
+/* ---- flow adjoint (no counterpart in the reference) ---------------------- */
+
+/* Tangents and gradients are su(3) fields acting by left multiplication,
+ * U -> exp(s X) U; the gradient of L is sum_a (dL/domega_a) T_a in the basis of
+ * matrix-hmc.h:76-106 (tr T_a T_b = -2 delta_ab).  With this convention the
+ * gradient of the gauge action is -2 x set_gm_force.
+ *
+ * Vector-Jacobian product of `steps` RK3 flow steps of size epsilon
+ * (gf_wilson_flow_step, wilson-flow.cpp:29-50; Wilson flow, c1 = 0): given the
+ * cotangent at the flowed field, writes the cotangent at gf.  Forward states
+ * are checkpointed every `checkpoint_every` steps and recomputed. */
+int qgb_gf_wilson_flow_vjp(const qgb_field* gf, double epsilon, int32_t steps, double c1, int32_t checkpoint_every,
+                           const qgb_field* cotangent, qgb_field* grad);
+/* L = gf_hamilton_node(V_t, GaugeAction(beta, c1_loss)) of the flowed field
+ * V_t (steps RK3 steps of epsilon) and its gradient with respect to gf. */
+int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, double c1, int32_t checkpoint_every,
+                            double beta, double c1_loss, qgb_field* grad, double* loss);
+/* set_anti_hermitian_matrix_from_basis / set_basis_from_anti_hermitian_matrix
+ * (hmc.h:108-113, hmc.cpp:647-697): fc[x, m] = sum_a T_a basis[x, 8 m + a]. */
+int qgb_set_anti_hermitian_matrix_from_basis(qgb_field* fc, const qgb_field* basis);
+int qgb_set_basis_from_anti_hermitian_matrix(qgb_field* basis, const qgb_field* fc);
+/* out = dexp_{-omega}(lam) per link: the gradient with respect to omega of a
+ * function of exp(omega) U whose gradient at exp(omega) U is lam. */
+int qgb_su3_dexp_adjoint(qgb_field* out, const qgb_field* omega, const qgb_field* lam);
+
 /* ---- hot path: topology (qcd-topology.h, everything.pxd:531-535) --------- */
 
 /* clf_topology_field(topf, gf) (qcd.cpp:416-423, 608-619); topf: real, multiplicity 1. */

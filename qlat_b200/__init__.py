@@ -17,6 +17,9 @@ from .hmc import (gf_avg_plaq, gf_evolve, gf_hamilton, gf_hamilton_node, gf_sum_
                   metropolis_accept, metropolis_accept_cpp, run_hmc_evolve_pure_gauge, run_hmc_pure_gauge,
                   set_gm_force, set_rand_gauge_momentum, unitarize)
 from .batch import ChainBatch
+from .flow_adjoint import (FlowedWilsonAction, gf_flow_action, gf_flow_action_grad, gf_wilson_flow_vjp,
+                           run_flowed_hmc_pure_gauge, set_anti_hermitian_matrix_from_basis,
+                           set_basis_from_anti_hermitian_matrix)
 from .wilson_flow import (gf_energy_density, gf_energy_density_field, gf_energy_derivative_density_field,
                           gf_topology_clf, gf_topology_field_clf, gf_wilson_flow, gf_wilson_flow_force,
                           gf_wilson_flow_step)

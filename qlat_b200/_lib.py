@@ -67,6 +67,13 @@ SIGNATURES = {
     "qgb_gf_energy_density_field": [c_field, c_field],
     "qgb_gf_energy_density": [c_field, c_dbl_p],
     "qgb_gf_wilson_flow": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_double, c_dbl_p],
+    "qgb_gf_wilson_flow_vjp": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, c_field,
+                               c_field],
+    "qgb_gf_flow_action_grad": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                ctypes.c_double, ctypes.c_double, c_field, c_dbl_p],
+    "qgb_set_anti_hermitian_matrix_from_basis": [c_field, c_field],
+    "qgb_set_basis_from_anti_hermitian_matrix": [c_field, c_field],
+    "qgb_su3_dexp_adjoint": [c_field, c_field, c_field],
     "qgb_clf_topology_field": [c_field, c_field],
     "qgb_gf_topology_clf": [c_field, c_dbl_p],
     "qgb_prof_enable": [ctypes.c_int32],

@@ -383,6 +383,122 @@ int hamiltonian_slots(const qgb_field* gm, const qgb_field* gf, double c1, int s
 
 }  // namespace
 
+// One flow step through fused stage kernels: W -> T -> W -> T and a
+// buffer swap, so the field handle ends up owning the result.
+static int flow_step(qgb_field* gf, double eps, double c1, bool rk3)
+{
+  const Geo g = geo_of(gf);
+  void *T = nullptr, *Z = nullptr;
+  QGB_RC(get_scratch(gf->bytes, 21, &T));
+  QGB_RC(get_scratch(gf->bytes, 22, &Z));
+  auto stage = [&](const void* in, void* out, double a, double b, const void* zp, void* zo) -> int {
+    ForceArgs fa = fargs(in, out, 3.0, c1, eps);
+    fa.a = a;
+    fa.b = b;
+    fa.zp = zp;
+    fa.z = zo;
+    if (gf->prec == QGB_F64) return force<double>(g, qgb::FORCE_FLOW, fa);
+    return force<float>(g, qgb::FORCE_FLOW, fa);
+  };
+  if (rk3) {
+    // wilson-flow.cpp:29-50: Z0 = F/4; Z1 = 8/9 F - 17/9 Z0; Z2 = 3/4 F - Z1
+    QGB_RC(stage(gf->d, T, 0.25, 0.0, nullptr, Z));
+    QGB_RC(stage(T, gf->d, 8.0 / 9.0, -17.0 / 9.0, Z, Z));
+    QGB_RC(stage(gf->d, T, 0.75, -1.0, Z, nullptr));
+  } else {
+    QGB_RC(stage(gf->d, T, 1.0, 0.0, nullptr, nullptr));
+  }
+  // the handle takes the result buffer; the old one becomes the scratch
+  auto& v = g_ctx.scratch[std::make_pair(gf->bytes, 21)];
+  v[0] = gf->d;
+  gf->d = T;
+  return QGB_OK;
+}
+
+// ---- flow adjoint ------------------------------------------------------------
+
+// Pull a cotangent back through RK3 flow steps (adjoint.cu): checkpoints every
+// `every` steps, each segment recomputed forward, each step's three stages
+// recomputed with their Z fields, then pulled back stage by stage.
+template <typename R>
+static int flow_vjp_impl(const qgb_field* gf, double eps, int steps, int every, const void* lam_in, void* grad)
+{
+  const Geo g = geo_of(gf);
+  const size_t bytes = gf->bytes;
+  const int ncp = (steps + every - 1) / every;
+  std::vector<void*> cps(ncp), wst(every);
+  for (int i = 0; i < ncp; ++i) QGB_RC(get_scratch(bytes, 100 + i, &cps[i]));
+  for (int i = 0; i < every; ++i) QGB_RC(get_scratch(bytes, 1000 + i, &wst[i]));
+  void *W1, *W2, *Wx, *Z0, *Z1, *Z2, *lam, *laml, *mua, *mub;
+  QGB_RC(get_scratch(bytes, 41, &W1));
+  QGB_RC(get_scratch(bytes, 42, &W2));
+  QGB_RC(get_scratch(bytes, 43, &Wx));
+  QGB_RC(get_scratch(bytes, 44, &Z0));
+  QGB_RC(get_scratch(bytes, 45, &Z1));
+  QGB_RC(get_scratch(bytes, 46, &Z2));
+  QGB_RC(get_scratch(bytes, 47, &lam));
+  QGB_RC(get_scratch(bytes, 48, &laml));
+  QGB_RC(get_scratch(bytes, 49, &mua));
+  QGB_RC(get_scratch(bytes, 50, &mub));
+  auto stage = [&](const void* in, void* out, double a, double b, const void* zp, void* zo) -> int {
+    ForceArgs fa = fargs(in, out, 3.0, 0.0, eps);
+    fa.a = a;
+    fa.b = b;
+    fa.zp = zp;
+    fa.z = zo;
+    return force<R>(g, qgb::FORCE_FLOW, fa);
+  };
+  auto step = [&](const void* in, void* out) -> int {  // one RK3 step in -> out, Z0..Z2 kept
+    QGB_RC(stage(in, W1, 0.25, 0.0, nullptr, Z0));
+    QGB_RC(stage(W1, W2, 8.0 / 9.0, -17.0 / 9.0, Z0, Z1));
+    QGB_RC(stage(W2, out, 0.75, -1.0, Z1, Z2));
+    return QGB_OK;
+  };
+  // forward pass: checkpoints
+  QGB_TRY_CUDA(cudaMemcpyAsync(cps[0], gf->d, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  for (int c = 1; c < ncp; ++c) {
+    QGB_TRY_CUDA(cudaMemcpyAsync(Wx, cps[c - 1], bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    for (int j = 0; j < every; ++j) {
+      QGB_RC(step(Wx, wst[0]));
+      QGB_TRY_CUDA(cudaMemcpyAsync(Wx, wst[0], bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    }
+    QGB_TRY_CUDA(cudaMemcpyAsync(cps[c], Wx, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  }
+  QGB_TRY_CUDA(cudaMemcpyAsync(lam, lam_in, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  // backward pass
+  for (int c = ncp - 1; c >= 0; --c) {
+    const int s0 = c * every, s1 = (s0 + every < steps) ? s0 + every : steps;
+    QGB_TRY_CUDA(cudaMemcpyAsync(wst[0], cps[c], bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    for (int j = 1; j < s1 - s0; ++j) QGB_RC(step(wst[j - 1], wst[j]));
+    for (int j = s1 - s0 - 1; j >= 0; --j) {
+      QGB_RC(step(wst[j], Wx));  // stage fields of this step: wst[j], W1, W2 and Z0, Z1, Z2
+      {
+        Prof p("flow_adjoint", 6);
+        // stage 3: W3 = exp(eps Z2) W2, Z2 = 3/4 F(W2) - Z1
+        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z2, nullptr, 0.0, eps, mua, laml, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W2, mua, laml, lam, 3.0, 0.75, g_ctx.stream));
+        // stage 2: W2 = exp(eps Z1) W1, Z1 = 8/9 F(W1) - 17/9 Z0; carry -mu2 into Z1
+        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z1, mua, -1.0, eps, mub, laml, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W1, mub, laml, lam, 3.0, 8.0 / 9.0, g_ctx.stream));
+        // stage 1: W1 = exp(eps Z0) W0, Z0 = 1/4 F(W0); carry -17/9 mu1 into Z0
+        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z0, mub, -17.0 / 9.0, eps, mua, laml, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, wst[j], mua, laml, lam, 3.0, 0.25, g_ctx.stream));
+      }
+    }
+  }
+  QGB_TRY_CUDA(cudaMemcpyAsync(grad, lam, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  return QGB_OK;
+}
+
+static int check_vjp_args(const qgb_field* gf, const qgb_field* a, const char* what)
+{
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, what));
+  QGB_RC(check_field(a, QGB_KIND_COLOR_MATRIX, what));
+  QGB_CHECK(gf->mult == 4 && a->mult == 4 && same_geo(gf, a) && gf->prec == a->prec, QGB_ERR_MISMATCH,
+            std::string(what) + ": field mismatch");
+  return QGB_OK;
+}
+
 namespace qgb
 {
 // Lets the allocation-free entry point (noalloc.cu) report through qgb_last_error.
@@ -896,38 +1012,6 @@ int qgb_set_wilson_flow_z(qgb_field* z, const qgb_field* gf, double c1)
   return qgb_set_gm_force(z, gf, 3.0, c1);
 }
 
-// One flow step through fused stage kernels: W -> T -> W -> T and a
-// buffer swap, so the field handle ends up owning the result.
-static int flow_step(qgb_field* gf, double eps, double c1, bool rk3)
-{
-  const Geo g = geo_of(gf);
-  void *T = nullptr, *Z = nullptr;
-  QGB_RC(get_scratch(gf->bytes, 21, &T));
-  QGB_RC(get_scratch(gf->bytes, 22, &Z));
-  auto stage = [&](const void* in, void* out, double a, double b, const void* zp, void* zo) -> int {
-    ForceArgs fa = fargs(in, out, 3.0, c1, eps);
-    fa.a = a;
-    fa.b = b;
-    fa.zp = zp;
-    fa.z = zo;
-    if (gf->prec == QGB_F64) return force<double>(g, qgb::FORCE_FLOW, fa);
-    return force<float>(g, qgb::FORCE_FLOW, fa);
-  };
-  if (rk3) {
-    // wilson-flow.cpp:29-50: Z0 = F/4; Z1 = 8/9 F - 17/9 Z0; Z2 = 3/4 F - Z1
-    QGB_RC(stage(gf->d, T, 0.25, 0.0, nullptr, Z));
-    QGB_RC(stage(T, gf->d, 8.0 / 9.0, -17.0 / 9.0, Z, Z));
-    QGB_RC(stage(gf->d, T, 0.75, -1.0, Z, nullptr));
-  } else {
-    QGB_RC(stage(gf->d, T, 1.0, 0.0, nullptr, nullptr));
-  }
-  // the handle takes the result buffer; the old one becomes the scratch
-  auto& v = g_ctx.scratch[std::make_pair(gf->bytes, 21)];
-  v[0] = gf->d;
-  gf->d = T;
-  return QGB_OK;
-}
-
 int qgb_gf_wilson_flow_step(qgb_field* gf, double epsilon, double c1)
 {
   QGB_CTX();
@@ -1011,6 +1095,99 @@ int qgb_gf_topology_clf(const qgb_field* gf, double* out)
 }
 
 // ---- instrumentation -------------------------------------------------------
+
+int qgb_gf_wilson_flow_vjp(const qgb_field* gf, double epsilon, int32_t steps, double c1, int32_t checkpoint_every,
+                           const qgb_field* cotangent, qgb_field* grad)
+{
+  QGB_CTX();
+  QGB_RC(check_vjp_args(gf, cotangent, "qgb_gf_wilson_flow_vjp"));
+  QGB_RC(check_vjp_args(gf, grad, "qgb_gf_wilson_flow_vjp"));
+  QGB_CHECK(c1 == 0.0, QGB_ERR_INVALID_ARG, "qgb_gf_wilson_flow_vjp: only the Wilson flow (c1 = 0) has an adjoint");
+  QGB_CHECK(steps >= 0 && checkpoint_every >= 1, QGB_ERR_INVALID_ARG, "qgb_gf_wilson_flow_vjp: bad steps");
+  if (steps == 0) {
+    QGB_TRY_CUDA(cudaMemcpyAsync(grad->d, cotangent->d, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    return QGB_OK;
+  }
+  const int every = checkpoint_every < steps ? checkpoint_every : steps;
+  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, steps, every, cotangent->d, grad->d);
+  return flow_vjp_impl<float>(gf, epsilon, steps, every, cotangent->d, grad->d);
+}
+
+int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, double c1, int32_t checkpoint_every,
+                            double beta, double c1_loss, qgb_field* grad, double* loss)
+{
+  QGB_CTX();
+  QGB_RC(check_vjp_args(gf, grad, "qgb_gf_flow_action_grad"));
+  QGB_CHECK(c1 == 0.0, QGB_ERR_INVALID_ARG, "qgb_gf_flow_action_grad: only the Wilson flow (c1 = 0) has an adjoint");
+  QGB_CHECK(steps >= 0 && checkpoint_every >= 1, QGB_ERR_INVALID_ARG, "qgb_gf_flow_action_grad: bad steps");
+  const Geo g = geo_of(gf);
+  void *V = nullptr, *lamN = nullptr;
+  QGB_RC(get_scratch(gf->bytes, 61, &V));
+  QGB_RC(get_scratch(gf->bytes, 62, &lamN));
+  // flowed field V_t
+  QGB_TRY_CUDA(cudaMemcpyAsync(V, gf->d, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  qgb_field_s fv = *gf;
+  fv.d = V;
+  for (int i = 0; i < steps; ++i) QGB_RC(flow_step(&fv, epsilon, 0.0, true));
+  V = fv.d;  // flow_step hands the result buffer to the handle
+  // loss and its gradient at V_t: dL = -2 <F(V_t), X> in the su(3) pairing
+  QGB_RC(action_slot(&fv, c1_loss != 0.0, 0));
+  double r[2] = {0, 0};
+  QGB_RC(read_results(0, c1_loss != 0.0 ? 2 : 1, r));
+  if (loss) *loss = gf_hamilton_from(r[0], r[1], beta, c1_loss);
+  ForceArgs a = fargs(V, lamN, beta, c1_loss, 0.0);
+  if (gf->prec == QGB_F64) QGB_RC(force<double>(g, qgb::FORCE_SET, a));
+  else QGB_RC(force<float>(g, qgb::FORCE_SET, a));
+  const long n = n_reals(gf);
+  if (gf->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_axpby<double>(n, lamN, 0.0, nullptr, -2.0, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_axpby<float>(n, lamN, 0.0, nullptr, -2.0, g_ctx.stream));
+  // restore the scratch bookkeeping of the flowed buffer, then pull back
+  auto& v61 = g_ctx.scratch[std::make_pair(gf->bytes, 61)];
+  v61[0] = V;
+  if (steps == 0) {
+    QGB_TRY_CUDA(cudaMemcpyAsync(grad->d, lamN, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    return QGB_OK;
+  }
+  const int every = checkpoint_every < steps ? checkpoint_every : steps;
+  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, steps, every, lamN, grad->d);
+  return flow_vjp_impl<float>(gf, epsilon, steps, every, lamN, grad->d);
+}
+
+int qgb_set_anti_hermitian_matrix_from_basis(qgb_field* fc, const qgb_field* basis)
+{
+  QGB_CTX();
+  QGB_RC(check_field(fc, QGB_KIND_COLOR_MATRIX, "qgb_set_anti_hermitian_matrix_from_basis"));
+  QGB_RC(check_field(basis, QGB_KIND_REAL, "qgb_set_anti_hermitian_matrix_from_basis"));
+  QGB_CHECK(same_geo(fc, basis) && basis->mult == 8 * fc->mult && fc->prec == basis->prec, QGB_ERR_MISMATCH,
+            "qgb_set_anti_hermitian_matrix_from_basis: basis must have multiplicity 8 x that of fc");
+  if (fc->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_basis_to_matrix<double>(fc->V, fc->mult, basis->d, fc->d, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_basis_to_matrix<float>(fc->V, fc->mult, basis->d, fc->d, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_set_basis_from_anti_hermitian_matrix(qgb_field* basis, const qgb_field* fc)
+{
+  QGB_CTX();
+  QGB_RC(check_field(fc, QGB_KIND_COLOR_MATRIX, "qgb_set_basis_from_anti_hermitian_matrix"));
+  QGB_RC(check_field(basis, QGB_KIND_REAL, "qgb_set_basis_from_anti_hermitian_matrix"));
+  QGB_CHECK(same_geo(fc, basis) && basis->mult == 8 * fc->mult && fc->prec == basis->prec, QGB_ERR_MISMATCH,
+            "qgb_set_basis_from_anti_hermitian_matrix: basis must have multiplicity 8 x that of fc");
+  if (fc->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_matrix_to_basis<double>(fc->V, fc->mult, fc->d, basis->d, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_matrix_to_basis<float>(fc->V, fc->mult, fc->d, basis->d, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_su3_dexp_adjoint(qgb_field* out, const qgb_field* omega, const qgb_field* lam)
+{
+  QGB_CTX();
+  QGB_RC(check_vjp_args(omega, lam, "qgb_su3_dexp_adjoint"));
+  QGB_RC(check_vjp_args(omega, out, "qgb_su3_dexp_adjoint"));
+  if (omega->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_dexp_adjoint<double>(omega->V, omega->mult, omega->d, lam->d, out->d, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_dexp_adjoint<float>(omega->V, omega->mult, omega->d, lam->d, out->d, g_ctx.stream));
+  return QGB_OK;
+}
 
 int qgb_prof_enable(int32_t on)
 {

@@ -81,6 +81,20 @@ cudaError_t launch_finalize(const double* partials, int n_values, int blocks, do
 // results[out] = results[a] + results[b] - results[c] (delta H bookkeeping on the device)
 cudaError_t launch_combine(double* results, int out, int a, int b, int c, cudaStream_t st);
 
+// Flow adjoint (adjoint.cu).
+template <typename R>
+cudaError_t launch_force_vjp(const Geo& g, const void* U, const void* Y, const void* lam_local, void* lam_out,
+                             double beta, double a, cudaStream_t st);
+template <typename R>
+cudaError_t launch_flow_adj_local(long V, const void* lam, const void* Z, const void* mu_carry, double carry, double eps,
+                                  void* mu_out, void* lam_local, cudaStream_t st);
+template <typename R>
+cudaError_t launch_dexp_adjoint(long V, int m, const void* omega, const void* lam, void* out, cudaStream_t st);
+template <typename R>
+cudaError_t launch_basis_to_matrix(long V, int m, const void* basis, void* fc, cudaStream_t st);
+template <typename R>
+cudaError_t launch_matrix_to_basis(long V, int m, const void* fc, void* basis, cudaStream_t st);
+
 // Per-site RNG kernels; rs = 24 x u32 serialised RngState.
 template <typename R>
 cudaError_t launch_rand_momentum(const Geo& g, void* P, const uint32_t* rs24, double sigma,

@@ -9,6 +9,8 @@
         `every` steps, FP64 and FP32 storage; prints timings and the FP32 errors
     python -m qlat_b200.kernel_bench batch [--per-size 64] [--trajs 10]
         256 independent chains of 4^4 ... 12^4 advanced together (CUDA graph per trajectory)
+    python -m qlat_b200.kernel_bench flow-adjoint [--lattice 16,16,16,16] [--steps 40] [--every 8]
+        backward through the Wilson flow: timing, finite-difference check, flowed-field HMC
 
 Each command prints one JSON line.
 """
@@ -150,6 +152,67 @@ def batch(args):
     print(json.dumps(out))
 
 
+def flow_adjoint(args):
+    """Backward through `steps` Wilson-flow steps of eps on a seeded hot start
+    (scale sigma), loss = Wilson gauge action (beta) of the flowed field,
+    checkpoints every k steps: timing, the finite-difference check along
+    `dirs` random su(3) directions (h = 1e-4, 4-point, FP64), the zero-flow
+    identity, and `trajs` flowed-field HMC trajectories."""
+    import numpy as np
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    ts = _lattice(args.lattice)
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("b200-c4-adjoint").split("gf-init"), args.sigma, 1)
+    out = {"lattice": list(ts), "eps": args.eps, "steps": args.steps, "checkpoint_every": args.every,
+           "beta_loss": args.beta}
+    q.gf_flow_action_grad(gf, args.eps, args.steps, args.beta, checkpoint_every=args.every)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss, grad = q.gf_flow_action_grad(gf, args.eps, args.steps, args.beta, checkpoint_every=args.every)
+    torch.cuda.synchronize()
+    out["ms_forward_and_backward"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    q.gf_flow_action(gf, args.eps, args.steps, args.beta)
+    torch.cuda.synchronize()
+    out["ms_forward_only"] = 1e3 * (time.perf_counter() - t0)
+    G = np.asarray(grad)
+    rel = []
+    for k in range(args.dirs):
+        X = q.GaugeMomentum(gf.geo)
+        X.set_rand(q.RngState(f"c4-direction-{k}"), 1.0)
+        Xn = np.asarray(X)
+
+        def L(h):
+            u = gf.copy()
+            q.gf_evolve(u, X, h)
+            return q.gf_flow_action(u, args.eps, args.steps, args.beta)
+
+        h = 1e-4
+        fd = (8 * (L(h) - L(-h)) - (L(2 * h) - L(-2 * h))) / (12 * h)
+        an = float(-0.5 * np.einsum("smij,smji->", G, Xn).real)
+        rel.append(abs(fd - an) / abs(fd))
+    out["fd_max_rel_err"] = max(rel)
+    out["fd_median_rel_err"] = float(np.median(rel))
+    _, g0 = q.gf_flow_action_grad(gf, args.eps, 0, args.beta)
+    F = q.GaugeMomentum(gf.geo)
+    q.set_gm_force(F, gf, q.GaugeAction(args.beta, 0.0))
+    out["zero_flow_max_abs_diff_vs_minus2_force"] = float(np.abs(np.asarray(g0) + 2 * np.asarray(F)).max())
+    if args.trajs:
+        rs = q.RngState("b200-c4-flowed-hmc")
+        hmc = []
+        u = gf.copy()
+        t0 = time.perf_counter()
+        for t in range(1, args.trajs + 1):
+            flag, dh = q.run_flowed_hmc_pure_gauge(u, args.hmc_beta, t, rs, epsilon=args.eps, flow_steps=args.steps,
+                                                   n_step=args.hmc_steps, checkpoint_every=args.every)
+            hmc.append({"traj": t, "accept": bool(flag), "delta_h": dh, "plaq": u.plaq()})
+        out["flowed_hmc"] = {"beta": args.hmc_beta, "n_step": args.hmc_steps,
+                             "s_per_traj": (time.perf_counter() - t0) / args.trajs, "trajectories": hmc}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -172,8 +235,20 @@ def main():
     d.add_argument("--n-step", type=int, default=10)
     d.add_argument("--trajs", type=int, default=10)
     d.add_argument("--warmup", type=int, default=10)
+    e = sub.add_parser("flow-adjoint")
+    e.add_argument("--lattice", default="16,16,16,16")
+    e.add_argument("--eps", type=float, default=0.05)
+    e.add_argument("--steps", type=int, default=40)
+    e.add_argument("--every", type=int, default=8)
+    e.add_argument("--beta", type=float, default=5.8)
+    e.add_argument("--sigma", type=float, default=0.4)
+    e.add_argument("--dirs", type=int, default=16)
+    e.add_argument("--trajs", type=int, default=10)
+    e.add_argument("--hmc-beta", type=float, default=5.8)
+    e.add_argument("--hmc-steps", type=int, default=10)
     args = ap.parse_args()
-    {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch}[args.cmd](args)
+    {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch,
+     "flow-adjoint": flow_adjoint}[args.cmd](args)
 
 
 if __name__ == "__main__":
