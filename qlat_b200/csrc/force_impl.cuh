@@ -102,6 +102,139 @@ __device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g,
 }
 
 // ------------------------------------------------------------------------
+// staples with precomputed neighbour offsets
+//
+// The same sum as staple_sum_rt, evaluated with
+// - neighbour sites as the thread's own site plus per-direction offsets:
+//   site(x + a mu + b nu) = site(x) + D_mu(a) + D_nu(b) because mu != nu, with
+//   D_k(a) = (wrap(x_k + a) - x_k) * stride_k computed once per thread for mu
+//   and once per nu, instead of a 4-d wrap and index polynomial per load;
+// - the sign of e = s nu as a template parameter, so the conjugate transposes
+//   of the stored links fold into the products (mul_adj / adj_mul) instead of
+//   being selected at run time;
+// - hop(x) and U_mu(x+e), each used twice per direction, loaded once.
+// Offsets are 32-bit: the launcher uses this form only when 36 V < 2^31.
+
+template <typename R>
+struct LinkLd {
+  const Cx<R>* __restrict__ p;
+  int V;
+  __device__ __forceinline__ M3<R> operator()(int link, int site) const
+  {
+    const Cx<R>* q = p + (link * 9 * V + site);
+    M3<R> r;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + k * V);
+    return r;
+  }
+};
+
+__device__ __forceinline__ int sel4(const int (&v)[4], int k)
+{
+  return k == 0 ? v[0] : k == 1 ? v[1] : k == 2 ? v[2] : v[3];
+}
+
+__device__ __forceinline__ int nb_delta(int xk, int a, int L, int stride) { return (wrap(xk + a, L) - xk) * stride; }
+
+// One signed direction e = SG nu.  dn1 = D_nu(SG), dn2 = D_nu(2 SG).
+// Stored links: hop(x + a mu + b e) is U_nu at D_nu(b) (SG > 0) or U_nu^+ at
+// D_nu(-b-1) (SG < 0); back(x + a mu + b e) is U_nu^+ at D_nu(b-1) (SG > 0) or
+// U_nu at D_nu(-b) (SG < 0).  For SG < 0 the products of two adjoints are
+// formed as the adjoint of the reversed product ((H2 H)^+ = H^+ H2^+).
+// Order: rect1 and rect3 (ending with U_mu(x+e)) first, then B = hop(x)
+// U_mu(x+e) and rect2, so at most the accumulators S and T, hop(x), the chain
+// product, a loaded link and the product being formed are live.
+template <typename R, bool RECT, bool PACKED, int SG>
+__device__ __forceinline__ void staple_dir_fast(M3<R>& S, const LinkLd<R>& L, int s, int mu, int nu, int dmm1,
+                                                int dmp1, int dmp2, int dn1, int dn2, R cp, R cr)
+{
+  using O = Ops<R, PACKED>;
+  if (SG > 0) {
+    const M3<R> H = L(nu, s);  // hop(x)
+    if (!RECT) {
+      S = add_mul_adj(S, O::mul(H, L(mu, s + dn1)), L(nu, s + dmp1));
+      return;
+    }
+    M3<R> T;
+    {  // rect1: hop(x) hop(x+e) U_mu(x+2e) back(x+2e+mu)
+      M3<R> C = O::mul(H, L(nu, s + dn1));
+      C = O::mul(C, L(mu, s + dn2));
+      C = O::mul_adj(C, L(nu, s + dmp1 + dn1));
+      T = scale(cr, C);
+    }
+    M3<R> U01;
+    {  // rect3: U_mu(x-mu)^+ hop(x-mu) U_mu(x-mu+e) U_mu(x+e)
+      M3<R> C = O::adj_mul(L(mu, s + dmm1), L(nu, s + dmm1));
+      C = O::mul(C, L(mu, s + dmm1 + dn1));
+      U01 = L(mu, s + dn1);
+      C = O::mul(C, U01);
+      axpy(T, cr, C);
+    }
+    const M3<R> B = O::mul(H, U01);
+    axpy(T, cp, B);
+    {  // rect2: B U_mu(x+e+mu) back(x+e+2mu) U_mu(x+mu)^+
+      M3<R> C = O::mul(B, L(mu, s + dmp1 + dn1));
+      C = O::mul_adj(C, L(nu, s + dmp2));
+      C = O::mul_adj(C, L(mu, s + dmp1));
+      axpy(S, cr, C);
+    }
+    S = add_mul_adj(S, T, L(nu, s + dmp1));
+  } else {
+    const M3<R> H = L(nu, s + dn1);  // hop(x)^+
+    if (!RECT) {
+      S = O::add_mul(S, O::adj_mul(H, L(mu, s + dn1)), L(nu, s + dmp1 + dn1));
+      return;
+    }
+    M3<R> T;
+    {  // rect1: (hop(x+e)^+ hop(x)^+)^+ U_mu(x+2e) back(x+2e+mu)
+      M3<R> C = O::mul(L(nu, s + dn2), H);
+      C = O::adj_mul(C, L(mu, s + dn2));
+      C = O::mul(C, L(nu, s + dmp1 + dn2));
+      T = scale(cr, C);
+    }
+    M3<R> U01;
+    {  // rect3: (hop(x-mu)^+ U_mu(x-mu))^+ U_mu(x-mu+e) U_mu(x+e)
+      M3<R> C = O::mul(L(nu, s + dmm1 + dn1), L(mu, s + dmm1));
+      C = O::adj_mul(C, L(mu, s + dmm1 + dn1));
+      U01 = L(mu, s + dn1);
+      C = O::mul(C, U01);
+      axpy(T, cr, C);
+    }
+    const M3<R> B = O::adj_mul(H, U01);
+    axpy(T, cp, B);
+    {  // rect2
+      M3<R> C = O::mul(B, L(mu, s + dmp1 + dn1));
+      C = O::mul(C, L(nu, s + dmp2 + dn1));
+      C = O::mul_adj(C, L(mu, s + dmp1));
+      axpy(S, cr, C);
+    }
+    S = O::add_mul(S, T, L(nu, s + dmp1 + dn1));
+  }
+}
+
+template <typename R, bool RECT, bool PACKED>
+__device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, int s, int mu, R cp, R cr)
+{
+  const LinkLd<R> L{U, (int)g.V};
+  const Coord x = coord_of(g, s);
+  const int st[4] = {1, g.d[0], g.d[0] * g.d[1], g.d[0] * g.d[1] * g.d[2]};
+  const int xm = sel4(x.c, mu), Lm = sel4(g.d, mu), sm = sel4(st, mu);
+  const int dmm1 = nb_delta(xm, -1, Lm, sm), dmp1 = nb_delta(xm, 1, Lm, sm), dmp2 = nb_delta(xm, 2, Lm, sm);
+  M3<R> S = m3_zero<R>();
+#pragma unroll 1
+  for (int i = 1; i < 4; ++i) {
+    const int nu = (mu + i) & 3;
+    const int xn = sel4(x.c, nu), Ln = sel4(g.d, nu), sn = sel4(st, nu);
+    staple_dir_fast<R, RECT, PACKED, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
+                                        nb_delta(xn, 2, Ln, sn), cp, cr);
+    staple_dir_fast<R, RECT, PACKED, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
+                                         nb_delta(xn, -2, Ln, sn), cp, cr);
+  }
+  if (!RECT) S = scale(cp, S);
+  return S;
+}
+
+// ------------------------------------------------------------------------
 // force: F = TA(-beta/3 U_mu(x) S^+) (hmc.cpp:64-75) and its fused consumers
 
 // F = TA(-beta/3 U_mu(x) S^+) (hmc.cpp:64-75) at global site s of a field with
@@ -142,7 +275,10 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
 // links of a compact tile of BS/4 sites (4 x 2 x 2 x 2 for 128 threads,
 // 4 x 4 x 2 x 2 for 256), one warp-group per mu, so the four directions share
 // the tile's neighbourhood in L1.  MAP 1 needs the lattice extents to be
-// multiples of the tile; otherwise the launcher uses MAP 0.
+// multiples of the tile; otherwise the launcher uses MAP 0.  MAP 2 is the
+// linear mapping of MAP 0 with the staple_sum_fast evaluation (per-thread
+// neighbour offsets, sign-specialised directions); it needs 36 V < 2^31 and
+// SPLIT = 1, otherwise the launcher uses MAP 0.
 struct ForceVariant {
   int bs, minb, split, packed, map;
 };
@@ -150,16 +286,17 @@ struct ForceVariant {
   X(0, 128, 1, 1, 0, 0)       \
   X(1, 256, 1, 1, 0, 0)       \
   X(2, 128, 3, 1, 0, 0)       \
-  X(3, 128, 4, 1, 0, 0)       \
-  X(4, 128, 5, 1, 0, 0)       \
-  X(5, 128, 1, 2, 0, 0)       \
-  X(6, 128, 1, 1, 1, 0)       \
-  X(7, 128, 1, 1, 0, 1)       \
-  X(8, 128, 3, 1, 0, 1)       \
-  X(9, 128, 4, 1, 0, 1)       \
-  X(10, 256, 1, 1, 0, 1)      \
-  X(11, 256, 2, 1, 0, 1)
-static const int N_FORCE_VARIANTS = 12;
+  X(3, 128, 1, 2, 0, 0)       \
+  X(4, 128, 1, 1, 1, 0)       \
+  X(5, 128, 1, 1, 0, 1)       \
+  X(6, 256, 1, 1, 0, 1)       \
+  X(7, 128, 1, 1, 0, 2)       \
+  X(8, 256, 1, 1, 0, 2)       \
+  X(9, 64, 1, 1, 0, 2)        \
+  X(10, 128, 3, 1, 0, 2)      \
+  X(11, 128, 4, 1, 0, 2)      \
+  X(12, 128, 1, 1, 1, 2)
+static const int N_FORCE_VARIANTS = 13;
 
 template <int BS>
 struct Tile {
@@ -170,6 +307,15 @@ struct Tile {
 template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, bool PACKED, int MAP>
 __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 {
+  const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
+  if constexpr (MAP == 2) {
+    const long t = (long)blockIdx.x * BS + threadIdx.x;
+    if (t >= g.V) return;
+    const int mu = blockIdx.y;
+    const M3<R> S = staple_sum_fast<R, RECT, PACKED>((const Cx<R>*)a.U, g, (int)t, mu, cp, cr);
+    force_epilogue<R, MODE>(a, CField<R>{(const Cx<R>*)a.U, g.V}, g.V, t, mu, S, a.beta);
+    return;
+  }
   long s0;
   int h, mu;
   if (MAP == 0) {
@@ -202,7 +348,6 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
   const long s = valid ? s0 : g.V - 1;
   const CField<R> U{(const Cx<R>*)a.U, g.V};
   const Coord x = coord_of(g, s);
-  const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
   M3<R> S = staple_sum_rt<R, RECT, PACKED>(U, g, x, mu, cp, cr, h * (6 / SPLIT), (h + 1) * (6 / SPLIT));
   if (SPLIT == 2) {
 #pragma unroll
@@ -222,11 +367,13 @@ cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cud
   const bool tiled = MAP == 1 && SPLIT == 1 && g.d[0] % TL::tx == 0 && g.d[1] % TL::ty == 0 &&
                      g.d[2] % TL::tz == 0 && g.d[3] % TL::tt == 0;
   if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
+  const bool fast = MAP == 2 && SPLIT == 1 && g.off == 0 && g.V * 36 < 2147483647L;
+  if (MAP == 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
   dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
   const bool rect = a.c1 != 0.0;
 #define QGB_LAUNCH(M)                                                                                  \
-  if (rect) k_force<R, M, true, BS, MINB, SPLIT, PACKED, (MAP == 1 ? 1 : 0)><<<grid, BS, 0, st>>>(g, a); \
-  else k_force<R, M, false, BS, MINB, SPLIT, PACKED, (MAP == 1 ? 1 : 0)><<<grid, BS, 0, st>>>(g, a);
+  if (rect) k_force<R, M, true, BS, MINB, SPLIT, PACKED, MAP><<<grid, BS, 0, st>>>(g, a); \
+  else k_force<R, M, false, BS, MINB, SPLIT, PACKED, MAP><<<grid, BS, 0, st>>>(g, a);
   switch (mode) {
     case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
     case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;

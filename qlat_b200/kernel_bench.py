@@ -157,7 +157,8 @@ def flow_adjoint(args):
     (scale sigma), loss = Wilson gauge action (beta) of the flowed field,
     checkpoints every k steps: timing, the finite-difference check along
     `dirs` random su(3) directions (h = 1e-4, 4-point, FP64), the zero-flow
-    identity, and `trajs` flowed-field HMC trajectories."""
+    identity, and `trajs` flowed-field HMC trajectories (flow time
+    eps * hmc_flow_steps) after `hmc_warmup` ordinary Wilson HMC trajectories."""
     import numpy as np
     import torch
     import qlat_b200 as q
@@ -167,7 +168,9 @@ def flow_adjoint(args):
     gf.set_rand(q.RngState("b200-c4-adjoint").split("gf-init"), args.sigma, 1)
     out = {"lattice": list(ts), "eps": args.eps, "steps": args.steps, "checkpoint_every": args.every,
            "beta_loss": args.beta}
-    q.gf_flow_action_grad(gf, args.eps, args.steps, args.beta, checkpoint_every=args.every)  # warm-up
+    # warm-up of both paths, then wall-clock timing of each (the calls synchronise)
+    q.gf_flow_action_grad(gf, args.eps, args.steps, args.beta, checkpoint_every=args.every)
+    q.gf_flow_action(gf, args.eps, args.steps, args.beta)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     loss, grad = q.gf_flow_action_grad(gf, args.eps, args.steps, args.beta, checkpoint_every=args.every)
@@ -200,15 +203,34 @@ def flow_adjoint(args):
     q.set_gm_force(F, gf, q.GaugeAction(args.beta, 0.0))
     out["zero_flow_max_abs_diff_vs_minus2_force"] = float(np.abs(np.asarray(g0) + 2 * np.asarray(F)).max())
     if args.trajs:
+        # flowed-field HMC: thermalise with ordinary Wilson HMC, then trajectories
+        # whose action is the Wilson action of the field flowed to
+        # t = eps * hmc_flow_steps; the energy error of one trajectory at n and 2n
+        # steps from the same start checks the dt^2 scaling of the integrator.
         rs = q.RngState("b200-c4-flowed-hmc")
-        hmc = []
         u = gf.copy()
+        ga = q.GaugeAction(args.hmc_beta, 0.0)
+        for t in range(1, args.hmc_warmup + 1):
+            q.run_hmc_pure_gauge(u, ga, t, rs.split("thermalise"), n_step=args.hmc_steps, integrator="leapfrog",
+                                 is_always_accept=t <= args.hmc_warmup // 2)
+        dh_n = []
+        for n in (args.hmc_steps, 2 * args.hmc_steps):
+            _, d = q.run_flowed_hmc_pure_gauge(u.copy(), args.hmc_beta, 0, rs.split("dt-check"), epsilon=args.eps,
+                                               flow_steps=args.hmc_flow_steps, n_step=n, checkpoint_every=args.every)
+            dh_n.append(d)
+        hmc = []
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         for t in range(1, args.trajs + 1):
-            flag, dh = q.run_flowed_hmc_pure_gauge(u, args.hmc_beta, t, rs, epsilon=args.eps, flow_steps=args.steps,
-                                                   n_step=args.hmc_steps, checkpoint_every=args.every)
+            flag, dh = q.run_flowed_hmc_pure_gauge(u, args.hmc_beta, t, rs, epsilon=args.eps,
+                                                   flow_steps=args.hmc_flow_steps, n_step=args.hmc_steps,
+                                                   checkpoint_every=args.every)
             hmc.append({"traj": t, "accept": bool(flag), "delta_h": dh, "plaq": u.plaq()})
-        out["flowed_hmc"] = {"beta": args.hmc_beta, "n_step": args.hmc_steps,
+        torch.cuda.synchronize()
+        out["flowed_hmc"] = {"beta": args.hmc_beta, "flow_t": args.eps * args.hmc_flow_steps,
+                             "n_step": args.hmc_steps, "thermalisation_trajs": args.hmc_warmup,
+                             "delta_h_n_and_2n": dh_n, "delta_h_ratio": dh_n[0] / dh_n[1] if dh_n[1] else None,
+                             "accept_rate": sum(h["accept"] for h in hmc) / len(hmc),
                              "s_per_traj": (time.perf_counter() - t0) / args.trajs, "trajectories": hmc}
     print(json.dumps(out))
 
@@ -245,7 +267,9 @@ def main():
     e.add_argument("--dirs", type=int, default=16)
     e.add_argument("--trajs", type=int, default=10)
     e.add_argument("--hmc-beta", type=float, default=5.8)
-    e.add_argument("--hmc-steps", type=int, default=10)
+    e.add_argument("--hmc-steps", type=int, default=20)
+    e.add_argument("--hmc-flow-steps", type=int, default=2)
+    e.add_argument("--hmc-warmup", type=int, default=10)
     args = ap.parse_args()
     {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch,
      "flow-adjoint": flow_adjoint}[args.cmd](args)
