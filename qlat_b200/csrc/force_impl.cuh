@@ -144,6 +144,76 @@ __device__ __forceinline__ int nb_delta(int xk, int a, int L, int stride) { retu
 // Order: rect1 and rect3 (ending with U_mu(x+e)) first, then B = hop(x)
 // U_mu(x+e) and rect2, so at most the accumulators S and T, hop(x), the chain
 // product, a loaded link and the product being formed are live.
+// TWO: carry the SU(3)-valued chains as two rows (mul2 / complete in
+// su3.cuh): 924 instead of 1188 multiply-adds per direction.  Used for FP32
+// only; FP64 keeps full products, identical in structure to the reference's.
+template <typename R, bool RECT, bool PACKED, int SG>
+__device__ __forceinline__ void staple_dir_two_row(M3<R>& S, const LinkLd<R>& L, int s, int mu, int nu, int dmm1,
+                                                   int dmp1, int dmp2, int dn1, int dn2, R cp, R cr)
+{
+  if (SG > 0) {
+    const M3<R> H = L(nu, s);
+    if (!RECT) {
+      S = add_mul_adj(S, complete(mul2(H, L(mu, s + dn1))), L(nu, s + dmp1));
+      return;
+    }
+    M3<R> T;
+    {
+      M32<R> C = mul2(H, L(nu, s + dn1));
+      C = mul2(C, L(mu, s + dn2));
+      C = mul2_adj(C, L(nu, s + dmp1 + dn1));
+      T = scale(cr, complete(C));
+    }
+    M3<R> U01;
+    {
+      M32<R> C = adj_mul2(L(mu, s + dmm1), L(nu, s + dmm1));
+      C = mul2(C, L(mu, s + dmm1 + dn1));
+      U01 = L(mu, s + dn1);
+      C = mul2(C, U01);
+      axpy(T, cr, complete(C));
+    }
+    const M32<R> B2 = mul2(H, U01);
+    axpy(T, cp, complete(B2));
+    {
+      M32<R> C = mul2(B2, L(mu, s + dmp1 + dn1));
+      C = mul2_adj(C, L(nu, s + dmp2));
+      C = mul2_adj(C, L(mu, s + dmp1));
+      axpy(S, cr, complete(C));
+    }
+    S = add_mul_adj(S, T, L(nu, s + dmp1));
+  } else {
+    const M3<R> H = L(nu, s + dn1);
+    if (!RECT) {
+      S = add_mul(S, complete(adj_mul2(H, L(mu, s + dn1))), L(nu, s + dmp1 + dn1));
+      return;
+    }
+    M3<R> T;
+    {
+      const M3<R> P = complete(mul2(L(nu, s + dn2), H));
+      M32<R> C = adj_mul2(P, L(mu, s + dn2));
+      C = mul2(C, L(nu, s + dmp1 + dn2));
+      T = scale(cr, complete(C));
+    }
+    M3<R> U01;
+    {
+      const M3<R> P = complete(mul2(L(nu, s + dmm1 + dn1), L(mu, s + dmm1)));
+      M32<R> C = adj_mul2(P, L(mu, s + dmm1 + dn1));
+      U01 = L(mu, s + dn1);
+      C = mul2(C, U01);
+      axpy(T, cr, complete(C));
+    }
+    const M32<R> B2 = adj_mul2(H, U01);
+    axpy(T, cp, complete(B2));
+    {
+      M32<R> C = mul2(B2, L(mu, s + dmp1 + dn1));
+      C = mul2(C, L(nu, s + dmp2 + dn1));
+      C = mul2_adj(C, L(mu, s + dmp1));
+      axpy(S, cr, complete(C));
+    }
+    S = add_mul(S, T, L(nu, s + dmp1 + dn1));
+  }
+}
+
 template <typename R, bool RECT, bool PACKED, int SG>
 __device__ __forceinline__ void staple_dir_fast(M3<R>& S, const LinkLd<R>& L, int s, int mu, int nu, int dmm1,
                                                 int dmp1, int dmp2, int dn1, int dn2, R cp, R cr)
@@ -212,7 +282,7 @@ __device__ __forceinline__ void staple_dir_fast(M3<R>& S, const LinkLd<R>& L, in
   }
 }
 
-template <typename R, bool RECT, bool PACKED>
+template <typename R, bool RECT, bool PACKED, bool TWO>
 __device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, int s, int mu, R cp, R cr)
 {
   const LinkLd<R> L{U, (int)g.V};
@@ -225,10 +295,17 @@ __device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, i
   for (int i = 1; i < 4; ++i) {
     const int nu = (mu + i) & 3;
     const int xn = sel4(x.c, nu), Ln = sel4(g.d, nu), sn = sel4(st, nu);
-    staple_dir_fast<R, RECT, PACKED, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
-                                        nb_delta(xn, 2, Ln, sn), cp, cr);
-    staple_dir_fast<R, RECT, PACKED, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
-                                         nb_delta(xn, -2, Ln, sn), cp, cr);
+    if constexpr (TWO) {
+      staple_dir_two_row<R, RECT, PACKED, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
+                                             nb_delta(xn, 2, Ln, sn), cp, cr);
+      staple_dir_two_row<R, RECT, PACKED, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
+                                              nb_delta(xn, -2, Ln, sn), cp, cr);
+    } else {
+      staple_dir_fast<R, RECT, PACKED, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
+                                          nb_delta(xn, 2, Ln, sn), cp, cr);
+      staple_dir_fast<R, RECT, PACKED, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
+                                           nb_delta(xn, -2, Ln, sn), cp, cr);
+    }
   }
   if (!RECT) S = scale(cp, S);
   return S;
@@ -278,7 +355,8 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
 // multiples of the tile; otherwise the launcher uses MAP 0.  MAP 2 is the
 // linear mapping of MAP 0 with the staple_sum_fast evaluation (per-thread
 // neighbour offsets, sign-specialised directions); it needs 36 V < 2^31 and
-// SPLIT = 1, otherwise the launcher uses MAP 0.
+// SPLIT = 1, otherwise the launcher uses MAP 0.  MAP 3 is MAP 2 with the
+// two-row SU(3) chains (FP32; FP64 runs MAP 2).
 struct ForceVariant {
   int bs, minb, split, packed, map;
 };
@@ -295,8 +373,11 @@ struct ForceVariant {
   X(9, 64, 1, 1, 0, 2)        \
   X(10, 128, 3, 1, 0, 2)      \
   X(11, 128, 4, 1, 0, 2)      \
-  X(12, 128, 1, 1, 1, 2)
-static const int N_FORCE_VARIANTS = 13;
+  X(12, 128, 1, 1, 1, 2)      \
+  X(13, 128, 1, 1, 0, 3)      \
+  X(14, 256, 1, 1, 0, 3)      \
+  X(15, 128, 3, 1, 0, 3)
+static const int N_FORCE_VARIANTS = 16;
 
 template <int BS>
 struct Tile {
@@ -308,11 +389,11 @@ template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, bool PAC
 __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 {
   const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
-  if constexpr (MAP == 2) {
+  if constexpr (MAP >= 2) {
     const long t = (long)blockIdx.x * BS + threadIdx.x;
     if (t >= g.V) return;
     const int mu = blockIdx.y;
-    const M3<R> S = staple_sum_fast<R, RECT, PACKED>((const Cx<R>*)a.U, g, (int)t, mu, cp, cr);
+    const M3<R> S = staple_sum_fast<R, RECT, PACKED, MAP == 3>((const Cx<R>*)a.U, g, (int)t, mu, cp, cr);
     force_epilogue<R, MODE>(a, CField<R>{(const Cx<R>*)a.U, g.V}, g.V, t, mu, S, a.beta);
     return;
   }
@@ -363,12 +444,15 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 template <typename R, int BS, int MINB, int SPLIT, bool PACKED, int MAP>
 cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
+  if constexpr (MAP == 3 && sizeof(R) == 8) {
+    return launch_force_v<R, BS, MINB, SPLIT, PACKED, 2>(g, mode, a, st);
+  } else {
   using TL = Tile<BS>;
   const bool tiled = MAP == 1 && SPLIT == 1 && g.d[0] % TL::tx == 0 && g.d[1] % TL::ty == 0 &&
                      g.d[2] % TL::tz == 0 && g.d[3] % TL::tt == 0;
   if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
-  const bool fast = MAP == 2 && SPLIT == 1 && g.off == 0 && g.V * 36 < 2147483647L;
-  if (MAP == 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
+  const bool fast = MAP >= 2 && SPLIT == 1 && g.off == 0 && g.V * 36 < 2147483647L;
+  if (MAP >= 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
   dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
   const bool rect = a.c1 != 0.0;
 #define QGB_LAUNCH(M)                                                                                  \
@@ -382,6 +466,7 @@ cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cud
   }
 #undef QGB_LAUNCH
   return cudaGetLastError();
+  }
 }
 
 template <typename R>

@@ -445,6 +445,122 @@ QGB_HD double neg_half_tr_square(const M3<R>& m)
          p17 * p17 * 0.75;
 }
 
+// ---- two-row products of SU(3) matrices -------------------------------------
+// For U in SU(3) the third row is conj(row0 x row1).  Rows 0 and 1 of a
+// product A B depend only on rows 0 and 1 of A, so a chain of SU(3) products
+// can carry two rows (18 complex multiply-adds per product instead of 27) and
+// rebuild the third row once at the end (complete: 24 FMAs).  Exact for exact
+// SU(3) factors; for links that are unitary to rounding the difference from
+// the full product is of that rounding size.
+
+template <typename R>
+struct M32 {
+  Cx<R> e[6];  // rows 0 and 1, row-major
+};
+
+// rows 0, 1 of a b, with a given by its first two rows (the first 6 entries)
+template <typename R, typename A>
+QGB_HD M32<R> mul2(const A& a, const M3<R>& b)
+{
+  M32<R> c;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = a.e[3 * i].re * b.e[j].re;
+      R im = a.e[3 * i].re * b.e[j].im;
+      re = fma(-a.e[3 * i].im, b.e[j].im, re);
+      im = fma(a.e[3 * i].im, b.e[j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; ++k) {
+        re = fma(a.e[3 * i + k].re, b.e[3 * k + j].re, re);
+        re = fma(-a.e[3 * i + k].im, b.e[3 * k + j].im, re);
+        im = fma(a.e[3 * i + k].re, b.e[3 * k + j].im, im);
+        im = fma(a.e[3 * i + k].im, b.e[3 * k + j].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// rows 0, 1 of a b^dagger
+template <typename R, typename A>
+QGB_HD M32<R> mul2_adj(const A& a, const M3<R>& b)
+{
+  M32<R> c;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = a.e[3 * i].re * b.e[3 * j].re;
+      R im = -a.e[3 * i].re * b.e[3 * j].im;
+      re = fma(a.e[3 * i].im, b.e[3 * j].im, re);
+      im = fma(a.e[3 * i].im, b.e[3 * j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; ++k) {
+        re = fma(a.e[3 * i + k].re, b.e[3 * j + k].re, re);
+        re = fma(a.e[3 * i + k].im, b.e[3 * j + k].im, re);
+        im = fma(-a.e[3 * i + k].re, b.e[3 * j + k].im, im);
+        im = fma(a.e[3 * i + k].im, b.e[3 * j + k].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// rows 0, 1 of a^dagger b (needs all of a)
+template <typename R>
+QGB_HD M32<R> adj_mul2(const M3<R>& a, const M3<R>& b)
+{
+  M32<R> c;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      R re = a.e[i].re * b.e[j].re;
+      R im = a.e[i].re * b.e[j].im;
+      re = fma(a.e[i].im, b.e[j].im, re);
+      im = fma(-a.e[i].im, b.e[j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; ++k) {
+        re = fma(a.e[3 * k + i].re, b.e[3 * k + j].re, re);
+        re = fma(a.e[3 * k + i].im, b.e[3 * k + j].im, re);
+        im = fma(a.e[3 * k + i].re, b.e[3 * k + j].im, im);
+        im = fma(-a.e[3 * k + i].im, b.e[3 * k + j].re, im);
+      }
+      c.e[3 * i + j] = cx<R>(re, im);
+    }
+  }
+  return c;
+}
+
+// the SU(3) matrix with rows 0, 1 of a and row 2 = conj(row0 x row1)
+template <typename R>
+QGB_HD M3<R> complete(const M32<R>& a)
+{
+  M3<R> m;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) m.e[k] = a.e[k];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const Cx<R> u1 = a.e[(j + 1) % 3], u2 = a.e[(j + 2) % 3];
+    const Cx<R> v1 = a.e[3 + (j + 1) % 3], v2 = a.e[3 + (j + 2) % 3];
+    // conj(u1 v2 - u2 v1)
+    R re = u1.re * v2.re;
+    re = fma(-u1.im, v2.im, re);
+    re = fma(-u2.re, v1.re, re);
+    re = fma(u2.im, v1.im, re);
+    R im = -u1.re * v2.im;
+    im = fma(-u1.im, v2.re, im);
+    im = fma(u2.re, v1.im, im);
+    im = fma(u2.im, v1.re, im);
+    m.e[6 + j] = cx<R>(re, im);
+  }
+  return m;
+}
+
 // Gram-Schmidt projection onto SU(3) (matrix-hmc.h:11-74): normalise row 1,
 // orthogonalise and normalise row 2, row 3 = conj(row1 x row2).  The
 // arithmetic type C may be wider than the storage type (FP64 arithmetic on
