@@ -258,7 +258,7 @@ def our_arm(args):
     ms_mixed, dh_mixed, fl_mixed, launches = timed(args.steps, "mixed", traj + 1, prof=True)
     traj += args.steps
     clk = clocks.stop()
-    prof = {k: q.prof_get(k) for k in ("force_update", "force_evolve", "evolve", "reduce", "rng", "convert",
+    prof = {k: q.prof_get(k) for k in ("force_update_evolve", "force_evolve", "evolve", "reduce", "rng", "convert",
                                           "unitarize")}
     ms_fp64, dh_fp64, fl_fp64, _ = timed(args.steps, "fp64", traj + 1)
     traj += args.steps
@@ -312,12 +312,16 @@ def our_arm(args):
     except Exception:
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    # dominant kernel: the fused force + momentum update (FP32, Iwasaki):
-    # reads U (288 B/site) and P (288 B/site), writes P (288 B/site)
-    t_fu, n_fu = prof["force_update"]
-    bytes_fu = 864.0 * V
+    # dominant kernel: the force-gradient step's fused force + momentum update +
+    # link update (FP32, Iwasaki): reads U' (288 B/site), P and U (288 B/site
+    # each), writes P and U (288 B/site each)
+    t_fu, n_fu = prof["force_update_evolve"]
+    bytes_fu = 1440.0 * V
     achieved = bytes_fu / (t_fu / n_fu / 1e3) / 1e9 if n_fu else None
-    flops_site = 4 * (6 * 11 + 1) * 198.0  # matrix products per link x flops per product
+    # flops of the staple sum + force counted as 67 full SU(3) products per link
+    # at 198 flop each (the FP32 kernel carries link chains as two rows and
+    # does fewer)
+    flops_site = 4 * (6 * 11 + 1) * 198.0
     tflops = flops_site * V / (t_fu / n_fu / 1e3) / 1e12 if n_fu else None
     traffic = None
     tf_path = os.path.join(ROOT, "profiles", "force_update_traffic.json")
@@ -341,7 +345,8 @@ def our_arm(args):
                     "check_same_start_fp64": dh_chk64, "check_same_start_mixed": dh_chkmx,
                     "check_plaq_fp64": plaq_64, "check_plaq_mixed": plaq_mx,
                     "accept_rate_mixed": sum(fl_mixed) / len(fl_mixed)},
-        "roofline": {"kernel": "force_update (FP32 Iwasaki force fused with P += dt F)", "bound": "hbm",
+        "roofline": {"kernel": "force_update_evolve (FP32 Iwasaki force fused with P += dt F and U = exp(eps P) U)",
+                     "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",

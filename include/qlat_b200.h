@@ -252,13 +252,16 @@ int qgb_batch_upload_chain(qgb_batch* b, int32_t chain, const double* host);
 
 /* The force kernels (set_gm_force and its fused HMC / flow consumers) exist
  * in several launch shapes: threads per block, a register cap through the
- * minimum resident blocks per SM, one or two threads per link, packed FP32
- * FMAs, and the site mapping (0: consecutive sites, one mu per block; 1: each
- * block takes the four links of a compact 4-d tile).  The shape is chosen per
- * (precision, rect): by hand, or by timing them all on a given gauge field. */
+ * minimum resident blocks per SM, one or two threads per link, and the site
+ * mapping and staple evaluation (0: consecutive sites, one mu per block; 1:
+ * each block takes the four links of a compact 4-d tile; 2: as 0 with
+ * per-thread neighbour offsets and sign-specialised staple directions; 3: as 2
+ * with SU(3) link chains carried as two rows, FP32 only -- FP64 runs 2).  The
+ * shape is chosen per (precision, rect): by hand, or by timing them all on a
+ * given gauge field. */
 int qgb_force_variant_count(int32_t* n);
 int qgb_force_variant_info(int32_t variant, int32_t* block_size, int32_t* min_blocks, int32_t* threads_per_link,
-                           int32_t* packed_fp32, int32_t* site_map);
+                           int32_t* site_map);
 int qgb_force_set_variant(int32_t precision, int32_t rect, int32_t variant);
 int qgb_force_get_variant(int32_t precision, int32_t rect, int32_t* variant);
 /* Time every variant (force + momentum update, `reps` launches each) on gf

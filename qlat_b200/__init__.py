@@ -77,17 +77,17 @@ def set_device(device: int):
 
 def force_variants():
     """The force-kernel launch shapes: list of dicts (block_size, min_blocks,
-    threads_per_link, packed_fp32, site_map)."""
+    threads_per_link, site_map)."""
     import ctypes
     from ._lib import call
     n = ctypes.c_int32()
     call("qgb_force_variant_count", ctypes.byref(n))
     out = []
     for v in range(n.value):
-        a = [ctypes.c_int32() for _ in range(5)]
+        a = [ctypes.c_int32() for _ in range(4)]
         call("qgb_force_variant_info", v, *[ctypes.byref(x) for x in a])
         out.append(dict(block_size=a[0].value, min_blocks=a[1].value, threads_per_link=a[2].value,
-                        packed_fp32=a[3].value, site_map=a[4].value))
+                        site_map=a[3].value))
     return out
 
 

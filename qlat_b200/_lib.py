@@ -80,7 +80,7 @@ SIGNATURES = {
     "qgb_prof_reset": [],
     "qgb_prof_get": [ctypes.c_char_p, c_dbl_p, c_i64_p],
     "qgb_force_variant_count": [c_i32_p],
-    "qgb_force_variant_info": [ctypes.c_int32, c_i32_p, c_i32_p, c_i32_p, c_i32_p, c_i32_p],
+    "qgb_force_variant_info": [ctypes.c_int32, c_i32_p, c_i32_p, c_i32_p, c_i32_p],
     "qgb_force_set_variant": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "qgb_force_get_variant": [ctypes.c_int32, ctypes.c_int32, c_i32_p],
     "qgb_autotune_force": [c_field, ctypes.c_double, ctypes.c_int32, c_i32_p, c_dbl_p],

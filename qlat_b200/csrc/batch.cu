@@ -121,14 +121,16 @@ int batch_md(qgb_batch_s* b, void* gf, void* gm, void* tmp, int n_step, double m
     const double fg_dt = 4.0 * ttheta / dt;
     QB_RC(batch_evolve<R>(b, gf, gm, lam * dt, unit_each));
     for (int i = 0; i < n_step; ++i) {
+      const bool reunit = reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step;
       for (int half = 0; half < 2; ++half) {
         QB_RC(batch_force<R>(b, qgb::FORCE_EVOLVE, bargs(gf, tmp, fg_dt, unit_each)));
-        QB_RC(batch_force<R>(b, qgb::FORCE_UPDATE, bargs(tmp, gm, 0.5 * dt, 1)));
-        if (half == 0) QB_RC(batch_evolve<R>(b, gf, gm, (1.0 - 2.0 * lam) * dt, unit_each));
+        // gm += dt/2 F(tmp), then gf = exp(eps gm) gf in the same launch
+        qgb::ForceArgs u = bargs(tmp, gm, 0.5 * dt, 1);
+        u.ev = gf;
+        u.ev_eps = half == 0 ? (1.0 - 2.0 * lam) * dt : (i < n_step - 1 ? 2.0 * lam : lam) * dt;
+        u.ev_unit = (half == 1 && reunit) ? 2 : unit_each;
+        QB_RC(batch_force<R>(b, qgb::FORCE_UPDATE_EVOLVE, u));
       }
-      QB_RC(batch_evolve<R>(b, gf, gm, (i < n_step - 1 ? 2.0 * lam : lam) * dt, unit_each));
-      if (reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step)
-        QB_CUDA((qgb::launch_unitarize<R, double>(g, 4, gf, b->stream)));
     }
   } else if (integrator == QGB_INTEGRATOR_LEAPFROG) {
     for (int i = 0; i < n_step; ++i) {

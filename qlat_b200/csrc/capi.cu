@@ -295,7 +295,7 @@ double gf_hamilton_from(double sp, double sr, double beta, double c1)
 template <typename R>
 int force(const Geo& g, qgb::ForceMode mode, const ForceArgs& a)
 {
-  static const char* names[] = {"force", "force_update", "force_evolve", "flow_stage"};
+  static const char* names[] = {"force", "force_update", "force_evolve", "flow_stage", "force_update_evolve"};
   const int v = g_force_variant[sizeof(R) == 8 ? 0 : 1][a.c1 != 0.0 ? 1 : 0];
   Prof p(names[mode]);
   QGB_TRY_CUDA(qgb::launch_force<R>(g, mode, a, v, g_ctx.stream));
@@ -335,6 +335,18 @@ int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, doub
                   int integrator, int unit_each, int reunit_every)
 {
   const double dt = md_time / n_step;
+  // gm += h F(U) followed by gf = exp(eps gm) gf, as one launch: the update
+  // kernel's epilogue evolves this thread's own link of gf (U is tmp for the
+  // force-gradient step, so gf is never read at other links; for leapfrog U is
+  // gf itself, so leapfrog keeps the separate evolve).  ev_unit 2 is the
+  // re-unitarisation with FP64 arithmetic due after that step.
+  auto update_evolve = [&](const void* U, double h, double eps, bool reunit) -> int {
+    ForceArgs b = fargs(U, gm, beta, c1, h);
+    b.ev = gf;
+    b.ev_eps = eps;
+    b.ev_unit = reunit ? 2 : unit_each;
+    return force<R>(g, qgb::FORCE_UPDATE_EVOLVE, b);
+  };
   if (integrator == QGB_INTEGRATOR_FORCE_GRADIENT) {
     const double lam = 0.5 * (1.0 - 1.0 / sqrt(3.0));
     const double theta = (2.0 - sqrt(3.0)) / 48.0;
@@ -342,18 +354,13 @@ int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, doub
     const double fg_dt = 4.0 * ttheta / dt;
     QGB_RC(evolve<R>(g, gf, gm, lam * dt, unit_each));
     for (int i = 0; i < n_step; ++i) {
+      const bool reunit = reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step;
       for (int half = 0; half < 2; ++half) {
         ForceArgs a = fargs(gf, tmp, beta, c1, fg_dt);
         a.unitarize = unit_each;
         QGB_RC(force<R>(g, qgb::FORCE_EVOLVE, a));
-        ForceArgs b = fargs(tmp, gm, beta, c1, 0.5 * dt);
-        QGB_RC(force<R>(g, qgb::FORCE_UPDATE, b));
-        if (half == 0) QGB_RC(evolve<R>(g, gf, gm, (1.0 - 2.0 * lam) * dt, unit_each));
-      }
-      QGB_RC(evolve<R>(g, gf, gm, (i < n_step - 1 ? 2.0 * lam : lam) * dt, unit_each));
-      if (reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step) {
-        Prof p("unitarize");
-        QGB_TRY_CUDA((qgb::launch_unitarize<R, double>(g, 4, gf, g_ctx.stream)));
+        const double eps = half == 0 ? (1.0 - 2.0 * lam) * dt : (i < n_step - 1 ? 2.0 * lam : lam) * dt;
+        QGB_RC(update_evolve(tmp, 0.5 * dt, eps, half == 1 && reunit));
       }
     }
   } else if (integrator == QGB_INTEGRATOR_LEAPFROG) {
@@ -1226,15 +1233,14 @@ int qgb_force_variant_count(int32_t* n)
 }
 
 int qgb_force_variant_info(int32_t variant, int32_t* block_size, int32_t* min_blocks, int32_t* threads_per_link,
-                           int32_t* packed_fp32, int32_t* site_map)
+                           int32_t* site_map)
 {
-  int bs, mb, sp, pk, mp;
-  QGB_CHECK(qgb::force_variant_info_c(variant, &bs, &mb, &sp, &pk, &mp), QGB_ERR_INVALID_ARG,
+  int bs, mb, sp, mp;
+  QGB_CHECK(qgb::force_variant_info_c(variant, &bs, &mb, &sp, &mp), QGB_ERR_INVALID_ARG,
             "qgb_force_variant_info: no such variant");
   if (block_size) *block_size = bs;
   if (min_blocks) *min_blocks = mb;
   if (threads_per_link) *threads_per_link = sp;
-  if (packed_fp32) *packed_fp32 = pk;
   if (site_map) *site_map = mp;
   return QGB_OK;
 }

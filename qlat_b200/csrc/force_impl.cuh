@@ -57,45 +57,44 @@ struct SignedDir {
   }
 };
 
-template <typename R, bool RECT, bool PACKED>
+template <typename R, bool RECT>
 __device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g, const Coord& x, int mu, R cp, R cr,
                                                int k0, int k1)
 {
-  using O = Ops<R, PACKED>;
   M3<R> S = m3_zero<R>();
 #pragma unroll 1
   for (int k = k0; k < k1; ++k) {
     const SignedDir<R> d{U, g, x, mu, (mu + 1 + (k >> 1)) & 3, (k & 1) ? -1 : 1};
     // B = hop(x) U_mu(x+e)
-    const M3<R> B = O::mul(d.hop(0, 0), d.umu(0, 1));
+    const M3<R> B = mul(d.hop(0, 0), d.umu(0, 1));
     if (!RECT) {
-      S = O::add_mul(S, B, d.back(1, 1));
+      S = add_mul(S, B, d.back(1, 1));
       continue;
     }
     // rect2: S += c1 B U_mu(x+e+mu) back(x+e+2mu) U_mu(x+mu)^+
     {
-      M3<R> C = O::mul(B, d.umu(1, 1));
-      C = O::mul(C, d.back(2, 1));
-      C = O::mul_adj(C, d.umu(1, 0));
+      M3<R> C = mul(B, d.umu(1, 1));
+      C = mul(C, d.back(2, 1));
+      C = mul_adj(C, d.umu(1, 0));
       axpy(S, cr, C);
     }
     M3<R> T = scale(cp, B);
     // rect1: C1 = hop(x) hop(x+e) U_mu(x+2e) back(x+2e+mu)
     {
-      M3<R> C = O::mul(d.hop(0, 0), d.hop(0, 1));
-      C = O::mul(C, d.umu(0, 2));
-      C = O::mul(C, d.back(1, 2));
+      M3<R> C = mul(d.hop(0, 0), d.hop(0, 1));
+      C = mul(C, d.umu(0, 2));
+      C = mul(C, d.back(1, 2));
       axpy(T, cr, C);
     }
     // rect3: C3 = U_mu(x-mu)^+ hop(x-mu) U_mu(x-mu+e) U_mu(x+e)
     {
-      M3<R> C = O::adj_mul(d.umu(-1, 0), d.hop(-1, 0));
-      C = O::mul(C, d.umu(-1, 1));
-      C = O::mul(C, d.umu(0, 1));
+      M3<R> C = adj_mul(d.umu(-1, 0), d.hop(-1, 0));
+      C = mul(C, d.umu(-1, 1));
+      C = mul(C, d.umu(0, 1));
       axpy(T, cr, C);
     }
     // S += T back(x+e+mu)
-    S = O::add_mul(S, T, d.back(1, 1));
+    S = add_mul(S, T, d.back(1, 1));
   }
   if (!RECT) S = scale(cp, S);
   return S;
@@ -147,7 +146,7 @@ __device__ __forceinline__ int nb_delta(int xk, int a, int L, int stride) { retu
 // TWO: carry the SU(3)-valued chains as two rows (mul2 / complete in
 // su3.cuh): 924 instead of 1188 multiply-adds per direction.  Used for FP32
 // only; FP64 keeps full products, identical in structure to the reference's.
-template <typename R, bool RECT, bool PACKED, int SG>
+template <typename R, bool RECT, int SG>
 __device__ __forceinline__ void staple_dir_two_row(M3<R>& S, const LinkLd<R>& L, int s, int mu, int nu, int dmm1,
                                                    int dmp1, int dmp2, int dn1, int dn2, R cp, R cr)
 {
@@ -214,75 +213,74 @@ __device__ __forceinline__ void staple_dir_two_row(M3<R>& S, const LinkLd<R>& L,
   }
 }
 
-template <typename R, bool RECT, bool PACKED, int SG>
+template <typename R, bool RECT, int SG>
 __device__ __forceinline__ void staple_dir_fast(M3<R>& S, const LinkLd<R>& L, int s, int mu, int nu, int dmm1,
                                                 int dmp1, int dmp2, int dn1, int dn2, R cp, R cr)
 {
-  using O = Ops<R, PACKED>;
   if (SG > 0) {
     const M3<R> H = L(nu, s);  // hop(x)
     if (!RECT) {
-      S = add_mul_adj(S, O::mul(H, L(mu, s + dn1)), L(nu, s + dmp1));
+      S = add_mul_adj(S, mul(H, L(mu, s + dn1)), L(nu, s + dmp1));
       return;
     }
     M3<R> T;
     {  // rect1: hop(x) hop(x+e) U_mu(x+2e) back(x+2e+mu)
-      M3<R> C = O::mul(H, L(nu, s + dn1));
-      C = O::mul(C, L(mu, s + dn2));
-      C = O::mul_adj(C, L(nu, s + dmp1 + dn1));
+      M3<R> C = mul(H, L(nu, s + dn1));
+      C = mul(C, L(mu, s + dn2));
+      C = mul_adj(C, L(nu, s + dmp1 + dn1));
       T = scale(cr, C);
     }
     M3<R> U01;
     {  // rect3: U_mu(x-mu)^+ hop(x-mu) U_mu(x-mu+e) U_mu(x+e)
-      M3<R> C = O::adj_mul(L(mu, s + dmm1), L(nu, s + dmm1));
-      C = O::mul(C, L(mu, s + dmm1 + dn1));
+      M3<R> C = adj_mul(L(mu, s + dmm1), L(nu, s + dmm1));
+      C = mul(C, L(mu, s + dmm1 + dn1));
       U01 = L(mu, s + dn1);
-      C = O::mul(C, U01);
+      C = mul(C, U01);
       axpy(T, cr, C);
     }
-    const M3<R> B = O::mul(H, U01);
+    const M3<R> B = mul(H, U01);
     axpy(T, cp, B);
     {  // rect2: B U_mu(x+e+mu) back(x+e+2mu) U_mu(x+mu)^+
-      M3<R> C = O::mul(B, L(mu, s + dmp1 + dn1));
-      C = O::mul_adj(C, L(nu, s + dmp2));
-      C = O::mul_adj(C, L(mu, s + dmp1));
+      M3<R> C = mul(B, L(mu, s + dmp1 + dn1));
+      C = mul_adj(C, L(nu, s + dmp2));
+      C = mul_adj(C, L(mu, s + dmp1));
       axpy(S, cr, C);
     }
     S = add_mul_adj(S, T, L(nu, s + dmp1));
   } else {
     const M3<R> H = L(nu, s + dn1);  // hop(x)^+
     if (!RECT) {
-      S = O::add_mul(S, O::adj_mul(H, L(mu, s + dn1)), L(nu, s + dmp1 + dn1));
+      S = add_mul(S, adj_mul(H, L(mu, s + dn1)), L(nu, s + dmp1 + dn1));
       return;
     }
     M3<R> T;
     {  // rect1: (hop(x+e)^+ hop(x)^+)^+ U_mu(x+2e) back(x+2e+mu)
-      M3<R> C = O::mul(L(nu, s + dn2), H);
-      C = O::adj_mul(C, L(mu, s + dn2));
-      C = O::mul(C, L(nu, s + dmp1 + dn2));
+      M3<R> C = mul(L(nu, s + dn2), H);
+      C = adj_mul(C, L(mu, s + dn2));
+      C = mul(C, L(nu, s + dmp1 + dn2));
       T = scale(cr, C);
     }
     M3<R> U01;
     {  // rect3: (hop(x-mu)^+ U_mu(x-mu))^+ U_mu(x-mu+e) U_mu(x+e)
-      M3<R> C = O::mul(L(nu, s + dmm1 + dn1), L(mu, s + dmm1));
-      C = O::adj_mul(C, L(mu, s + dmm1 + dn1));
+      M3<R> C = mul(L(nu, s + dmm1 + dn1), L(mu, s + dmm1));
+      C = adj_mul(C, L(mu, s + dmm1 + dn1));
       U01 = L(mu, s + dn1);
-      C = O::mul(C, U01);
+      C = mul(C, U01);
       axpy(T, cr, C);
     }
-    const M3<R> B = O::adj_mul(H, U01);
+    const M3<R> B = adj_mul(H, U01);
     axpy(T, cp, B);
     {  // rect2
-      M3<R> C = O::mul(B, L(mu, s + dmp1 + dn1));
-      C = O::mul(C, L(nu, s + dmp2 + dn1));
-      C = O::mul_adj(C, L(mu, s + dmp1));
+      M3<R> C = mul(B, L(mu, s + dmp1 + dn1));
+      C = mul(C, L(nu, s + dmp2 + dn1));
+      C = mul_adj(C, L(mu, s + dmp1));
       axpy(S, cr, C);
     }
-    S = O::add_mul(S, T, L(nu, s + dmp1 + dn1));
+    S = add_mul(S, T, L(nu, s + dmp1 + dn1));
   }
 }
 
-template <typename R, bool RECT, bool PACKED, bool TWO>
+template <typename R, bool RECT, bool TWO>
 __device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, int s, int mu, R cp, R cr)
 {
   const LinkLd<R> L{U, (int)g.V};
@@ -296,14 +294,14 @@ __device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, i
     const int nu = (mu + i) & 3;
     const int xn = sel4(x.c, nu), Ln = sel4(g.d, nu), sn = sel4(st, nu);
     if constexpr (TWO) {
-      staple_dir_two_row<R, RECT, PACKED, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
+      staple_dir_two_row<R, RECT, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
                                              nb_delta(xn, 2, Ln, sn), cp, cr);
-      staple_dir_two_row<R, RECT, PACKED, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
+      staple_dir_two_row<R, RECT, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
                                               nb_delta(xn, -2, Ln, sn), cp, cr);
     } else {
-      staple_dir_fast<R, RECT, PACKED, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
+      staple_dir_fast<R, RECT, 1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, 1, Ln, sn),
                                           nb_delta(xn, 2, Ln, sn), cp, cr);
-      staple_dir_fast<R, RECT, PACKED, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
+      staple_dir_fast<R, RECT, -1>(S, L, s, mu, nu, dmm1, dmp1, dmp2, nb_delta(xn, -1, Ln, sn),
                                            nb_delta(xn, -2, Ln, sn), cp, cr);
     }
   }
@@ -326,11 +324,21 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
   F = scale(R(-beta / 3.0), F);
   if (MODE == FORCE_SET) {
     WField<R>{(Cx<R>*)a.out, stride}.st(s, mu, F);
-  } else if (MODE == FORCE_UPDATE) {
+  } else if (MODE == FORCE_UPDATE || MODE == FORCE_UPDATE_EVOLVE) {
     const WField<R> P{(Cx<R>*)a.out, stride};
     M3<R> p = P.ld(s, mu);
     axpy(p, R(a.dt), F);
     P.st(s, mu, p);
+    if (MODE == FORCE_UPDATE_EVOLVE) {
+      // the link update that follows the momentum update in the integrators
+      // (k_evolve, then k_unitarize<R, double> when ev_unit == 2), on this
+      // thread's own link of W
+      const WField<R> W{(Cx<R>*)a.ev, stride};
+      M3<R> wn = mul(exp_ch(scale(R(a.ev_eps), p)), W.ld(s, mu));
+      if (a.ev_unit == 1) unitarize(wn);
+      else if (a.ev_unit == 2) unitarize_as<double, R>(wn);
+      W.st(s, mu, wn);
+    }
   } else {
     M3<R> Z = F;
     if (MODE == FORCE_FLOW) {
@@ -347,37 +355,29 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
 // Launch variants for the autotuner: threads per block, minimum resident
 // blocks per SM (caps registers), threads per link (SPLIT = 2 gives each link
 // to a lane pair, each doing 3 of the 6 signed directions, combined by a
-// shuffle), packed FP32 FMAs, and the site mapping: MAP 0 runs blocks of
-// consecutive sites with mu = blockIdx.y; MAP 1 gives each block the four
-// links of a compact tile of BS/4 sites (4 x 2 x 2 x 2 for 128 threads,
-// 4 x 4 x 2 x 2 for 256), one warp-group per mu, so the four directions share
-// the tile's neighbourhood in L1.  MAP 1 needs the lattice extents to be
-// multiples of the tile; otherwise the launcher uses MAP 0.  MAP 2 is the
-// linear mapping of MAP 0 with the staple_sum_fast evaluation (per-thread
-// neighbour offsets, sign-specialised directions); it needs 36 V < 2^31 and
-// SPLIT = 1, otherwise the launcher uses MAP 0.  MAP 3 is MAP 2 with the
-// two-row SU(3) chains (FP32; FP64 runs MAP 2).
-struct ForceVariant {
-  int bs, minb, split, packed, map;
-};
+// shuffle), and the site mapping and staple evaluation: MAP 0 runs blocks of
+// consecutive sites with mu = blockIdx.y and staple_sum_rt; MAP 1 gives each
+// block the four links of a compact tile of BS/4 sites (4 x 2 x 2 x 2 for 128
+// threads, 4 x 4 x 2 x 2 for 256), one warp-group per mu, so the four
+// directions share the tile's neighbourhood in L1 (it needs the lattice
+// extents to be multiples of the tile, otherwise the launcher uses MAP 0);
+// MAP 2 is the linear mapping of MAP 0 with staple_sum_fast (per-thread
+// neighbour offsets, sign-specialised directions; needs 36 V < 2^31 and
+// SPLIT = 1, otherwise MAP 0); MAP 3 is MAP 2 with the two-row SU(3) chains
+// (FP32; FP64 runs MAP 2).
 #define QGB_FORCE_VARIANTS(X) \
-  X(0, 128, 1, 1, 0, 0)       \
-  X(1, 256, 1, 1, 0, 0)       \
-  X(2, 128, 3, 1, 0, 0)       \
-  X(3, 128, 1, 2, 0, 0)       \
-  X(4, 128, 1, 1, 1, 0)       \
-  X(5, 128, 1, 1, 0, 1)       \
-  X(6, 256, 1, 1, 0, 1)       \
-  X(7, 128, 1, 1, 0, 2)       \
-  X(8, 256, 1, 1, 0, 2)       \
-  X(9, 64, 1, 1, 0, 2)        \
-  X(10, 128, 3, 1, 0, 2)      \
-  X(11, 128, 4, 1, 0, 2)      \
-  X(12, 128, 1, 1, 1, 2)      \
-  X(13, 128, 1, 1, 0, 3)      \
-  X(14, 256, 1, 1, 0, 3)      \
-  X(15, 128, 3, 1, 0, 3)
-static const int N_FORCE_VARIANTS = 16;
+  X(0, 128, 1, 1, 0)          \
+  X(1, 256, 1, 1, 0)          \
+  X(2, 128, 1, 2, 0)          \
+  X(3, 128, 1, 1, 1)          \
+  X(4, 128, 1, 1, 2)          \
+  X(5, 256, 1, 1, 2)          \
+  X(6, 128, 3, 1, 2)          \
+  X(7, 128, 1, 1, 3)          \
+  X(8, 256, 1, 1, 3)          \
+  X(9, 128, 3, 1, 3)          \
+  X(10, 128, 4, 1, 3)
+static const int N_FORCE_VARIANTS = 11;
 
 template <int BS>
 struct Tile {
@@ -385,7 +385,7 @@ struct Tile {
   static const int sites = tx * ty * tz * tt;
 };
 
-template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, bool PACKED, int MAP>
+template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, int MAP>
 __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 {
   const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
     const long t = (long)blockIdx.x * BS + threadIdx.x;
     if (t >= g.V) return;
     const int mu = blockIdx.y;
-    const M3<R> S = staple_sum_fast<R, RECT, PACKED, MAP == 3>((const Cx<R>*)a.U, g, (int)t, mu, cp, cr);
+    const M3<R> S = staple_sum_fast<R, RECT, MAP == 3>((const Cx<R>*)a.U, g, (int)t, mu, cp, cr);
     force_epilogue<R, MODE>(a, CField<R>{(const Cx<R>*)a.U, g.V}, g.V, t, mu, S, a.beta);
     return;
   }
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
   const long s = valid ? s0 : g.V - 1;
   const CField<R> U{(const Cx<R>*)a.U, g.V};
   const Coord x = coord_of(g, s);
-  M3<R> S = staple_sum_rt<R, RECT, PACKED>(U, g, x, mu, cp, cr, h * (6 / SPLIT), (h + 1) * (6 / SPLIT));
+  M3<R> S = staple_sum_rt<R, RECT>(U, g, x, mu, cp, cr, h * (6 / SPLIT), (h + 1) * (6 / SPLIT));
   if (SPLIT == 2) {
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
@@ -441,28 +441,29 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
   force_epilogue<R, MODE>(a, U, g.V, s, mu, S, a.beta);
 }
 
-template <typename R, int BS, int MINB, int SPLIT, bool PACKED, int MAP>
+template <typename R, int BS, int MINB, int SPLIT, int MAP>
 cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
   if constexpr (MAP == 3 && sizeof(R) == 8) {
-    return launch_force_v<R, BS, MINB, SPLIT, PACKED, 2>(g, mode, a, st);
+    return launch_force_v<R, BS, MINB, SPLIT, 2>(g, mode, a, st);
   } else {
   using TL = Tile<BS>;
   const bool tiled = MAP == 1 && SPLIT == 1 && g.d[0] % TL::tx == 0 && g.d[1] % TL::ty == 0 &&
                      g.d[2] % TL::tz == 0 && g.d[3] % TL::tt == 0;
-  if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
+  if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
   const bool fast = MAP >= 2 && SPLIT == 1 && g.off == 0 && g.V * 36 < 2147483647L;
-  if (MAP >= 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, PACKED, 0>(g, mode, a, st);
+  if (MAP >= 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
   dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
   const bool rect = a.c1 != 0.0;
 #define QGB_LAUNCH(M)                                                                                  \
-  if (rect) k_force<R, M, true, BS, MINB, SPLIT, PACKED, MAP><<<grid, BS, 0, st>>>(g, a); \
-  else k_force<R, M, false, BS, MINB, SPLIT, PACKED, MAP><<<grid, BS, 0, st>>>(g, a);
+  if (rect) k_force<R, M, true, BS, MINB, SPLIT, MAP><<<grid, BS, 0, st>>>(g, a); \
+  else k_force<R, M, false, BS, MINB, SPLIT, MAP><<<grid, BS, 0, st>>>(g, a);
   switch (mode) {
     case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
     case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;
     case FORCE_EVOLVE: QGB_LAUNCH(FORCE_EVOLVE) break;
     case FORCE_FLOW: QGB_LAUNCH(FORCE_FLOW) break;
+    case FORCE_UPDATE_EVOLVE: QGB_LAUNCH(FORCE_UPDATE_EVOLVE) break;
   }
 #undef QGB_LAUNCH
   return cudaGetLastError();
@@ -473,19 +474,19 @@ template <typename R>
 cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, int variant, cudaStream_t st)
 {
   switch (variant) {
-#define QGB_V(ID, BS, MINB, SPLIT, PACKED, MAP) \
-  case ID: return launch_force_v<R, BS, MINB, SPLIT, (PACKED != 0), MAP>(g, mode, a, st);
+#define QGB_V(ID, BS, MINB, SPLIT, MAP) \
+  case ID: return launch_force_v<R, BS, MINB, SPLIT, MAP>(g, mode, a, st);
     QGB_FORCE_VARIANTS(QGB_V)
 #undef QGB_V
     default: return cudaErrorInvalidValue;
   }
 }
 
-inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* packed, int* map)
+inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* map)
 {
   switch (variant) {
-#define QGB_V(ID, BS, MINB, SPLIT, PACKED, MAP) \
-  case ID: *bs = BS; *minb = MINB; *split = SPLIT; *packed = PACKED; *map = MAP; return 1;
+#define QGB_V(ID, BS, MINB, SPLIT, MAP) \
+  case ID: *bs = BS; *minb = MINB; *split = SPLIT; *map = MAP; return 1;
     QGB_FORCE_VARIANTS(QGB_V)
 #undef QGB_V
     default: return 0;
@@ -510,7 +511,7 @@ __global__ void __launch_bounds__(128) k_force_batch(long Vtot, int nchain, cons
   const CField<R> U{(const Cx<R>*)a.U, Vtot};
   const Coord x = coord_of(g, sg - ci.off);
   const R cp = R(1.0 - 8.0 * ci.c1), cr = R(ci.c1);
-  const M3<R> S = staple_sum_rt<R, RECT, false>(U, g, x, mu, cp, cr, 0, 6);
+  const M3<R> S = staple_sum_rt<R, RECT>(U, g, x, mu, cp, cr, 0, 6);
   force_epilogue<R, MODE>(a, U, Vtot, sg, mu, S, ci.beta);
 }
 
@@ -527,6 +528,7 @@ cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const Ch
     case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;
     case FORCE_EVOLVE: QGB_LAUNCH(FORCE_EVOLVE) break;
     case FORCE_FLOW: QGB_LAUNCH(FORCE_FLOW) break;
+    case FORCE_UPDATE_EVOLVE: QGB_LAUNCH(FORCE_UPDATE_EVOLVE) break;
   }
 #undef QGB_LAUNCH
   return cudaGetLastError();

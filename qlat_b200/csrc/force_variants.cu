@@ -4,8 +4,8 @@
 namespace qgb
 {
 int force_variant_count() { return N_FORCE_VARIANTS; }
-int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed, int* map)
+int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* map)
 {
-  return force_variant_info(variant, bs, minb, split, packed, map);
+  return force_variant_info(variant, bs, minb, split, map);
 }
 }  // namespace qgb

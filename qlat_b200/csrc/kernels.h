@@ -21,23 +21,27 @@ struct ChainInfo {
   double beta, c1;
 };
 
-// Force kernel output modes (see kernels.cu).
+// Force kernel output modes (force_impl.cuh).
 enum ForceMode {
-  FORCE_SET = 0,      // out = F
-  FORCE_UPDATE = 1,   // P += dt F
-  FORCE_EVOLVE = 2,   // U_out = unitarize(exp(eps F) U)
-  FORCE_FLOW = 3,     // Z = a F + b Z_prev; U_out = unitarize(exp(eps Z) U)
+  FORCE_SET = 0,            // out = F
+  FORCE_UPDATE = 1,         // P += dt F
+  FORCE_EVOLVE = 2,         // U_out = unitarize(exp(eps F) U)
+  FORCE_FLOW = 3,           // Z = a F + b Z_prev; U_out = unitarize(exp(eps Z) U)
+  FORCE_UPDATE_EVOLVE = 4,  // P += dt F, then W = exp(ev_eps P) W on a second link field W
 };
 
 struct ForceArgs {
   const void* U;    // links in (SoA)
-  void* out;        // F (SET) / P (UPDATE) / U_out (EVOLVE, FLOW)
+  void* out;        // F (SET) / P (UPDATE, UPDATE_EVOLVE) / U_out (EVOLVE, FLOW)
   const void* zp;   // FLOW: Z_prev (may be null when b == 0)
   void* z;          // FLOW: Z out (may be null)
   double beta, c1;  // gauge action
   double dt;        // UPDATE: P += dt F; EVOLVE/FLOW: exp step
   double a, b;      // FLOW combination
   int unitarize;    // EVOLVE/FLOW: unitarize after exp
+  void* ev;         // UPDATE_EVOLVE: W, evolved in place (never read at other links, so W != U)
+  double ev_eps;    // UPDATE_EVOLVE: exponential step of W
+  int ev_unit;      // UPDATE_EVOLVE: 0 none, 1 unitarize in R, 2 unitarize with FP64 arithmetic
 };
 
 void init_constants();  // SHA-256 and log tables into constant memory (per device)
@@ -50,7 +54,7 @@ int force_variant_count();
 template <typename R>
 cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
                                ForceMode mode, const ForceArgs& a, cudaStream_t st);
-int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* packed, int* map);
+int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* map);
 
 // U = exp(eps P) U (optionally unitarized; exp by Cayley-Hamilton series or the
 // reference's order-20 Taylor series).

@@ -203,139 +203,6 @@ QGB_HD M3<R> add_adj_mul(const M3<R>& s, const M3<R>& a, const M3<R>& b)
   return c;
 }
 
-// ---- packed FP32 variants (sm_100 FFMA2: two FP32 FMAs per instruction) --
-// A complex multiply-accumulate c += a b is (c.re, c.im) += (a.re, a.re) *
-// (b.re, b.im) + (-a.im, a.im) * (b.im, b.re): two packed FMAs instead of four.
-#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
-#define QGB_HAVE_FFMA2 1
-__device__ __forceinline__ float2 p2(float a, float b) { return make_float2(a, b); }
-
-__device__ __forceinline__ M3<float> mul_p(const M3<float>& a, const M3<float>& b)
-{
-  M3<float> c;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      float2 acc = p2(0.f, 0.f);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const Cx<float> x = a.e[3 * i + k], y = b.e[3 * k + j];
-        acc = __ffma2_rn(p2(x.re, x.re), p2(y.re, y.im), acc);
-        acc = __ffma2_rn(p2(-x.im, x.im), p2(y.im, y.re), acc);
-      }
-      c.e[3 * i + j] = cx<float>(acc.x, acc.y);
-    }
-  return c;
-}
-
-// s + a b
-__device__ __forceinline__ M3<float> add_mul_p(const M3<float>& s, const M3<float>& a, const M3<float>& b)
-{
-  M3<float> c;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      float2 acc = p2(s.e[3 * i + j].re, s.e[3 * i + j].im);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const Cx<float> x = a.e[3 * i + k], y = b.e[3 * k + j];
-        acc = __ffma2_rn(p2(x.re, x.re), p2(y.re, y.im), acc);
-        acc = __ffma2_rn(p2(-x.im, x.im), p2(y.im, y.re), acc);
-      }
-      c.e[3 * i + j] = cx<float>(acc.x, acc.y);
-    }
-  return c;
-}
-
-// a b^dagger
-__device__ __forceinline__ M3<float> mul_adj_p(const M3<float>& a, const M3<float>& b)
-{
-  M3<float> c;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      float2 acc = p2(0.f, 0.f);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const Cx<float> x = a.e[3 * i + k], y = b.e[3 * j + k];
-        acc = __ffma2_rn(p2(x.re, x.re), p2(y.re, -y.im), acc);
-        acc = __ffma2_rn(p2(x.im, x.im), p2(y.im, y.re), acc);
-      }
-      c.e[3 * i + j] = cx<float>(acc.x, acc.y);
-    }
-  return c;
-}
-
-// a^dagger b
-__device__ __forceinline__ M3<float> adj_mul_p(const M3<float>& a, const M3<float>& b)
-{
-  M3<float> c;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      float2 acc = p2(0.f, 0.f);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const Cx<float> x = a.e[3 * k + i], y = b.e[3 * k + j];
-        acc = __ffma2_rn(p2(x.re, x.re), p2(y.re, y.im), acc);
-        acc = __ffma2_rn(p2(x.im, -x.im), p2(y.im, y.re), acc);
-      }
-      c.e[3 * i + j] = cx<float>(acc.x, acc.y);
-    }
-  return c;
-}
-#endif
-
-// Dispatch: Ops<R, PACKED>::mul etc. use the packed forms for FP32 when asked.
-template <typename R, bool PACKED>
-struct Ops {
-  static QGB_HD M3<R> mul(const M3<R>& a, const M3<R>& b) { return qgb::mul(a, b); }
-  static QGB_HD M3<R> add_mul(const M3<R>& s, const M3<R>& a, const M3<R>& b) { return qgb::add_mul(s, a, b); }
-  static QGB_HD M3<R> mul_adj(const M3<R>& a, const M3<R>& b) { return qgb::mul_adj(a, b); }
-  static QGB_HD M3<R> adj_mul(const M3<R>& a, const M3<R>& b) { return qgb::adj_mul(a, b); }
-};
-#if defined(__CUDACC__)
-template <>
-struct Ops<float, true> {
-  static __device__ __forceinline__ M3<float> mul(const M3<float>& a, const M3<float>& b)
-  {
-#if defined(QGB_HAVE_FFMA2)
-    return mul_p(a, b);
-#else
-    return qgb::mul(a, b);
-#endif
-  }
-  static __device__ __forceinline__ M3<float> add_mul(const M3<float>& s, const M3<float>& a, const M3<float>& b)
-  {
-#if defined(QGB_HAVE_FFMA2)
-    return add_mul_p(s, a, b);
-#else
-    return qgb::add_mul(s, a, b);
-#endif
-  }
-  static __device__ __forceinline__ M3<float> mul_adj(const M3<float>& a, const M3<float>& b)
-  {
-#if defined(QGB_HAVE_FFMA2)
-    return mul_adj_p(a, b);
-#else
-    return qgb::mul_adj(a, b);
-#endif
-  }
-  static __device__ __forceinline__ M3<float> adj_mul(const M3<float>& a, const M3<float>& b)
-  {
-#if defined(QGB_HAVE_FFMA2)
-    return adj_mul_p(a, b);
-#else
-    return qgb::adj_mul(a, b);
-#endif
-  }
-};
-#endif
-
 template <typename R>
 QGB_HD M3<R> adj(const M3<R>& a)
 {
