@@ -164,7 +164,7 @@ __global__ void k_basis_to_matrix(long V, int m, const R* basis, Cx<R>* fc)
   for (int mu = 0; mu < m; ++mu) {
     R b[8];
 #pragma unroll
-    for (int a = 0; a < 8; ++a) b[a] = basis[(long)(8 * mu + a) * V + s];
+    for (int a = 0; a < 8; ++a) b[a] = basis[lay_index<1>(V, 8 * mu + a, 0, s)];
     const R s3 = R(0.57735026918962584) * b[7];
     M3<R> r;
     r.e[0] = cx<R>(R(0), b[2] + s3);
@@ -197,7 +197,7 @@ __global__ void k_matrix_to_basis(long V, int m, const Cx<R>* fc, R* basis)
     b[6] = x.e[5].re;
     b[7] = R(0.86602540378443865) * (x.e[0].im + x.e[4].im);
 #pragma unroll
-    for (int a = 0; a < 8; ++a) basis[(long)(8 * mu + a) * V + s] = b[a];
+    for (int a = 0; a < 8; ++a) basis[lay_index<1>(V, 8 * mu + a, 0, s)] = b[a];
   }
 }
 

@@ -50,7 +50,7 @@ struct qgb_batch_s {
   double* d_sums = nullptr;  // per-chain sums (8 n)
   double* h_sums = nullptr;  // pinned mirror
   int* d_ambiguous = nullptr;
-  double* d_chain_tmp = nullptr;  // one chain's field for download / upload (2 x max chain)
+  double* d_chain_tmp = nullptr;  // one chain's links in the reference image (download / upload)
   long max_chain_reals = 0;
   cudaStream_t stream = nullptr;
   std::map<std::tuple<int, double, int, int, int>, cudaGraphExec_t> graphs;
@@ -166,8 +166,8 @@ int batch_hamiltonian(qgb_batch_s* b, int slot)
 // One trajectory of every chain, enqueued on b->stream (recordable as a graph).
 int enqueue_trajectory(qgb_batch_s* b, int n_step, double md_time, int integrator, int mixed, int reunit)
 {
-  const size_t bytes64 = (size_t)b->Vtot * 72 * sizeof(double);
-  const long n = b->Vtot * 72;
+  const size_t bytes64 = (size_t)qgb::padded_sites(b->Vtot) * 72 * sizeof(double);
+  const long n = qgb::padded_sites(b->Vtot) * 72;
   qgb::Geo g;
   g.d[0] = g.d[1] = g.d[2] = g.d[3] = 1;
   g.V = b->Vtot;
@@ -232,10 +232,11 @@ int qgb_batch_create(qgb_batch** out, int32_t n_chains, const int32_t* total_sit
   }
   b->Vtot = offs[n_chains];
   b->max_chain_reals = max_v * 72;
-  const size_t b64 = (size_t)b->Vtot * 72 * sizeof(double), b32 = b64 / 2;
+  const size_t b64 = (size_t)qgb::padded_sites(b->Vtot) * 72 * sizeof(double), b32 = b64 / 2;
   cudaError_t e = cudaSuccess;
   auto A = [&](void** p, size_t bytes) {
     if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);  // padding sites stay zero
   };
   A((void**)&b->d_offs, (n_chains + 1) * sizeof(long));
   A((void**)&b->d_chains, n_chains * sizeof(qgb::ChainInfo));
@@ -251,7 +252,7 @@ int qgb_batch_create(qgb_batch** out, int32_t n_chains, const int32_t* total_sit
   A((void**)&b->d_vals, 2 * b->Vtot * sizeof(double));
   A((void**)&b->d_sums, 8 * (size_t)n_chains * sizeof(double));
   A((void**)&b->d_ambiguous, sizeof(int));
-  A((void**)&b->d_chain_tmp, 2 * b->max_chain_reals * sizeof(double));
+  A((void**)&b->d_chain_tmp, b->max_chain_reals * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_rs, (size_t)n_chains * 24 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_flags, n_chains * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_sums, 8 * (size_t)n_chains * sizeof(double));
@@ -415,15 +416,8 @@ int qgb_batch_download_chain(qgb_batch* b, int32_t chain, double* host)
 {
   if (!b || !host || chain < 0 || chain >= b->n) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_download_chain: bad argument");
   const qgb::ChainInfo& ci = b->chains[chain];
-  double* soa = b->d_chain_tmp;
-  double* aos = b->d_chain_tmp + b->max_chain_reals;
-  // 36 components of 16-byte complex numbers: [mu*9 + k][site] with pitch Vtot -> pitch V
-  QB_CUDA(cudaMemcpy2DAsync(soa, ci.V * 16, b->gf + ci.off * 2, b->Vtot * 16, ci.V * 16, 36, cudaMemcpyDeviceToDevice,
-                            b->stream));
-  qgb::Geo g;
-  for (int i = 0; i < 4; ++i) g.d[i] = ci.d[i];
-  g.V = ci.V;
-  QB_CUDA(qgb::launch_soa_to_aos<double>(g, 4, 18, soa, aos, b->stream));
+  double* aos = b->d_chain_tmp;
+  QB_CUDA(qgb::launch_store_to_aos<double>(b->Vtot, ci.off, ci.V, 4, 18, b->gf, aos, b->stream));
   QB_CUDA(cudaMemcpyAsync(host, aos, ci.V * 72 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
   QB_CUDA(cudaStreamSynchronize(b->stream));
   return QGB_OK;
@@ -433,15 +427,9 @@ int qgb_batch_upload_chain(qgb_batch* b, int32_t chain, const double* host)
 {
   if (!b || !host || chain < 0 || chain >= b->n) return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_upload_chain: bad argument");
   const qgb::ChainInfo& ci = b->chains[chain];
-  double* soa = b->d_chain_tmp;
-  double* aos = b->d_chain_tmp + b->max_chain_reals;
+  double* aos = b->d_chain_tmp;
   QB_CUDA(cudaMemcpyAsync(aos, host, ci.V * 72 * sizeof(double), cudaMemcpyHostToDevice, b->stream));
-  qgb::Geo g;
-  for (int i = 0; i < 4; ++i) g.d[i] = ci.d[i];
-  g.V = ci.V;
-  QB_CUDA(qgb::launch_aos_to_soa<double>(g, 4, 18, aos, soa, b->stream));
-  QB_CUDA(cudaMemcpy2DAsync(b->gf + ci.off * 2, b->Vtot * 16, soa, ci.V * 16, ci.V * 16, 36, cudaMemcpyDeviceToDevice,
-                            b->stream));
+  QB_CUDA(qgb::launch_aos_to_store<double>(b->Vtot, ci.off, ci.V, 4, 18, aos, b->gf, b->stream));
   QB_CUDA(cudaStreamSynchronize(b->stream));
   return QGB_OK;
 }

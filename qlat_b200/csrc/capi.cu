@@ -170,7 +170,11 @@ Geo geo_of(const qgb_field_s* f)
 }
 
 size_t elem_reals(const qgb_field_s* f) { return f->kind == QGB_KIND_COLOR_MATRIX ? 18 : 1; }
+// reals in the reference image of a field (host transfers)
 long n_reals(const qgb_field_s* f) { return f->V * f->mult * (long)elem_reals(f); }
+// reals in the device storage of a field (sites padded to a multiple of 32;
+// elementwise kernels run over all of it, the padding is zero)
+long n_store(const qgb_field_s* f) { return qgb::padded_sites(f->V) * f->mult * (long)elem_reals(f); }
 
 int ensure_partials(size_t n)
 {
@@ -200,6 +204,9 @@ int get_scratch(size_t bytes, int tag, void** out)
     void* p = nullptr;
     QGB_TRY_CUDA(cudaMalloc(&p, bytes));
     v.push_back(p);
+    // zero once: scratch buffers can become a field's storage (flow_step swaps
+    // them), and the padding sites of every field stay zero
+    QGB_TRY_CUDA(cudaMemsetAsync(p, 0, bytes, g_ctx.stream));
   }
   *out = v[0];
   return QGB_OK;
@@ -570,7 +577,8 @@ int qgb_field_create(qgb_field** out, const int32_t total_site[4], int32_t multi
   f->mult = multiplicity;
   f->kind = kind;
   f->prec = precision;
-  f->bytes = (size_t)V * multiplicity * (kind == QGB_KIND_COLOR_MATRIX ? 18 : 1) * (precision == QGB_F64 ? 8 : 4);
+  f->bytes = (size_t)qgb::padded_sites(V) * multiplicity * (kind == QGB_KIND_COLOR_MATRIX ? 18 : 1) *
+             (precision == QGB_F64 ? 8 : 4);
   f->d = nullptr;
   cudaError_t e = cudaMalloc(&f->d, f->bytes);
   if (e != cudaSuccess) {
@@ -615,9 +623,9 @@ static int upload_from_device_aos(qgb_field* f, const double* aos)
   const Geo g = geo_of(f);
   Prof p("convert");
   if (f->prec == QGB_F64)
-    QGB_TRY_CUDA(qgb::launch_aos_to_soa<double>(g, f->mult, (int)elem_reals(f), aos, f->d, g_ctx.stream));
+    QGB_TRY_CUDA(qgb::launch_aos_to_store<double>(g.V, 0, g.V, f->mult, (int)elem_reals(f), aos, f->d, g_ctx.stream));
   else
-    QGB_TRY_CUDA(qgb::launch_aos_to_soa<float>(g, f->mult, (int)elem_reals(f), aos, f->d, g_ctx.stream));
+    QGB_TRY_CUDA(qgb::launch_aos_to_store<float>(g.V, 0, g.V, f->mult, (int)elem_reals(f), aos, f->d, g_ctx.stream));
   return QGB_OK;
 }
 
@@ -626,9 +634,9 @@ static int download_to_device_aos(const qgb_field* f, double* aos)
   const Geo g = geo_of(f);
   Prof p("convert");
   if (f->prec == QGB_F64)
-    QGB_TRY_CUDA(qgb::launch_soa_to_aos<double>(g, f->mult, (int)elem_reals(f), f->d, aos, g_ctx.stream));
+    QGB_TRY_CUDA(qgb::launch_store_to_aos<double>(g.V, 0, g.V, f->mult, (int)elem_reals(f), f->d, aos, g_ctx.stream));
   else
-    QGB_TRY_CUDA(qgb::launch_soa_to_aos<float>(g, f->mult, (int)elem_reals(f), f->d, aos, g_ctx.stream));
+    QGB_TRY_CUDA(qgb::launch_store_to_aos<float>(g.V, 0, g.V, f->mult, (int)elem_reals(f), f->d, aos, g_ctx.stream));
   return QGB_OK;
 }
 
@@ -681,7 +689,7 @@ int qgb_field_copy(qgb_field* dst, const qgb_field* src)
   QGB_CHECK(same_geo(dst, src) && dst->mult == src->mult && dst->kind == src->kind, QGB_ERR_MISMATCH,
             "qgb_field_copy: geometry / multiplicity / kind mismatch");
   if (dst == src) return QGB_OK;
-  const long n = n_reals(dst);
+  const long n = n_store(dst);
   Prof p("convert");
   if (dst->prec == src->prec) {
     QGB_TRY_CUDA(cudaMemcpyAsync(dst->d, src->d, dst->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
@@ -709,7 +717,7 @@ int qgb_field_axpby(qgb_field* y, double a, const qgb_field* x, double b)
     QGB_CHECK(same_geo(x, y) && x->mult == y->mult && x->kind == y->kind && x->prec == y->prec, QGB_ERR_MISMATCH,
               "qgb_field_axpby: field mismatch");
   }
-  const long n = n_reals(y);
+  const long n = n_store(y);
   Prof p("axpby");
   if (y->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_axpby<double>(n, y->d, a, x ? x->d : nullptr, b, g_ctx.stream));
   else QGB_TRY_CUDA(qgb::launch_axpby<float>(n, y->d, a, x ? x->d : nullptr, b, g_ctx.stream));
@@ -724,8 +732,8 @@ int qgb_field_qnorm(const qgb_field* f, double* out)
   const int nb = 148 * 8;
   QGB_RC(ensure_partials(nb));
   Prof p("reduce", 2);
-  if (f->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_qnorm<double>(n_reals(f), f->d, g_ctx.partials, nb, g_ctx.stream));
-  else QGB_TRY_CUDA(qgb::launch_qnorm<float>(n_reals(f), f->d, g_ctx.partials, nb, g_ctx.stream));
+  if (f->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_qnorm<double>(n_store(f), f->d, g_ctx.partials, nb, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_qnorm<float>(n_store(f), f->d, g_ctx.partials, nb, g_ctx.stream));
   QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 0, g_ctx.stream));
   return read_results(0, 1, out);
 }
@@ -988,7 +996,7 @@ int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c
   QGB_RC(get_scratch(b32, 12, &gm32));
   QGB_RC(get_scratch(b32, 13, &tmp32));
   QGB_RC(hamiltonian_slots(gm, gf, c1, 0));
-  const long n = n_reals(gf);
+  const long n = n_store(gf);
   {
     Prof p("convert", 2);
     QGB_TRY_CUDA((qgb::launch_convert<double, float>(n, gf->d, gf32, g_ctx.stream)));
@@ -1145,7 +1153,7 @@ int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, 
   ForceArgs a = fargs(V, lamN, beta, c1_loss, 0.0);
   if (gf->prec == QGB_F64) QGB_RC(force<double>(g, qgb::FORCE_SET, a));
   else QGB_RC(force<float>(g, qgb::FORCE_SET, a));
-  const long n = n_reals(gf);
+  const long n = n_store(gf);
   if (gf->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_axpby<double>(n, lamN, 0.0, nullptr, -2.0, g_ctx.stream));
   else QGB_TRY_CUDA(qgb::launch_axpby<float>(n, lamN, 0.0, nullptr, -2.0, g_ctx.stream));
   // restore the scratch bookkeeping of the flowed buffer, then pull back

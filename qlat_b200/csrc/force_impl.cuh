@@ -117,13 +117,13 @@ __device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g,
 template <typename R>
 struct LinkLd {
   const Cx<R>* __restrict__ p;
-  int V;
+  int nblk;  // 32-site blocks of the field
   __device__ __forceinline__ M3<R> operator()(int link, int site) const
   {
-    const Cx<R>* q = p + (link * 9 * V + site);
+    const Cx<R>* q = p + (((link * nblk + (site >> 5)) * 9) * 32 + (site & 31));
     M3<R> r;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + k * V);
+    for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + 32 * k);
     return r;
   }
 };
@@ -283,7 +283,7 @@ __device__ __forceinline__ void staple_dir_fast(M3<R>& S, const LinkLd<R>& L, in
 template <typename R, bool RECT, bool TWO>
 __device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, int s, int mu, R cp, R cr)
 {
-  const LinkLd<R> L{U, (int)g.V};
+  const LinkLd<R> L{U, (int)site_blocks(g.V)};
   const Coord x = coord_of(g, s);
   const int st[4] = {1, g.d[0], g.d[0] * g.d[1], g.d[0] * g.d[1] * g.d[2]};
   const int xm = sel4(x.c, mu), Lm = sel4(g.d, mu), sm = sel4(st, mu);
@@ -451,7 +451,7 @@ cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cud
   const bool tiled = MAP == 1 && SPLIT == 1 && g.d[0] % TL::tx == 0 && g.d[1] % TL::ty == 0 &&
                      g.d[2] % TL::tz == 0 && g.d[3] % TL::tt == 0;
   if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
-  const bool fast = MAP >= 2 && SPLIT == 1 && g.off == 0 && g.V * 36 < 2147483647L;
+  const bool fast = MAP >= 2 && SPLIT == 1 && g.off == 0 && padded_sites(g.V) * 36 < 2147483647L;
   if (MAP >= 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
   dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
   const bool rect = a.c1 != 0.0;

@@ -1,13 +1,19 @@
 // gauge_common.cuh -- device-side field access and lattice geometry shared by
 // the kernel translation units.
 //
-// Memory layout in HBM: a color-matrix field with multiplicity m over V sites
-// is stored structure-of-arrays, element (site, mu, k) of the 3x3 matrix at
-// Cx<R>[(mu * 9 + k) * V + site], sites in the reference's order (x fastest,
-// coordinate.h:182-188).  A warp touches 32 consecutive sites per component,
-// so every load and store is a fully coalesced 512-byte (FP64) or 256-byte
-// (FP32) transaction.  Neighbour links come through L1/L2; the lattice is
-// periodic.
+// Memory layout in HBM: the sites of a field are cut into blocks of 32
+// consecutive sites (the reference's order, x fastest, coordinate.h:182-188),
+// and entry k of component m of site s (k < K: the 9 complex entries of a
+// color matrix, K = 9; or one real, K = 1) is stored at
+//     ((m * nblk + s / 32) * K + k) * 32 + s % 32,     nblk = ceil(V / 32).
+// A warp touching 32 consecutive sites reads one fully coalesced 512-byte
+// (FP64) or 256-byte (FP32) segment per matrix entry, as in a plain
+// structure-of-arrays layout, but the 9 entries of one link are a fixed 32
+// elements apart, so a link costs one address computation and 9 loads with
+// immediate offsets instead of 9 address computations.  A real field is plain
+// structure-of-arrays with the site count padded to a multiple of 32.  Padding
+// sites are zero and no kernel writes them.  Neighbour links come through L1 /
+// L2; the lattice is periodic.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -33,6 +39,13 @@ __device__ __forceinline__ Cx<float> ldg_cx(const Cx<float>* p)
   return cx<float>(v.x, v.y);
 }
 
+// offset (in Cx<R> for K = 9, in reals for K = 1) of entry k of component m of site s
+template <int K>
+__host__ __device__ __forceinline__ long lay_index(long V, int m, int k, long s)
+{
+  return ((m * site_blocks(V) + (s >> 5)) * K + k) * 32 + (s & 31);
+}
+
 template <typename R>
 struct CField {
   const Cx<R>* __restrict__ p;
@@ -40,9 +53,9 @@ struct CField {
   __device__ __forceinline__ M3<R> ld(long site, int mu) const
   {
     M3<R> r;
-    const Cx<R>* q = p + (long)mu * 9 * V + site;
+    const Cx<R>* q = p + lay_index<9>(V, mu, 0, site);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + (long)k * V);
+    for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + 32 * k);
     return r;
   }
 };
@@ -54,16 +67,16 @@ struct WField {
   __device__ __forceinline__ M3<R> ld(long site, int mu) const
   {
     M3<R> r;
-    const Cx<R>* q = p + (long)mu * 9 * V + site;
+    const Cx<R>* q = p + lay_index<9>(V, mu, 0, site);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) r.e[k] = q[(long)k * V];
+    for (int k = 0; k < 9; ++k) r.e[k] = q[32 * k];
     return r;
   }
   __device__ __forceinline__ void st(long site, int mu, const M3<R>& r) const
   {
-    Cx<R>* q = p + (long)mu * 9 * V + site;
+    Cx<R>* q = p + lay_index<9>(V, mu, 0, site);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) q[(long)k * V] = r.e[k];
+    for (int k = 0; k < 9; ++k) q[32 * k] = r.e[k];
   }
 };
 

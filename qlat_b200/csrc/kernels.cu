@@ -690,59 +690,65 @@ cudaError_t launch_axpby(long n, void* y, double a, const void* x, double b, cud
   return cudaGetLastError();
 }
 
-// reference image [site][m][k] (doubles) <-> SoA [m][k/2 complex or 1 real][site]
+// reference image [site][m][k] (doubles) <-> device layout (gauge_common.cuh).
+// Sites [off, off + n) of a field of Vf sites; the image holds those n sites.
+// One thread per (component, site), sites fastest, so the device-side accesses
+// of a warp are coalesced.
 template <typename R>
-__global__ void k_aos_to_soa(long V, int m, int k_per, const double* __restrict__ aos, R* __restrict__ soa)
+__global__ void k_aos_to_store(long Vf, long off, long n, int m, int k_per, const double* __restrict__ aos,
+                               R* __restrict__ store)
 {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over V * m * k_per, SoA order
-  const long n = V * m * k_per;
-  if (i >= n) return;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * m) return;
+  const int mm = (int)(i / n);
+  const long s = i % n;
+  const double* src = aos + (s * m + mm) * k_per;
   if (k_per == 1) {
-    const long s = i % V, mm = i / V;
-    soa[i] = (R)aos[s * m + mm];
+    store[lay_index<1>(Vf, mm, 0, off + s)] = (R)src[0];
   } else {
-    // SoA element (mm, c, s, re/im): index ((mm*9 + c)*V + s)*2 + ri
-    const int ri = (int)(i & 1);
-    const long j = i >> 1;
-    const long s = j % V;
-    const long mc = j / V;
-    const long mm = mc / 9, c = mc % 9;
-    soa[i] = (R)aos[((s * m + mm) * 9 + c) * 2 + ri];
+    Cx<R>* dst = (Cx<R>*)store + lay_index<9>(Vf, mm, 0, off + s);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dst[32 * c] = cx<R>((R)src[2 * c], (R)src[2 * c + 1]);
   }
 }
 
 template <typename R>
-__global__ void k_soa_to_aos(long V, int m, int k_per, const R* __restrict__ soa, double* __restrict__ aos)
+__global__ void k_store_to_aos(long Vf, long off, long n, int m, int k_per, const R* __restrict__ store,
+                               double* __restrict__ aos)
 {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over AoS order
-  const long n = V * m * k_per;
-  if (i >= n) return;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * m) return;
+  const int mm = (int)(i / n);
+  const long s = i % n;
+  double* dst = aos + (s * m + mm) * k_per;
   if (k_per == 1) {
-    const long s = i / m, mm = i % m;
-    aos[i] = (double)soa[mm * V + s];
+    dst[0] = (double)store[lay_index<1>(Vf, mm, 0, off + s)];
   } else {
-    const int ri = (int)(i & 1);
-    const long j = i >> 1;  // (s*m + mm)*9 + c
-    const long c = j % 9;
-    const long sm = j / 9;
-    const long mm = sm % m, s = sm / m;
-    aos[i] = (double)soa[((mm * 9 + c) * V + s) * 2 + ri];
+    const Cx<R>* src = (const Cx<R>*)store + lay_index<9>(Vf, mm, 0, off + s);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const Cx<R> v = src[32 * c];
+      dst[2 * c] = (double)v.re;
+      dst[2 * c + 1] = (double)v.im;
+    }
   }
 }
 
 template <typename R>
-cudaError_t launch_aos_to_soa(const Geo& g, int m, int k_per, const double* aos, void* soa, cudaStream_t st)
+cudaError_t launch_aos_to_store(long Vf, long off, long n, int m, int k_per, const double* aos, void* store,
+                                cudaStream_t st)
 {
-  const long n = g.V * m * k_per;
-  k_aos_to_soa<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g.V, m, k_per, aos, (R*)soa);
+  const long t = n * m;
+  k_aos_to_store<R><<<(unsigned)((t + 255) / 256), 256, 0, st>>>(Vf, off, n, m, k_per, aos, (R*)store);
   return cudaGetLastError();
 }
 
 template <typename R>
-cudaError_t launch_soa_to_aos(const Geo& g, int m, int k_per, const void* soa, double* aos, cudaStream_t st)
+cudaError_t launch_store_to_aos(long Vf, long off, long n, int m, int k_per, const void* store, double* aos,
+                                cudaStream_t st)
 {
-  const long n = g.V * m * k_per;
-  k_soa_to_aos<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g.V, m, k_per, (const R*)soa, aos);
+  const long t = n * m;
+  k_store_to_aos<R><<<(unsigned)((t + 255) / 256), 256, 0, st>>>(Vf, off, n, m, k_per, (const R*)store, aos);
   return cudaGetLastError();
 }
 
@@ -774,8 +780,8 @@ cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st)
   template cudaError_t launch_hot_start<R>(const Geo&, void*, const uint32_t*, double, int, int*, cudaStream_t); \
   template cudaError_t launch_set_unit<R>(const Geo&, int, void*, cudaStream_t);                          \
   template cudaError_t launch_axpby<R>(long, void*, double, const void*, double, cudaStream_t);           \
-  template cudaError_t launch_aos_to_soa<R>(const Geo&, int, int, const double*, void*, cudaStream_t);    \
-  template cudaError_t launch_soa_to_aos<R>(const Geo&, int, int, const void*, double*, cudaStream_t);
+  template cudaError_t launch_aos_to_store<R>(long, long, long, int, int, const double*, void*, cudaStream_t); \
+  template cudaError_t launch_store_to_aos<R>(long, long, long, int, int, const void*, double*, cudaStream_t);
 
 QGB_INST(double)
 QGB_INST(float)

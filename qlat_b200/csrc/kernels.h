@@ -7,6 +7,11 @@
 namespace qgb
 {
 
+// Device layout (gauge_common.cuh): sites in blocks of 32; the number of
+// blocks and the padded site count of a field of V sites.
+__host__ __device__ inline long site_blocks(long V) { return (V + 31) >> 5; }
+__host__ __device__ inline long padded_sites(long V) { return site_blocks(V) << 5; }
+
 struct Geo {
   int d[4];      // X, Y, Z, T
   long V;        // sites of this lattice
@@ -127,12 +132,17 @@ cudaError_t launch_accept_batch(long Vtot, int nchain, const long* offs, const i
 // y = a x + b y over n reals
 template <typename R>
 cudaError_t launch_axpby(long n, void* y, double a, const void* x, double b, cudaStream_t st);
-// Layout conversion: reference image (AoS doubles, [site][m][k]) <-> SoA field.
-// k_per = 18 for color matrices, 1 for real fields.
+// Layout conversion: reference image (AoS doubles, [site][m][k]) <-> device
+// layout, for sites [off, off + n) of a field of Vf sites (the image holds
+// those n sites).  k_per = 18 for color matrices, 1 for real fields.
 template <typename R>
-cudaError_t launch_aos_to_soa(const Geo& g, int m, int k_per, const double* aos, void* soa, cudaStream_t st);
+cudaError_t launch_aos_to_store(long Vf, long off, long n, int m, int k_per, const double* aos, void* store,
+                                cudaStream_t st);
 template <typename R>
-cudaError_t launch_soa_to_aos(const Geo& g, int m, int k_per, const void* soa, double* aos, cudaStream_t st);
+cudaError_t launch_store_to_aos(long Vf, long off, long n, int m, int k_per, const void* store, double* aos,
+                                cudaStream_t st);
+// Elementwise conversion over n reals of two fields of the same layout
+// (n counts the padded storage).
 template <typename RI, typename RO>
 cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st);
 
