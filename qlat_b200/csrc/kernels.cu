@@ -14,6 +14,7 @@
 // order (warp shuffles, block, then one block over the partials), so results
 // are deterministic run to run.
 #include <cuda_runtime.h>
+#include <type_traits>
 #include <stdint.h>
 #include <string.h>
 
@@ -378,28 +379,38 @@ struct RngArg {
   uint32_t v[24];
 };
 
+// One link's momentum from its 8 Gaussians (make_g_rand_anti_hermitian_matrix,
+// matrix-hmc.h:125-142), stored in the field's precision.
+template <typename R>
+__device__ __forceinline__ void momentum_store(const WField<R>& Pf, long s, int mu, const double* b, double inv_sqrt3)
+{
+  const M3<double> m = x_make_anti_hermitian(b, inv_sqrt3);
+  M3<R> mr;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) mr.e[k] = cx<R>((R)m.e[k].re, (R)m.e[k].im);
+  Pf.st(s, mu, mr);
+}
+
 // set_g_rand_anti_hermitian_matrix_field: per site RngState(rs, gindex),
 // 4 x make_g_rand_anti_hermitian_matrix (matrix-hmc.h:125-142).
 template <typename R>
 __global__ void __launch_bounds__(128) k_rand_momentum(Geo g, RngArg ra, double s_sigma, double inv_sqrt3,
                                                        Cx<R>* P, int* ambiguous)
 {
+  // every lane of the warp stays to the end (warp-wide refills); lanes past
+  // the last site draw nothing
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= g.V) return;
+  const bool active = s < g.V;
   Rng base, rs;
   rng_import(base, ra.v);
-  rng_split_long(rs, base, (int64_t)s);
+  if (active) rng_split_long(rs, base, (int64_t)s);
   int amb = 0;
   const WField<R> Pf{P, g.V};
-  for (int mu = 0; mu < 4; ++mu) {
-    double b[8];
-    for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
-    const M3<double> m = x_make_anti_hermitian(b, inv_sqrt3);
-    M3<R> mr;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) mr.e[k] = cx<R>((R)m.e[k].re, (R)m.e[k].im);
-    Pf.st(s, mu, mr);
-  }
+  double b[8];
+  rng_gaussians_converged<32>(rs, s_sigma, active, &amb, [&](int i, double v) {
+    b[i & 7] = v;
+    if ((i & 7) == 7) momentum_store(Pf, s, i >> 3, b, inv_sqrt3);
+  });
   if (amb) atomicAdd(ambiguous, 1);
 }
 
@@ -473,22 +484,21 @@ __global__ void __launch_bounds__(128) k_rand_momentum_batch(long Vtot, int ncha
                                                              double inv_sqrt3, Cx<R>* P, int* ambiguous)
 {
   const long sg = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (sg >= Vtot) return;
-  const int c = chain_of(offs, nchain, sg);
-  Rng base, rs;
-  rng_import(base, rs24 + 24 * c);
-  rng_split_long(rs, base, (int64_t)(sg - offs[c]));
+  const bool active = sg < Vtot;
+  Rng rs;
+  if (active) {
+    const int c = chain_of(offs, nchain, sg);
+    Rng base;
+    rng_import(base, rs24 + 24 * c);
+    rng_split_long(rs, base, (int64_t)(sg - offs[c]));
+  }
   int amb = 0;
   const WField<R> Pf{P, Vtot};
-  for (int mu = 0; mu < 4; ++mu) {
-    double b[8];
-    for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
-    const M3<double> m = x_make_anti_hermitian(b, inv_sqrt3);
-    M3<R> mr;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) mr.e[k] = cx<R>((R)m.e[k].re, (R)m.e[k].im);
-    Pf.st(sg, mu, mr);
-  }
+  double b[8];
+  rng_gaussians_converged<32>(rs, s_sigma, active, &amb, [&](int i, double v) {
+    b[i & 7] = v;
+    if ((i & 7) == 7) momentum_store(Pf, sg, i >> 3, b, inv_sqrt3);
+  });
   if (amb) atomicAdd(ambiguous, 1);
 }
 
@@ -759,11 +769,33 @@ __global__ void k_convert(long n, const RI* in, RO* out)
     out[i] = (RO)in[i];
 }
 
+// four elements per thread: 16- or 32-byte loads and stores (n % 4 == 0, 16-byte aligned buffers)
+template <typename RI, typename RO>
+__global__ void k_convert4(long n4, const RI* __restrict__ in, RO* __restrict__ out)
+{
+  using I2 = typename std::conditional<sizeof(RI) == 8, double2, float2>::type;
+  using O2 = typename std::conditional<sizeof(RO) == 8, double2, float2>::type;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long)gridDim.x * blockDim.x) {
+    const I2 a = reinterpret_cast<const I2*>(in)[2 * i], b = reinterpret_cast<const I2*>(in)[2 * i + 1];
+    O2 c, d;
+    c.x = (decltype(c.x))a.x;
+    c.y = (decltype(c.y))a.y;
+    d.x = (decltype(d.x))b.x;
+    d.y = (decltype(d.y))b.y;
+    reinterpret_cast<O2*>(out)[2 * i] = c;
+    reinterpret_cast<O2*>(out)[2 * i + 1] = d;
+  }
+}
+
 template <typename RI, typename RO>
 cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st)
 {
-  const long blocks = (n + 255) / 256;
-  k_convert<RI, RO><<<(unsigned)(blocks < 148 * 32 ? blocks : 148 * 32), 256, 0, st>>>(n, (const RI*)in, (RO*)out);
+  const bool vec = n % 4 == 0 && ((uintptr_t)in % 16) == 0 && ((uintptr_t)out % 16) == 0;
+  const long work = vec ? n / 4 : n;
+  const long blocks = (work + 255) / 256;
+  const unsigned grid = (unsigned)(blocks < 148 * 16 ? blocks : 148 * 16);
+  if (vec) k_convert4<RI, RO><<<grid, 256, 0, st>>>(work, (const RI*)in, (RO*)out);
+  else k_convert<RI, RO><<<grid, 256, 0, st>>>(n, (const RI*)in, (RO*)out);
   return cudaGetLastError();
 }
 

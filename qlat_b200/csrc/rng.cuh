@@ -391,15 +391,11 @@ QGB_HD void rng_split_long(Rng& out, const Rng& rs0, int64_t sindex)
 }
 
 // rand_gen (rng-state.cpp:203-238): three cached u64 per hash of "[index]".
-QGB_HD uint64_t rng_rand_gen(Rng& rs)
+// New cache block of rand_gen: SHA-256 of "[index]" (or "[type,index]")
+// appended to the state, with the already advanced index; caches three of the
+// four 64-bit words and returns the fourth.
+QGB_HD uint64_t rng_refill(Rng& rs)
 {
-  rs.index += 1;
-  if (rs.cacheAvail > 0) {
-    rs.cacheAvail -= 1;
-    const uint64_t r = rs.cache[rs.cacheAvail];
-    rs.cache[rs.cacheAvail] = 0;
-    return r;
-  }
   uint8_t blk[64];
   for (int i = 0; i < 64; ++i) blk[i] = 0;
   int n = 0;
@@ -421,6 +417,19 @@ QGB_HD uint64_t rng_rand_gen(Rng& rs)
   rs.cache[2] = ((uint64_t)h[4] << 32) | h[5];
   rs.cacheAvail = 3;
   return ((uint64_t)h[6] << 32) | h[7];
+}
+
+// rand_gen (rng-state.cpp:215-238)
+QGB_HD uint64_t rng_rand_gen(Rng& rs)
+{
+  rs.index += 1;
+  if (rs.cacheAvail > 0) {
+    rs.cacheAvail -= 1;
+    const uint64_t r = rs.cache[rs.cacheAvail];
+    rs.cache[rs.cacheAvail] = 0;
+    return r;
+  }
+  return rng_refill(rs);
 }
 
 // u_rand_gen (rng-state.cpp:240-246): u * 2^-64 * (upper - lower) + lower.
@@ -462,6 +471,92 @@ QGB_HD double rng_g_rand_gen(Rng& rs, double center, double sigma, int* ambiguou
   rs.gaussianAvail = 1;
   return QGB_DADD(QGB_DMUL(QGB_DMUL(v2, fac), sigma), center);
 }
+
+#if defined(__CUDACC__)
+// N successive g_rand_gen(rs, 0, sigma) values of each lane's own stream,
+// handed to sink(i, value) in order -- the same values and the same final
+// state as N calls of rng_g_rand_gen<true> -- with the SHA-256 refills of a
+// warp executed together.  Called by all 32 lanes of a warp (lanes with
+// active == false take part in the synchronisation only).
+//
+// Each lane advances its stream through the cheap steps (index increments,
+// cache pops, the polar accept test, the logarithm) until it needs a new cache
+// block; then every lane that is blocked computes its block at once.  Drawing
+// stream by stream instead leaves the lanes' refills at different times, and a
+// warp runs each lane's 64-round compression with most lanes idle.
+template <int N, typename Sink>
+__device__ __forceinline__ void rng_gaussians_converged(Rng& rs, double sigma, bool active, int* ambiguous,
+                                                        Sink&& sink)
+{
+  int produced = 0;
+  if (active && rs.gaussianAvail && N > 0) {  // a Gaussian cached by an earlier call comes first
+    rs.index += 1;
+    rs.gaussianAvail = 0;
+    sink(produced++, QGB_DADD(QGB_DMUL(rs.gaussian, sigma), 0.0));
+  }
+  int stage = 0;  // 0: next call starts a pair; 1: v1 next; 2: v2 next
+  int num_try = 1;
+  double v1 = 0.0;
+  bool done = !active || produced >= N;
+  bool need = false;
+  // take one uniform of [-1, 1) (u_rand_gen(rs, 1, -1)) into the polar step
+  auto consume = [&](uint64_t u) {
+    const double x = QGB_DADD(QGB_DMUL(QGB_DMUL(QGB_U2D(u), 5.421010862427522e-20), 2.0), -1.0);
+    if (stage == 1) {
+      v1 = x;
+      stage = 2;
+      return;
+    }
+    const double v2 = x;
+    const double rsq = QGB_DADD(QGB_DMUL(v1, v1), QGB_DMUL(v2, v2));
+    num_try++;
+    if (num_try < 10000 && (rsq >= 1.0 || rsq == 0)) {
+      stage = 1;
+      return;
+    }
+    stage = 0;
+    if (num_try > 9999) {
+      sink(produced++, 1e+10);
+    } else {
+      const double lg = log_cr(rsq, ambiguous);
+      const double fac = QGB_DSQRT(QGB_DDIV(QGB_DMUL(-2.0, lg), rsq));
+      sink(produced++, QGB_DADD(QGB_DMUL(QGB_DMUL(v2, fac), sigma), 0.0));
+      const double g1 = QGB_DMUL(v1, fac);
+      if (produced < N) {
+        rs.index += 1;  // the next g_rand_gen call returns the cached value
+        sink(produced++, QGB_DADD(QGB_DMUL(g1, sigma), 0.0));
+      } else {
+        rs.gaussian = g1;
+        rs.gaussianAvail = 1;
+      }
+    }
+    if (produced >= N) done = true;
+  };
+  while (true) {
+    while (!done && !need) {
+      if (stage == 0) {
+        rs.index += 1;  // g_rand_gen call that starts a pair
+        num_try = 1;
+        stage = 1;
+      }
+      rs.index += 1;  // rand_gen
+      if (rs.cacheAvail > 0) {
+        rs.cacheAvail -= 1;
+        const uint64_t u = rs.cache[rs.cacheAvail];
+        rs.cache[rs.cacheAvail] = 0;
+        consume(u);
+      } else {
+        need = true;
+      }
+    }
+    if (__all_sync(0xffffffffu, done)) break;
+    if (need) {
+      need = false;
+      consume(rng_refill(rs));
+    }
+  }
+}
+#endif
 
 // ------------------------------------------------------------------------
 // Exactly rounded complex / matrix arithmetic in the reference's order

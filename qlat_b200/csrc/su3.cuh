@@ -530,6 +530,14 @@ QGB_HD Cx<R> cmul(Cx<R> a, Cx<R> b)
   return cx<R>(fma(a.re, b.re, -a.im * b.im), fma(a.re, b.im, a.im * b.re));
 }
 
+#if defined(__CUDACC__)
+// 1/n for the exponential's recursion (compile-time constants, so the
+// correctly rounded quotients)
+static __constant__ double qgb_inv_n[21] = {0.0,        1.0 / 1,  1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,  1.0 / 6,
+                                            1.0 / 7,    1.0 / 8,  1.0 / 9,  1.0 / 10, 1.0 / 11, 1.0 / 12, 1.0 / 13,
+                                            1.0 / 14,   1.0 / 15, 1.0 / 16, 1.0 / 17, 1.0 / 18, 1.0 / 19, 1.0 / 20};
+#endif
+
 // The reference's exponential, sum_{n=0}^{20} a^n / n! (the order-20 Taylor
 // polynomial that make_matrix_exp evaluates in Horner form,
 // matrix-hmc.h:155-167), evaluated through the Cayley-Hamilton theorem: with
@@ -540,7 +548,9 @@ QGB_HD Cx<R> cmul(Cx<R> a, Cx<R> b)
 // the 19 matrix products of the Horner form.  It is the same polynomial, so it
 // keeps the reference's truncation (which matters when |a| reaches ~3, as in
 // gradient flow of rough fields with large steps) and differs from it only by
-// rounding.
+// rounding.  In FP32 the recursion stops as soon as the omitted terms are below
+// FP32 resolution (the same polynomial to FP32 accuracy, fewer steps for the
+// small arguments of molecular dynamics).
 template <typename R>
 QGB_HD M3<R> exp_ch(const M3<R>& a)
 {
@@ -559,9 +569,7 @@ QGB_HD M3<R> exp_ch(const M3<R>& a)
   const Cx<R> d = cx<R>(d0.re + d1.re + d2.re, d0.im + d1.im + d2.im);
   Cx<R> x = cx<R>(R(1), R(0)), y = cx<R>(R(0), R(0)), z = cx<R>(R(0), R(0));
   Cx<R> f0 = x, f1 = y, f2 = z;
-#pragma unroll 4
-  for (int n = 1; n <= 20; ++n) {
-    const R inv = R(1) / R(n);
+  auto step = [&](R inv) {
     const Cx<R> zd = cmul(z, d), zs = cmul(z, s), zt = cmul(z, t);
     const Cx<R> xn = cx<R>(zd.re * inv, zd.im * inv);
     const Cx<R> yn = cx<R>((x.re - zs.re) * inv, (x.im - zs.im) * inv);
@@ -575,7 +583,33 @@ QGB_HD M3<R> exp_ch(const M3<R>& a)
     f1.im += y.im;
     f2.re += z.re;
     f2.im += z.im;
+  };
+#if defined(__CUDA_ARCH__)
+  if constexpr (sizeof(R) == 4) {
+    // FP32: after step n the partial sums are the Taylor polynomial of order n.
+    // Stop once the remainder, bounded with the Frobenius norm by
+    // sum_{k>n} |a|^k / k! <= 2 |a|^(n+1) / (n+1)! when |a| < (n+2)/2, is below
+    // 2^-27 (under FP32 resolution); large |a| still runs all 20 terms.
+    R nrm2 = R(0);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) nrm2 = fma(a.e[i].re, a.e[i].re, fma(a.e[i].im, a.e[i].im, nrm2));
+    const R nrm = sqrt(nrm2);
+    R term = R(1);  // |a|^n / n!
+#pragma unroll 1
+    for (int n = 1; n <= 20; ++n) {
+      const R inv = __frcp_rn(R(n));  // the correctly rounded 1 / n
+      step(inv);
+      term *= nrm * inv;
+      if (R(2) * term * nrm < R(7.450580596923828e-9) * R(n + 1) && nrm < R(0.5) * R(n + 2)) break;
+    }
+  } else {
+    // FP64: all 20 steps, 1/n from a table of the correctly rounded values
+#pragma unroll 1
+    for (int n = 1; n <= 20; ++n) step(R(qgb_inv_n[n]));
   }
+#else
+  for (int n = 1; n <= 20; ++n) step(R(1) / R(n));
+#endif
   M3<R> r;
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
