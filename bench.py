@@ -324,7 +324,7 @@ def our_arm(args):
     flops_site = 4 * (6 * 11 + 1) * 198.0
     tflops = flops_site * V / (t_fu / n_fu / 1e3) / 1e12 if n_fu else None
     traffic = None
-    tf_path = os.path.join(ROOT, "profiles", "force_update_traffic.json")
+    tf_path = os.path.join(ROOT, "profiles", "force_update_evolve_traffic.json")
     if os.path.exists(tf_path):
         try:
             traffic = json.load(open(tf_path)).get("bytes_per_launch_full_size")

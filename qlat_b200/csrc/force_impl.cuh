@@ -356,7 +356,7 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
 // blocks per SM (caps registers), threads per link (SPLIT = 2 gives each link
 // to a lane pair, each doing 3 of the 6 signed directions, combined by a
 // shuffle), and the site mapping and staple evaluation: MAP 0 runs blocks of
-// consecutive sites with mu = blockIdx.y and staple_sum_rt; MAP 1 gives each
+// consecutive sites (block = 4 * site block + mu) and staple_sum_rt; MAP 1 gives each
 // block the four links of a compact tile of BS/4 sites (4 x 2 x 2 x 2 for 128
 // threads, 4 x 4 x 2 x 2 for 256), one warp-group per mu, so the four
 // directions share the tile's neighbourhood in L1 (it needs the lattice
@@ -389,10 +389,14 @@ template <typename R, int MODE, bool RECT, int BS, int MINB, int SPLIT, int MAP>
 __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 {
   const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
+  // linear maps: block b = 4 * (site block) + mu, so the four directions of a
+  // site block run back to back and share its neighbourhood in L2 (a grid
+  // that sweeps the lattice once per direction reads the link field from DRAM
+  // four times when it exceeds L2)
   if constexpr (MAP >= 2) {
-    const long t = (long)blockIdx.x * BS + threadIdx.x;
+    const long t = (long)(blockIdx.x >> 2) * BS + threadIdx.x;
     if (t >= g.V) return;
-    const int mu = blockIdx.y;
+    const int mu = blockIdx.x & 3;
     const M3<R> S = staple_sum_fast<R, RECT, MAP == 3>((const Cx<R>*)a.U, g, (int)t, mu, cp, cr);
     force_epilogue<R, MODE>(a, CField<R>{(const Cx<R>*)a.U, g.V}, g.V, t, mu, S, a.beta);
     return;
@@ -400,10 +404,10 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
   long s0;
   int h, mu;
   if (MAP == 0) {
-    const long t = (long)blockIdx.x * BS + threadIdx.x;
+    const long t = (long)(blockIdx.x >> 2) * BS + threadIdx.x;
     s0 = t / SPLIT;
     h = (int)(t % SPLIT);
-    mu = blockIdx.y;
+    mu = blockIdx.x & 3;
   } else {
     // tile of Tile<BS>::sites sites; thread = mu * sites + site-in-tile
     using TL = Tile<BS>;
@@ -453,7 +457,7 @@ cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cud
   if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
   const bool fast = MAP >= 2 && SPLIT == 1 && g.off == 0 && padded_sites(g.V) * 36 < 2147483647L;
   if (MAP >= 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
-  dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)((g.V * SPLIT + BS - 1) / BS), 4);
+  dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)(4 * ((g.V * SPLIT + BS - 1) / BS)), 1);
   const bool rect = a.c1 != 0.0;
 #define QGB_LAUNCH(M)                                                                                  \
   if (rect) k_force<R, M, true, BS, MINB, SPLIT, MAP><<<grid, BS, 0, st>>>(g, a); \
@@ -494,7 +498,7 @@ inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* 
 }
 
 // Batched force: every chain of a batch in one launch, one thread per link of
-// the concatenated field (Vtot sites, mu = blockIdx.y).  Each thread finds its
+// the concatenated field (Vtot sites, block = 4 * site block + mu).  Each thread finds its
 // chain by binary search over the chain offsets and uses that chain's lattice,
 // beta and c1.  RECT is set when any chain has c1 != 0 (Wilson chains then add
 // rectangle terms with weight 0).
@@ -502,12 +506,12 @@ template <typename R, int MODE, bool RECT>
 __global__ void __launch_bounds__(128) k_force_batch(long Vtot, int nchain, const long* __restrict__ offs,
                                                      const ChainInfo* __restrict__ chains, ForceArgs a)
 {
-  const long sg = (long)blockIdx.x * 128 + threadIdx.x;
+  const long sg = (long)(blockIdx.x >> 2) * 128 + threadIdx.x;  // block = 4 * (site block) + mu
   if (sg >= Vtot) return;
   const int c = chain_of(offs, nchain, sg);
   const ChainInfo ci = chains[c];
   const Geo g = chain_geo(ci);
-  const int mu = blockIdx.y;
+  const int mu = blockIdx.x & 3;
   const CField<R> U{(const Cx<R>*)a.U, Vtot};
   const Coord x = coord_of(g, sg - ci.off);
   const R cp = R(1.0 - 8.0 * ci.c1), cr = R(ci.c1);
@@ -519,7 +523,7 @@ template <typename R>
 cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
                                ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
-  dim3 grid((unsigned)((Vtot + 127) / 128), 4);
+  dim3 grid((unsigned)(4 * ((Vtot + 127) / 128)), 1);
 #define QGB_LAUNCH(M)                                                                      \
   if (rect) k_force_batch<R, M, true><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a); \
   else k_force_batch<R, M, false><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);
