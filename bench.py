@@ -164,6 +164,22 @@ def cpu_baseline(lattice):
                       f"extrapolated to 32 pairs + ends per trajectory ({wall:.1f} s of CPU work)"}
 
 
+def max_over_ranks(ms: float, dist, device) -> float:
+    """The slowest rank's time: every rank passes its own CUDA-event time and
+    gets the maximum back (all ranks must call it, in the same order)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world: int, units_per_rank: int, ms: float) -> float:
+    """Whole-job units per second: every rank processed units_per_rank in at most ms."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def our_arm(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -237,11 +253,7 @@ def our_arm(args):
             q.prof_enable(False)
         launches = q.launch_count() - l0
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
         return ms, dhs, flags, launches
 
     # warm-up (W trajectories of each form; always accepted state evolves normally)
@@ -291,12 +303,8 @@ def our_arm(args):
             _ = q.gf_avg_plaq(gf)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms_e2e = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e2e = float(t.item())
-        e2e = {"value": world * n_e2e / (ms_e2e / 1e3), "unit": "traj/s",
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+        e2e = {"value": job_throughput(world, n_e2e, ms_e2e), "unit": "traj/s",
                "h2d_bytes_per_step": V * 4 * 9 * 16, "d2h_bytes_per_step": 8 * 2 + 8 * 6}
 
     if rank != 0:
@@ -304,8 +312,8 @@ def our_arm(args):
             dist.destroy_process_group()
         return 0
 
-    value = world * args.steps / (ms_mixed / 1e3)
-    fp64_value = world * args.steps / (ms_fp64 / 1e3)
+    value = job_throughput(world, args.steps, ms_mixed)
+    fp64_value = job_throughput(world, args.steps, ms_fp64)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
