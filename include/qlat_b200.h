@@ -200,6 +200,22 @@ int qgb_clf_topology_field(qgb_field* topf, const qgb_field* gf);
 /* gf_topology_clf(gf) = glb_sum of clf_topology_field (topology.pyx:89-96). */
 int qgb_gf_topology_clf(const qgb_field* gf, double* out);
 
+/* The 5-loop improved topological charge (hep-lat/9701012 Eq. 2-7): the five
+ * terms c_k / (m n)^2 q_{m x n} of the m x n clover-leaf densities, (m, n) =
+ * (1,1), (2,2), (1,2), (1,3), (3,3), the 1 x 2 and 1 x 3 leaves averaged with
+ * their transposes.
+ * Replaces clf_topology_field_5_terms (qcd.cpp:425-489; topology.pyx:121-140,
+ * gf_topology_terms_field / gf_topology_terms): topf real, multiplicity 5, the
+ * links' precision. */
+int qgb_clf_topology_field_5_terms(qgb_field* topf, const qgb_field* gf);
+/* Replaces clf_topology_field_5 (qcd.cpp:491-509; topology.pyx:98-108,
+ * gf_topology_field): per-site sum of the five terms, topf multiplicity 1. */
+int qgb_clf_topology_field_5(qgb_field* topf, const qgb_field* gf);
+/* The five terms summed over the lattice (topology.pyx:130-140, gf_topology_terms). */
+int qgb_gf_topology_terms(const qgb_field* gf, double out[5]);
+/* Their sum, the improved charge (topology.pyx:110-118, gf_topology). */
+int qgb_gf_topology(const qgb_field* gf, double* out);
+
 /* ---- instrumentation (timer.h:48-414 TIMER / Timer::display) ------------ */
 
 /* Per-kernel-class device timing with CUDA events on the library stream. */

@@ -98,6 +98,8 @@ def lib():
             "or_gf_energy_density": (ctypes.c_double, [_dbl_p, _int4]),
             "or_clf_topology_field": (None, [_dbl_p, _dbl_p, _int4]),
             "or_gf_topology_clf": (ctypes.c_double, [_dbl_p, _int4]),
+            "or_clf_topology_field_5_terms": (None, [_dbl_p, _dbl_p, _int4]),
+            "or_gf_topology": (ctypes.c_double, [_dbl_p, _int4]),
             "or_run_hmc_evolve_fg": (ctypes.c_double, [_dbl_p, _dbl_p, _int4, ctypes.c_double, ctypes.c_double,
                                                        ctypes.c_int, ctypes.c_double]),
             "or_run_hmc_evolve_leapfrog": (ctypes.c_double, [_dbl_p, _dbl_p, _int4, ctypes.c_double,
@@ -270,6 +272,18 @@ def clf_topology_field(gf, total_site) -> np.ndarray:
 
 def gf_topology_clf(gf, total_site) -> float:
     return lib().or_gf_topology_clf(_p(gf), _dims(total_site))
+
+
+def clf_topology_field_5_terms(gf, total_site) -> np.ndarray:
+    """qcd.cpp:425-489: (V, 5) terms of the improved charge density."""
+    tf = np.zeros((volume(total_site), 5), dtype=np.float64)
+    lib().or_clf_topology_field_5_terms(_p(tf), _p(gf), _dims(total_site))
+    return tf
+
+
+def gf_topology(gf, total_site) -> float:
+    """topology.pyx:98-108: the 5-loop improved charge."""
+    return lib().or_gf_topology(_p(gf), _dims(total_site))
 
 
 def run_hmc_evolve(gm, gf, total_site, beta, c1, n_step, md_time=1.0, integrator="force-gradient") -> float:

@@ -914,6 +914,98 @@ void or_clf_topology_field(double* topf, const double* gf, const int dims[4])
   }
 }
 
+/* qcd.cpp:11-31: the four m x n leaves at x in the (mu, nu) plane, times 1/4;
+ * each path of qcd-acc.h:23-41 with direction counts (m, n, m, n) expanded
+ * into unit steps */
+static cm clover_leaf_mn(const double* gf, const geo_t* g, const int x[4], int mu, int m, int nu, int n)
+{
+  const int dirs[4][4] = {{mu, nu, -mu - 1, -nu - 1},
+                          {-mu - 1, -nu - 1, mu, nu},
+                          {nu, -mu - 1, -nu - 1, mu},
+                          {-nu - 1, mu, nu, -mu - 1}};
+  const int reps[4][4] = {{m, n, m, n}, {m, n, m, n}, {n, m, n, m}, {n, m, n, m}};
+  cm acc = m_zero();
+  for (int l = 0; l < 4; ++l) {
+    int path[32];
+    int len = 0;
+    for (int i = 0; i < 4; ++i)
+      for (int r = 0; r < reps[l][i]; ++r) path[len++] = dirs[l][i];
+    cm w = wilson_line(gf, g, x, path, len);
+    m_add_to(&acc, &w);
+  }
+  return m_rscale(0.25, &acc);
+}
+
+/* qcd.cpp:64-79 on the six planes' leaves of qcd.cpp:536-568 (m != n: the
+ * average of the m x n and n x m leaves) */
+static double clf_topology_density_mn(const double* gf, const geo_t* g, const int x[4], int m, int n)
+{
+  const int pl[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+  const double PI = 3.141592653589793;
+  cm arr[6];
+  for (int k = 0; k < 6; ++k) {
+    cm v = clover_leaf_mn(gf, g, x, pl[k][0], m, pl[k][1], n);
+    if (m != n) {
+      cm w = clover_leaf_mn(gf, g, x, pl[k][0], n, pl[k][1], m);
+      m_add_to(&v, &w);
+      v = m_rscale(0.5, &v);
+    }
+    cm va = m_adj(&v);
+    cm d = v;
+    m_sub_to(&d, &va);
+    arr[k] = m_rscale(0.5, &d);
+  }
+  const double fac = -1.0 / (4.0 * PI * PI);
+  double sum = 0.0;
+  cm t = m_mul(&arr[1], &arr[4]);
+  sum -= m_trace(&t).re;
+  t = m_mul(&arr[2], &arr[3]);
+  sum += m_trace(&t).re;
+  t = m_mul(&arr[5], &arr[0]);
+  sum += m_trace(&t).re;
+  return fac * sum;
+}
+
+/* qcd.cpp:425-489 (hep-lat/9701012 Eq. 2-7): the five terms of the improved
+ * topological charge density, topf[5 * site + k] */
+void or_clf_topology_field_5_terms(double* topf, const double* gf, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+  const double c5 = 1.0 / 20.0;
+  const double c1 = (19.0 - 55.0 * c5) / 9.0;
+  const double c2 = (1.0 - 64.0 * c5) / 9.0;
+  const double c3 = (-64.0 + 640.0 * c5) / 45.0;
+  const double c4 = 1.0 / 5.0 - 2.0 * c5;
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    double* v = topf + 5 * i;
+    v[0] = c1 * clf_topology_density_mn(gf, &g, x, 1, 1);
+    v[1] = c2 / 16.0 * clf_topology_density_mn(gf, &g, x, 2, 2);
+    v[2] = c3 / 4.0 * clf_topology_density_mn(gf, &g, x, 1, 2);
+    v[3] = c4 / 9.0 * clf_topology_density_mn(gf, &g, x, 1, 3);
+    v[4] = c5 / 81.0 * clf_topology_density_mn(gf, &g, x, 3, 3);
+  }
+}
+
+/* topology.pyx:98-108 -> qcd.cpp:491-509: the improved charge (sum of the
+ * five terms over all sites) */
+double or_gf_topology(const double* gf, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+  double* t = (double*)malloc(5 * g.vol * sizeof(double));
+  or_clf_topology_field_5_terms(t, gf, dims);
+  double s = 0.0;
+  for (long i = 0; i < g.vol; ++i) {
+    double si = 0.0;
+    for (int k = 0; k < 5; ++k) si += t[5 * i + k];
+    s += si;
+  }
+  free(t);
+  return s;
+}
+
 double or_gf_topology_clf(const double* gf, const int dims[4])
 {
   const geo_t g = mk_geo(dims);

@@ -71,6 +71,10 @@ void or_gf_energy_density_field(double* fd, const double* gf, const int dims[4])
 double or_gf_energy_density(const double* gf, const int dims[4]);
 void or_clf_topology_field(double* topf, const double* gf, const int dims[4]);
 double or_gf_topology_clf(const double* gf, const int dims[4]);
+/* qcd.cpp:425-489: the five terms of the improved (5-loop) charge density, topf[5 * site + k] */
+void or_clf_topology_field_5_terms(double* topf, const double* gf, const int dims[4]);
+/* topology.pyx:98-108: the improved charge, summed over the lattice */
+double or_gf_topology(const double* gf, const int dims[4]);
 /* Omelyan force-gradient trajectory (hmc.pyx:170-188); returns delta_h. */
 double or_run_hmc_evolve_fg(double* gm, double* gf, const int dims[4], double beta, double c1,
                             int n_step, double md_time);

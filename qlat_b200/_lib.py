@@ -76,6 +76,10 @@ SIGNATURES = {
     "qgb_su3_dexp_adjoint": [c_field, c_field, c_field],
     "qgb_clf_topology_field": [c_field, c_field],
     "qgb_gf_topology_clf": [c_field, c_dbl_p],
+    "qgb_clf_topology_field_5_terms": [c_field, c_field],
+    "qgb_clf_topology_field_5": [c_field, c_field],
+    "qgb_gf_topology_terms": [c_field, c_dbl_p],
+    "qgb_gf_topology": [c_field, c_dbl_p],
     "qgb_prof_enable": [ctypes.c_int32],
     "qgb_prof_reset": [],
     "qgb_prof_get": [ctypes.c_char_p, c_dbl_p, c_i64_p],

@@ -291,6 +291,24 @@ int clover_slot(const qgb_field* gf, qgb_field* ef, qgb_field* qf, int slot)
   return QGB_OK;
 }
 
+// The five terms of the 5-loop improved charge into results[slot .. slot + 4]
+// (and the optional terms / total fields).
+int topology_5li_slot(const qgb_field* gf, qgb_field* terms, qgb_field* total, int slot)
+{
+  const Geo g = geo_of(gf);
+  const int nb = qgb::reduce_blocks(g);
+  QGB_RC(ensure_partials((size_t)nb * 5));
+  Prof p("topology_5li");
+  if (gf->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_topology_5li<double>(g, gf->d, terms ? terms->d : nullptr, total ? total->d : nullptr,
+                                                  g_ctx.partials, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_topology_5li<float>(g, gf->d, terms ? terms->d : nullptr, total ? total->d : nullptr,
+                                                 g_ctx.partials, g_ctx.stream));
+  QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 5, nb, g_ctx.results, slot, g_ctx.stream));
+  return QGB_OK;
+}
+
 double gf_hamilton_from(double sp, double sr, double beta, double c1)
 {
   // hmc.cpp:254-277
@@ -1106,6 +1124,45 @@ int qgb_gf_topology_clf(const qgb_field* gf, double* out)
   double r[2];
   QGB_RC(read_results(0, 2, r));
   *out = r[1];
+  return QGB_OK;
+}
+
+int qgb_clf_topology_field_5_terms(qgb_field* topf, const qgb_field* gf)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_clf_topology_field_5_terms"));
+  QGB_RC(check_field(topf, QGB_KIND_REAL, "qgb_clf_topology_field_5_terms"));
+  QGB_CHECK(gf->mult == 4 && same_geo(topf, gf) && topf->mult == 5 && topf->prec == gf->prec, QGB_ERR_MISMATCH,
+            "qgb_clf_topology_field_5_terms: topf must be a real field of multiplicity 5 in the links' precision");
+  return topology_5li_slot(gf, topf, nullptr, 0);
+}
+
+int qgb_clf_topology_field_5(qgb_field* topf, const qgb_field* gf)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_clf_topology_field_5"));
+  QGB_RC(check_field(topf, QGB_KIND_REAL, "qgb_clf_topology_field_5"));
+  QGB_CHECK(gf->mult == 4 && same_geo(topf, gf) && topf->mult == 1 && topf->prec == gf->prec, QGB_ERR_MISMATCH,
+            "qgb_clf_topology_field_5: topf must be a real field of multiplicity 1 in the links' precision");
+  return topology_5li_slot(gf, nullptr, topf, 0);
+}
+
+int qgb_gf_topology_terms(const qgb_field* gf, double out[5])
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_topology_terms"));
+  QGB_CHECK(gf->mult == 4 && out, QGB_ERR_INVALID_ARG, "qgb_gf_topology_terms: bad argument");
+  QGB_RC(topology_5li_slot(gf, nullptr, nullptr, 0));
+  return read_results(0, 5, out);
+}
+
+int qgb_gf_topology(const qgb_field* gf, double* out)
+{
+  QGB_CTX();
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_gf_topology: null output");
+  double t[5];
+  QGB_RC(qgb_gf_topology_terms(gf, t));
+  *out = t[0] + t[1] + t[2] + t[3] + t[4];
   return QGB_OK;
 }
 

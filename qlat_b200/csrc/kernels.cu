@@ -319,6 +319,134 @@ cudaError_t launch_clover(const Geo& g, const void* U, void* e_field, void* q_fi
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------
+// 5-loop improved topological charge (qcd.cpp:425-489, hep-lat/9701012)
+
+// Site index of x + the offsets (o0, o1, o2, o3), periodic.
+__device__ __forceinline__ long site_of4(const Geo& g, int y0, int y1, int y2, int y3)
+{
+  return (long)y0 + (long)g.d[0] * ((long)y1 + (long)g.d[1] * ((long)y2 + (long)g.d[2] * (long)y3));
+}
+
+// Sum of the four m x n leaves at x in the (mu, nu) plane (qcd.cpp:11-31,
+// without its 1/4): each a Wilson line of qcd-acc.h:23-41 walked link by link
+// -- forward steps multiply by U_dir(y), backward steps by U_dir(y - dir)^+.
+template <typename R>
+__device__ M3<R> leaf_sum_mn(const CField<R>& U, const Geo& g, const Coord& x, int mu, int m, int nu, int n)
+{
+  M3<R> acc = m3_zero<R>();
+#pragma unroll 1
+  for (int l = 0; l < 4; ++l) {
+    // leaves (mu m, nu n, -mu m, -nu n), (-mu m, -nu n, mu m, nu n),
+    //        (nu n, -mu m, -nu n, mu m), (-nu n, mu m, nu n, -mu m)
+    const int first = l < 2 ? mu : nu, second = l < 2 ? nu : mu;
+    const int cf = l < 2 ? m : n, cs = l < 2 ? n : m;
+    const int sf = (l == 0 || l == 2) ? 1 : -1;  // sign of the first leg
+    const int ss = (l == 0 || l == 3) ? 1 : -1;  // sign of the second leg
+    int y0 = x.c[0], y1 = x.c[1], y2 = x.c[2], y3 = x.c[3];
+    M3<R> w = m3_unit<R>();
+    bool first_link = true;
+#pragma unroll 1
+    for (int leg = 0; leg < 4; ++leg) {
+      const int dir = (leg & 1) ? second : first;
+      const int cnt = (leg & 1) ? cs : cf;
+      const int sgn = ((leg & 1) ? ss : sf) * (leg < 2 ? 1 : -1);
+#pragma unroll 1
+      for (int r = 0; r < cnt; ++r) {
+        if (sgn < 0) {
+          y0 = dir == 0 ? wrap(y0 - 1, g.d[0]) : y0;
+          y1 = dir == 1 ? wrap(y1 - 1, g.d[1]) : y1;
+          y2 = dir == 2 ? wrap(y2 - 1, g.d[2]) : y2;
+          y3 = dir == 3 ? wrap(y3 - 1, g.d[3]) : y3;
+        }
+        const M3<R> u = U.ld(site_of4(g, y0, y1, y2, y3), dir);
+        if (first_link) w = sgn > 0 ? u : adj(u);  // 1 * u is u exactly
+        else w = sgn > 0 ? mul(w, u) : mul_adj(w, u);
+        first_link = false;
+        if (sgn > 0) {
+          y0 = dir == 0 ? wrap(y0 + 1, g.d[0]) : y0;
+          y1 = dir == 1 ? wrap(y1 + 1, g.d[1]) : y1;
+          y2 = dir == 2 ? wrap(y2 + 1, g.d[2]) : y2;
+          y3 = dir == 3 ? wrap(y3 + 1, g.d[3]) : y3;
+        }
+      }
+    }
+    add_to(acc, w);
+  }
+  return acc;
+}
+
+// F = (C - C^+)/2 of the (averaged) m x n leaf C of plane p (qcd.cpp:536-568)
+template <typename R>
+__device__ M3<R> leaf_f_mn(const CField<R>& U, const Geo& g, const Coord& x, int p, int m, int n)
+{
+  const int mu = p < 3 ? 0 : (p < 5 ? 1 : 2);
+  const int nu = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
+  M3<R> c = scale(R(0.25), leaf_sum_mn(U, g, x, mu, m, nu, n));
+  if (m != n) {
+    add_to(c, scale(R(0.25), leaf_sum_mn(U, g, x, mu, n, nu, m)));
+    c = scale(R(0.5), c);
+  }
+  M3<R> f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      f.e[3 * i + j] = cx<R>(R(0.5) * (c.e[3 * i + j].re - c.e[3 * j + i].re),
+                             R(0.5) * (c.e[3 * i + j].im + c.e[3 * j + i].im));
+  return f;
+}
+
+// Per site the five terms c_k / (m n)^2 * q_{m x n} (terms field, multiplicity
+// 5, optional), their per-site sum (total field, optional), and the block
+// partial sums of the five terms.
+template <typename R>
+__global__ void __launch_bounds__(RED_BS) k_topology_5li(Geo g, const Cx<R>* Up, R* terms, R* total, double* partials)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (s < g.V) {
+    const CField<R> U{Up, g.V};
+    const Coord x = coord_of(g, s);
+    const double c5 = 1.0 / 20.0;
+    const double coef[5] = {(19.0 - 55.0 * c5) / 9.0, (1.0 - 64.0 * c5) / 9.0 / 16.0,
+                            (-64.0 + 640.0 * c5) / 45.0 / 4.0, (1.0 / 5.0 - 2.0 * c5) / 9.0, c5 / 81.0};
+    const double fac = -1.0 / (4.0 * 3.141592653589793 * 3.141592653589793);
+    double tot = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const int m = k == 1 ? 2 : (k == 4 ? 3 : 1);
+      const int n = k == 0 ? 1 : (k == 1 ? 2 : (k == 2 ? 2 : 3));
+      double q = 0.0;
+      // qcd.cpp:64-79: -tr(F02 F13) + tr(F03 F12) + tr(F23 F01)
+#pragma unroll 1
+      for (int pr = 0; pr < 3; ++pr) {
+        const int pa = pr == 0 ? 1 : (pr == 1 ? 2 : 5), pb = pr == 0 ? 4 : (pr == 1 ? 3 : 0);
+        const M3<R> fa = leaf_f_mn(U, g, x, pa, m, n);
+        const M3<R> fb = leaf_f_mn(U, g, x, pb, m, n);
+        const double t = (double)re_tr_mul(fa, fb);
+        q += pr == 0 ? -t : t;
+      }
+      v[k] = coef[k] * (fac * q);
+      tot += v[k];
+    }
+    if (terms) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) terms[lay_index<1>(g.V, k, 0, s)] = (R)v[k];
+    }
+    if (total) total[s] = (R)tot;
+  }
+  block_reduce_store<5>(v, partials);
+}
+
+template <typename R>
+cudaError_t launch_topology_5li(const Geo& g, const void* U, void* terms, void* total, double* partials,
+                                cudaStream_t st)
+{
+  k_topology_5li<R><<<reduce_blocks(g), RED_BS, 0, st>>>(g, (const Cx<R>*)U, (R*)terms, (R*)total, partials);
+  return cudaGetLastError();
+}
+
 template <typename R>
 __global__ void __launch_bounds__(RED_BS) k_qnorm(long n, const R* x, double* partials)
 {
@@ -807,6 +935,7 @@ cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st)
   template cudaError_t launch_gm_hamilton<R>(const Geo&, const void*, double*, cudaStream_t);              \
   template cudaError_t launch_action<R>(const Geo&, const void*, int, double*, cudaStream_t);              \
   template cudaError_t launch_clover<R>(const Geo&, const void*, void*, void*, double*, cudaStream_t);     \
+  template cudaError_t launch_topology_5li<R>(const Geo&, const void*, void*, void*, double*, cudaStream_t); \
   template cudaError_t launch_qnorm<R>(long, const void*, double*, int, cudaStream_t);                    \
   template cudaError_t launch_rand_momentum<R>(const Geo&, void*, const uint32_t*, double, int*, cudaStream_t); \
   template cudaError_t launch_hot_start<R>(const Geo&, void*, const uint32_t*, double, int, int*, cudaStream_t); \

@@ -83,6 +83,11 @@ cudaError_t launch_action(const Geo& g, const void* U, int rect, double* partial
 template <typename R>
 cudaError_t launch_clover(const Geo& g, const void* U, void* e_field, void* q_field, double* partials,
                           cudaStream_t st);
+// values 0..4: the five terms of the 5-loop improved charge (qcd.cpp:425-489);
+// optional fields: terms (real, multiplicity 5) and their per-site sum (multiplicity 1)
+template <typename R>
+cudaError_t launch_topology_5li(const Geo& g, const void* U, void* terms, void* total, double* partials,
+                                cudaStream_t st);
 template <typename R>
 cudaError_t launch_qnorm(long n_reals, const void* x, double* partials, int blocks, cudaStream_t st);
 cudaError_t launch_finalize(const double* partials, int n_values, int blocks, double* results, int slot,

@@ -88,3 +88,33 @@ def gf_topology_clf(gf: GaugeField) -> float:
     o = ctypes.c_double()
     call("qgb_gf_topology_clf", gf.handle, ctypes.byref(o))
     return o.value
+
+
+def gf_topology_field(gf: GaugeField) -> FieldRealD:
+    """topology.pyx:98-108 -> clf_topology_field_5 (qcd.cpp:491-509): the 5-loop
+    improved charge density (hep-lat/9701012 Eq. 2-7), multiplicity 1."""
+    topf = FieldRealD(gf.geo, 1, precision=gf.precision)
+    call("qgb_clf_topology_field_5", topf.handle, gf.handle)
+    return topf
+
+
+def gf_topology(gf: GaugeField) -> float:
+    """topology.pyx:110-118: the 5-loop improved charge."""
+    o = ctypes.c_double()
+    call("qgb_gf_topology", gf.handle, ctypes.byref(o))
+    return o.value
+
+
+def gf_topology_terms_field(gf: GaugeField) -> FieldRealD:
+    """topology.pyx:120-128 -> clf_topology_field_5_terms (qcd.cpp:425-489):
+    the five terms per site, multiplicity 5; their sum is gf_topology_field."""
+    topf = FieldRealD(gf.geo, 5, precision=gf.precision)
+    call("qgb_clf_topology_field_5_terms", topf.handle, gf.handle)
+    return topf
+
+
+def gf_topology_terms(gf: GaugeField) -> np.ndarray:
+    """topology.pyx:130-140: the five terms summed over the lattice, shape (5,)."""
+    out = np.zeros(5, dtype=np.float64)
+    call("qgb_gf_topology_terms", gf.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return out

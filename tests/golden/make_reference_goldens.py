@@ -8,7 +8,7 @@ Run in a checkout that has the reference source tree (default
   examples-py/hmc-pure-gauge.log.json         Python HMC, plaq and delta_h per trajectory
   examples-py/hmc-pure-gauge-test.log.json    Python HMC from a unit start, plaq per trajectory
   examples-py/flow-and-smear.log.json         Wilson flow steps and energies
-  examples-py/gf-utils.log.json               hot-start plaquette and clover charge along the flow
+  examples-py/gf-utils.log.json               hot-start plaquette, clover and 5-loop charges along the flow
 """
 
 import json
@@ -55,6 +55,9 @@ def main():
     out["gf_utils"] = {"source": "examples-py/gf-utils.log.json",
                        "hot_plaq": g["gf_ape_list[0] plaq"][0],
                        "topo_clf": {str(t): g[f"t={t} topo_clf"][0] for t in ("0", "1.0", "2.0", "3.0", "4.0", "5.0")},
+                       "topo_5li": {str(t): g[f"t={t} topo_5li"][0] for t in ("0", "1.0", "2.0", "3.0", "4.0", "5.0")},
+                       "topo_5li_terms_sum": {str(t): g[f"t={t} topo_5li sum(topo_terms)"][0]
+                                              for t in ("0", "1.0", "2.0", "3.0", "4.0", "5.0")},
                        "eps_topo": 1e-9}
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "reference_goldens.json"), "w") as f:

@@ -159,6 +159,11 @@ def test_gf_utils_topology_log(q, goldens):
     gf.set_rand(rs.split("gf-init"), 0.5, 10)
     assert rel(gf.plaq(), g["hot_plaq"]) < 1e-10
     assert abs(q.gf_topology_clf(gf) - g["topo_clf"]["0"]) < 1e-12
-    for t in ("1.0", "2.0", "3.0", "4.0", "5.0"):
-        q.gf_wilson_flow(gf, 1.0, 50, c1=-0.331)
-        assert rel(q.gf_topology_clf(gf), g["topo_clf"][t]) < g["eps_topo"]
+    for t in ("0", "1.0", "2.0", "3.0", "4.0", "5.0"):
+        if t != "0":
+            q.gf_wilson_flow(gf, 1.0, 50, c1=-0.331)
+            assert rel(q.gf_topology_clf(gf), g["topo_clf"][t]) < g["eps_topo"]
+        # 5-loop improved charge (topo_5li) and the sum of its terms
+        q5 = q.gf_topology(gf)
+        assert abs(q5 - g["topo_5li"][t]) < g["eps_topo"] * max(1.0, abs(q5)), (t, q5)
+        assert abs(q.gf_topology_terms(gf).sum() - g["topo_5li_terms_sum"][t]) < g["eps_topo"] * max(1.0, abs(q5))

@@ -138,6 +138,21 @@ def test_energy_density_and_topology(q, oracle, ts):
     assert nrel(np.asarray(tf)[:, 0], oracle.clf_topology_field(ref, ts)) < 1e-12
 
 
+@pytest.mark.parametrize("ts", GEOS)
+def test_topology_5li(q, oracle, ts):
+    """The five terms of the 5-loop improved charge per site, their per-site sum
+    and the lattice sums (qcd.cpp:425-509) against the oracle."""
+    gf, ref = hot_start(q, oracle, ts)
+    terms_ref = oracle.clf_topology_field_5_terms(ref, ts)
+    terms = np.asarray(q.gf_topology_terms_field(gf))
+    assert terms.shape == terms_ref.shape
+    assert np.abs(terms - terms_ref).max() <= 1e-12 * max(1.0, np.abs(terms_ref).max())
+    tot = np.asarray(q.gf_topology_field(gf))[:, 0]
+    assert np.abs(tot - terms_ref.sum(axis=1)).max() <= 1e-12 * max(1.0, np.abs(terms_ref).max())
+    assert np.allclose(q.gf_topology_terms(gf), terms_ref.sum(axis=0), rtol=0, atol=1e-11)
+    assert abs(q.gf_topology(gf) - oracle.gf_topology(ref, ts)) <= 1e-11
+
+
 def test_fp32_storage(q, oracle):
     ts = (4, 4, 4, 8)
     gf, ref = hot_start(q, oracle, ts)

@@ -102,6 +102,22 @@ def test_gf_utils_topology_log(oracle, goldens):
         assert rel(oracle.gf_topology_clf(gf, TS), g["topo_clf"][t]) < g["eps_topo"]
 
 
+def test_gf_utils_topology_5li_log(oracle, goldens):
+    """examples-py/gf-utils.py: the 5-loop improved charge (gf_topology) and the
+    sum of its five terms at t = 0, 1, 2 of the c1 = -0.331 flow."""
+    g = goldens["gf_utils"]
+    rs = oracle.RngState("seed")
+    gf = oracle.new_field(TS)
+    oracle.gf_set_rand(gf, TS, rs.split("gf-init"), 0.5, 10)
+    for t in ("0", "1.0", "2.0"):
+        if t != "0":
+            oracle.gf_wilson_flow(gf, TS, 1.0, 50, -0.331)
+        q = oracle.gf_topology(gf, TS)
+        assert abs(q - g["topo_5li"][t]) < g["eps_topo"] * max(1.0, abs(q)), (t, q)
+        terms = oracle.clf_topology_field_5_terms(gf, TS).sum(axis=0)
+        assert abs(terms.sum() - g["topo_5li_terms_sum"][t]) < g["eps_topo"] * max(1.0, abs(q))
+
+
 def test_metropolis_draw_conventions(oracle):
     """The C++ metropolis_accept draws u_rand_gen(rs, 0.0, 1.0) = 1 - u
     (hmc.cpp:91); the Python one draws u_rand_gen(1.0, 0.0) = u (hmc.pyx:149)."""
