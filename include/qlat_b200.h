@@ -43,6 +43,7 @@ extern "C" {
 #define QGB_ERR_TIMEOUT 6
 #define QGB_ERR_MISMATCH 7
 #define QGB_ERR_NO_DEVICE 8
+#define QGB_ERR_IO 9 /* file missing, unreadable, short or not in the expected format */
 
 #define QGB_F64 64
 #define QGB_F32 32
@@ -263,6 +264,40 @@ int qgb_batch_plaq(qgb_batch* b, double* plaq);
 /* One chain's links in the reference memory image. */
 int qgb_batch_download_chain(qgb_batch* b, int32_t chain, double* host);
 int qgb_batch_upload_chain(qgb_batch* b, int32_t chain, const double* host);
+
+/* ---- NERSC gauge-configuration files ------------------------------------ */
+
+/* The format of save_gauge_field / load_gauge_field (qcd.h:66-250): ASCII
+ * header, then the links as IEEE doubles in the reference site order, first two
+ * rows of each link ("4D_SU3_GAUGE"; "4D_SU3_GAUGE_3x3" is also read),
+ * big-endian ("IEEE64BIG"; "IEEE64LITTLE" is also read), with the simple
+ * checksum (sum of 32-bit words, field-io.h:11-25) and the CRC-32
+ * (field-io.h:84-88) in the header.  The *_host functions need no GPU and use
+ * host buffers in the reference memory image ([site][mu][3][3] complex128).
+ * Null strings take the reference's defaults (GaugeFieldInfo, qcd.h:34-58):
+ * ensemble_id "42", ensemble_label "default-ensemble", creator "Qlat", date =
+ * now (ctime). */
+int qgb_nersc_write_host(const char* path, const double* links, const int32_t total_site[4], double plaq,
+                         double link_trace, const char* ensemble_id, const char* ensemble_label, const char* creator,
+                         const char* date, double beta, int64_t sequence_num, int64_t* file_size);
+/* read_gauge_field_header (qcd.h:94-144).  n_rows: 2, 3, or 0 for an unknown
+ * DATATYPE; big_endian: 1, 0, or -1 for an unknown FLOATING_POINT. */
+int qgb_nersc_read_header(const char* path, int32_t total_site[4], int32_t* n_rows, int32_t* big_endian, double* plaq,
+                          double* link_trace, uint32_t* simple_checksum, uint32_t* crc32);
+/* The links of the file (whose lattice must be total_site).  Two-row files
+ * leave row 3 zero: unitarize rebuilds it.  checks: bit 0 CRC-32 matches, bit 1
+ * simple checksum matches, bit 2 two-row file.  A mismatch is reported, not an
+ * error (the reference warns). */
+int qgb_nersc_read_host(const char* path, double* links, const int32_t total_site[4], int32_t* checks,
+                        int64_t* file_size);
+/* Replace save_gauge_field (qcd.h:146-181; GaugeField.save, qcd.pyx:55-60): the
+ * header's plaquette and link trace are computed from gf. */
+int qgb_save_gauge_field(const qgb_field* gf, const char* path, const char* ensemble_id, const char* ensemble_label,
+                         const char* creator, double beta, int64_t sequence_num, int64_t* file_size);
+/* Replace load_gauge_field (qcd.h:183-250; GaugeField.load, qcd.pyx:62-67): gf
+ * must have the file's lattice (qgb_nersc_read_header gives it); two-row links
+ * are unitarized on the GPU. */
+int qgb_load_gauge_field(qgb_field* gf, const char* path, int32_t* checks, int64_t* file_size);
 
 /* ---- force-kernel autotuner (no counterpart in the reference) ---------- */
 

@@ -30,6 +30,14 @@ SIGNATURES = {
     "qgb_synchronize": [],
     "qgb_field_create": [c_field_p, i32x4, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "qgb_field_destroy": [c_field],
+    "qgb_nersc_write_host": [ctypes.c_char_p, c_dbl_p, i32x4, ctypes.c_double, ctypes.c_double, ctypes.c_char_p,
+                             ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int64,
+                             c_i64_p],
+    "qgb_nersc_read_header": [ctypes.c_char_p, i32x4, c_i32_p, c_i32_p, c_dbl_p, c_dbl_p, c_u32_p, c_u32_p],
+    "qgb_nersc_read_host": [ctypes.c_char_p, c_dbl_p, i32x4, c_i32_p, c_i64_p],
+    "qgb_save_gauge_field": [c_field, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                             ctypes.c_double, ctypes.c_int64, c_i64_p],
+    "qgb_load_gauge_field": [c_field, ctypes.c_char_p, c_i32_p, c_i64_p],
     "qgb_field_info": [c_field, i32x4, c_i32_p, c_i32_p, c_i32_p],
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],

@@ -291,6 +291,46 @@ class GaugeField(FieldColorMatrix):
         from .hmc import gf_avg_plaq
         return gf_avg_plaq(self)
 
+    def save(self, path: str, *, ensemble_id: str | None = None, ensemble_label: str | None = None,
+             creator: str | None = None, beta: float = 0.0, sequence_num: int = 0) -> int:
+        """Save in the NERSC format (qcd.pyx:55-60 -> save_gauge_field, qcd.h:146-181);
+        returns the number of data bytes written."""
+        n = ctypes.c_int64()
+        enc = lambda v: None if v is None else str(v).encode()  # noqa: E731
+        call("qgb_save_gauge_field", self.handle, str(path).encode(), enc(ensemble_id), enc(ensemble_label),
+             enc(creator), float(beta), int(sequence_num), ctypes.byref(n))
+        return n.value
+
+    def load(self, path: str) -> int:
+        """Load a NERSC file (qcd.pyx:62-67 -> load_gauge_field, qcd.h:183-250),
+        taking the file's lattice; returns the number of data bytes read.  A
+        checksum mismatch is reported with a warning, as the reference does."""
+        info = read_gauge_field_header(path)
+        ts = tuple(info["total_site"])
+        if self.geo is None or tuple(self.geo.total_site) != ts or self._h is None:
+            self.init(Geometry(ts))
+        checks = ctypes.c_int32()
+        n = ctypes.c_int64()
+        call("qgb_load_gauge_field", self.handle, str(path).encode(), ctypes.byref(checks), ctypes.byref(n))
+        if not checks.value & 1 or not checks.value & 2:
+            import warnings
+            warnings.warn(f"load_gauge_field: '{path}': checksum mismatch "
+                          f"(CRC32HASH {'ok' if checks.value & 1 else 'differs'}, "
+                          f"CHECKSUM {'ok' if checks.value & 2 else 'differs'})")
+        return n.value
+
+
+def read_gauge_field_header(path: str) -> dict:
+    """The header of a NERSC gauge file (read_gauge_field_header, qcd.h:94-144)."""
+    ts = _lib.i32x4()
+    rows, big = ctypes.c_int32(), ctypes.c_int32()
+    plaq, trace = ctypes.c_double(), ctypes.c_double()
+    simple, crc = ctypes.c_uint32(), ctypes.c_uint32()
+    call("qgb_nersc_read_header", str(path).encode(), ts, ctypes.byref(rows), ctypes.byref(big),
+         ctypes.byref(plaq), ctypes.byref(trace), ctypes.byref(simple), ctypes.byref(crc))
+    return {"total_site": list(ts), "n_rows": rows.value, "big_endian": big.value, "plaq": plaq.value,
+            "link_trace": trace.value, "simple_checksum": simple.value, "crc32": crc.value}
+
 
 class GaugeMomentum(FieldColorMatrix):
     """qlat.GaugeMomentum (hmc.pyx:39-53)."""
