@@ -97,7 +97,8 @@ int qgb_field_qnorm(const qgb_field* f, double* out);
 
 /* ---- RngState (rng-state.h:12-99, lib/rng-state.cpp:150-281) ------------ */
 
-/* RngState(seed): reset(rs, seed). */
+/* RngState(seed): reset(rs, seed); seed NULL: RngState(), reset(rs)
+ * (rng-state.cpp:150-164). */
 int qgb_rng_seed(uint32_t out[24], const char* seed);
 /* rs.split(sindex) (split_rng_state, rng-state.cpp:173-201). */
 int qgb_rng_split(uint32_t out[24], const uint32_t rs[24], const char* sindex);

@@ -760,7 +760,11 @@ int qgb_field_qnorm(const qgb_field* f, double* out)
 
 int qgb_rng_seed(uint32_t out[24], const char* seed)
 {
-  QGB_CHECK(out && seed, QGB_ERR_INVALID_ARG, "qgb_rng_seed: null argument");
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_rng_seed: null argument");
+  if (!seed) {  // RngState(): reset(rs) (rng-state.cpp:150-164)
+    qgb::rng_host_seed(out, nullptr);
+    return QGB_OK;
+  }
   QGB_CHECK(strlen(seed) < 200, QGB_ERR_INVALID_ARG, "qgb_rng_seed: seed string too long");
   qgb::rng_host_seed(out, seed);
   return QGB_OK;

@@ -967,6 +967,10 @@ void rng_host_seed(uint32_t out[24], const char* seed)
   memset(&r, 0, sizeof(r));
   memcpy(r.hash, qgb_sha_host.h0, 32);
   r.type = RNG_NO_TYPE;
+  if (!seed) {  // RngState(): reset(rs) only
+    rng_export(out, r);
+    return;
+  }
   Rng o;
   rng_split_bytes(o, r, (const uint8_t*)seed, (int)strlen(seed));
   rng_export(out, o);
