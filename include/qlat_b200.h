@@ -300,6 +300,41 @@ int qgb_save_gauge_field(const qgb_field* gf, const char* path, const char* ense
  * are unitarized on the GPU. */
 int qgb_load_gauge_field(qgb_field* gf, const char* path, int32_t* checks, int64_t* file_size);
 
+/* ---- flowed HMC with masked invertible flows (flowed-hmc.h) --------------- */
+
+/* FlowStepInfo (flowed-hmc.h:26-41): flow the links U_mu(x) of the sites of
+ * mask 1 or 2 (even/odd sites for flow_size 1; even/odd 2^4 blocks for
+ * flow_size 2) with step epsilon, by the plaquette staple (flow_size 1) or the
+ * staple of the rectangles whose short edge is the link (flow_size 2).  Lattice
+ * extents must be multiples of 2 * flow_size.  FP64 fields only. */
+typedef struct {
+  int32_t mask;
+  int32_t mu;
+  double epsilon;
+  int32_t flow_size;
+} qgb_flow_step;
+/* mk_flow_info_step(rs, epsilon) (two_eps = 0) or mk_flow_info_step(rs,
+ * epsilon, epsilon2) (two_eps = 1) (flowed-hmc.cpp:21-69): the steps in the
+ * reference's order, including its random_permute; out holds up to 16. */
+int qgb_flow_info_step(const uint32_t rs[24], double epsilon, double epsilon2, int32_t two_eps, qgb_flow_step* out,
+                       int32_t* n_out);
+/* gf_flow(gf, gf0, fi) / gf_flow_inv(gf, gf1, fi) (flowed-hmc.cpp:540-594). */
+int qgb_gf_flow(qgb_field* gf, const qgb_field* gf0, const qgb_flow_step* steps, int32_t n);
+int qgb_gf_flow_inv(qgb_field* gf, const qgb_field* gf1, const qgb_flow_step* steps, int32_t n);
+/* gf_flow_and_ln_det_node (flowed-hmc.cpp:1257-1299): gf = flowed gf0, ln_det
+ * = sum of ln det of the flow's Jacobian. */
+int qgb_gf_flow_and_ln_det_node(qgb_field* gf, const qgb_field* gf0, const qgb_flow_step* steps, int32_t n,
+                                double* ln_det);
+/* gf_hamilton_flowed (flowed-hmc.cpp:1301-1321): the gauge action of the flowed
+ * field and ln det; the flowed-HMC action is flowed_action - ln_det. */
+int qgb_gf_hamilton_flowed_node(const qgb_field* gf0, double beta, double c1, const qgb_flow_step* steps, int32_t n,
+                                double* flowed_action, double* ln_det);
+/* set_gm_force_flowed (with_det = 1, flowed-hmc.cpp:1500-1509), or the force of
+ * the flowed field propagated without the determinant term (with_det = 0,
+ * set_gm_force_flowed_no_det of set_gm_force of the flowed field). */
+int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double beta, double c1,
+                            const qgb_flow_step* steps, int32_t n, int32_t with_det);
+
 /* ---- force-kernel autotuner (no counterpart in the reference) ---------- */
 
 /* The force kernels (set_gm_force and its fused HMC / flow consumers) exist

@@ -17,6 +17,9 @@ from .hmc import (gf_avg_plaq, gf_evolve, gf_hamilton, gf_hamilton_node, gf_sum_
                   metropolis_accept, metropolis_accept_cpp, run_hmc_evolve_pure_gauge, run_hmc_pure_gauge,
                   set_gm_force, set_rand_gauge_momentum, unitarize)
 from .batch import ChainBatch
+from .flowed_hmc import (FlowInfo, FlowStepInfo, gf_flow, gf_flow_and_ln_det_node, gf_flow_inv, gf_hamilton_flowed,
+                         gf_hamilton_flowed_node, gm_evolve_fg_flowed, mk_flow_info_step, run_flowed_hmc,
+                         run_hmc_evolve_flowed, set_gm_force_flowed)
 from .flow_adjoint import (FlowedWilsonAction, gf_flow_action, gf_flow_action_grad, gf_wilson_flow_vjp,
                            run_flowed_hmc_pure_gauge, set_anti_hermitian_matrix_from_basis,
                            set_basis_from_anti_hermitian_matrix)

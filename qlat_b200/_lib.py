@@ -38,6 +38,14 @@ SIGNATURES = {
     "qgb_save_gauge_field": [c_field, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                              ctypes.c_double, ctypes.c_int64, c_i64_p],
     "qgb_load_gauge_field": [c_field, ctypes.c_char_p, c_i32_p, c_i64_p],
+    "qgb_flow_info_step": [c_u32_p, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_void_p, c_i32_p],
+    "qgb_gf_flow": [c_field, c_field, ctypes.c_void_p, ctypes.c_int32],
+    "qgb_gf_flow_inv": [c_field, c_field, ctypes.c_void_p, ctypes.c_int32],
+    "qgb_gf_flow_and_ln_det_node": [c_field, c_field, ctypes.c_void_p, ctypes.c_int32, c_dbl_p],
+    "qgb_gf_hamilton_flowed_node": [c_field, ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_int32,
+                                    c_dbl_p, c_dbl_p],
+    "qgb_set_gm_force_flowed": [c_field, c_field, ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_int32,
+                                ctypes.c_int32],
     "qgb_field_info": [c_field, i32x4, c_i32_p, c_i32_p, c_i32_p],
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],

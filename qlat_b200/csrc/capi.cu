@@ -533,6 +533,15 @@ static int check_vjp_args(const qgb_field* gf, const qgb_field* a, const char* w
 
 namespace qgb
 {
+// Internal accessors for the other translation units (flowed.cu).
+void* field_data(const qgb_field* f) { return f ? f->d : nullptr; }
+int library_stream(cudaStream_t* st)
+{
+  QGB_CTX();
+  *st = g_ctx.stream;
+  return QGB_OK;
+}
+
 // Lets the allocation-free entry point (noalloc.cu) report through qgb_last_error.
 void set_last_error(const std::string& msg) { g_err = msg; }
 }  // namespace qgb

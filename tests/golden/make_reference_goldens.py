@@ -5,6 +5,7 @@ reference's own test logs into reference_goldens.json.
 Run in a checkout that has the reference source tree (default
 /root/reference, or pass its path).  Sources:
   examples-cpp/hmc/log                        C++ force-gradient HMC, plaq per trajectory
+  examples-cpp/flowed-hmc/log                 C++ flowed HMC (masked invertible flows), plaq per trajectory
   examples-py/hmc-pure-gauge.log.json         Python HMC, plaq and delta_h per trajectory
   examples-py/hmc-pure-gauge-test.log.json    Python HMC from a unit start, plaq per trajectory
   examples-py/flow-and-smear.log.json         Wilson flow steps and energies
@@ -28,6 +29,14 @@ def main():
         if m:
             cpp.append([int(m.group(1)), float(m.group(2)), float(m.group(3))])
     out["cpp_hmc"] = {"source": "examples-cpp/hmc/log", "rows": cpp, "printed_digits": 13}
+    lines = open(os.path.join(ref, "examples-cpp/flowed-hmc/log")).read().splitlines()
+    rows = []
+    for ln in lines:
+        m = re.match(r"CHECK: test_hmc: traj=(\d+) ; plaq_avg=\s*(\S+) ; plaq_sum=\s*(\S+)\.", ln)
+        if m:
+            rows.append([int(m.group(1)), float(m.group(2)), float(m.group(3))])
+    out["cpp_flowed_hmc"] = {"source": "examples-cpp/flowed-hmc/log", "rows": rows, "printed_digits": 13,
+                             "beta": 2.31, "c1": -0.331, "total_site": [4, 4, 4, 8]}
 
     def load(name):
         d = json.load(open(os.path.join(ref, "examples-py", name)))
