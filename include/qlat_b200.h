@@ -335,6 +335,56 @@ int qgb_gf_hamilton_flowed_node(const qgb_field* gf0, double beta, double c1, co
 int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double beta, double c1,
                             const qgb_flow_step* steps, int32_t n, int32_t with_det);
 
+/* ---- field-accelerated HMC: per-link masses and dual momenta (hmc.h:20-80) */
+
+/* A mass field is an FP64 real field of multiplicity 4 (Field<RealD>, one mass
+ * per link); +inf freezes a link's momentum at zero.  gm moves a link from the
+ * left, gm_dual from the right; momenta and gauge fields share one lattice and
+ * precision. */
+/* set_rand_gauge_momentum(gm, mf, rs) (hmc.cpp:121-149; GaugeMomentum.set_rand_fa,
+ * hmc.pyx:51-63): unit-sigma draw, then gm_mu(x) *= sqrt(mf_mu(x)), zero where
+ * the mass is +inf. */
+int qgb_set_rand_gauge_momentum_fa(qgb_field* gm, const qgb_field* mf, const uint32_t rs[24]);
+/* gm_hamilton_node(gm, mf) (hmc.cpp:175-201; gm_hamilton_node_fa, hmc.pyx:65-66):
+ * sum of (-1/2 tr gm^2) / mf over the links. */
+int qgb_gm_hamilton_node_fa(const qgb_field* gm, const qgb_field* mf, double* out);
+/* gf_evolve(gf, gm, mf, dt) (hmc.cpp:350-372; gf_evolve_fa, hmc.pyx:77-78):
+ * U = unitarize(exp(dt / mf P) U). */
+int qgb_gf_evolve_fa(qgb_field* gf, const qgb_field* gm, const qgb_field* mf, double step_size);
+/* gf_evolve_dual(gf, gm_dual, dt) (hmc.cpp:330-348; hmc.pyx:74-75):
+ * U = unitarize(U exp(-dt P)). */
+int qgb_gf_evolve_dual(qgb_field* gf, const qgb_field* gm_dual, double step_size);
+/* gf_evolve_dual(gf, gm_dual, mf_dual, dt) (hmc.cpp:374-396; gf_evolve_fa_dual,
+ * hmc.pyx:80-81): U = unitarize(U exp(-dt / mf_dual P)). */
+int qgb_gf_evolve_fa_dual(qgb_field* gf, const qgb_field* gm_dual, const qgb_field* mf_dual, double step_size);
+/* set_gm_force_dual (hmc.cpp:492-513): gm_force_dual = -U^+ gm_force U
+ * (output distinct from both inputs). */
+int qgb_set_gm_force_dual(qgb_field* gm_force_dual, const qgb_field* gf, const qgb_field* gm_force);
+/* project_gauge_transform (hmc.cpp:515-589): subtract the gauge-transformation
+ * motion from gm and gm_dual; change_qnorm = qnorm of the per-site average it
+ * removed / total volume (NULL: not computed, and the call does not
+ * synchronise). */
+int qgb_project_gauge_transform(qgb_field* gm, qgb_field* gm_dual, const qgb_field* mf, const qgb_field* mf_dual,
+                                double* change_qnorm);
+/* set_gauge_transform_momentum (hmc.cpp:591-626): gm_mu(x) = gtm(x),
+ * gm_dual_mu(x) = gtm(x + mu); gtm a color-matrix field of multiplicity 1. */
+int qgb_set_gauge_transform_momentum(qgb_field* gm, qgb_field* gm_dual, const qgb_field* gtm);
+/* dot_gauge_momentum (hmc.cpp:628-645): f_mu(x) = Re tr(gm1_mu(x)^+ gm2_mu(x)),
+ * f an FP64 real field of multiplicity 4. */
+int qgb_dot_gauge_momentum(qgb_field* f, const qgb_field* gm1, const qgb_field* gm2);
+/* set_u_rand / set_g_rand (core.h:1585-1636; FieldRealD.set_rand / set_rand_g,
+ * field_types.pyx.in:194-200): per site the state rs.newtype(site index), one
+ * draw per real of the site in memory order.  rs must be untyped. */
+int qgb_field_set_u_rand(qgb_field* f, const uint32_t rs[24], double upper, double lower);
+int qgb_field_set_g_rand(qgb_field* f, const uint32_t rs[24], double center, double sigma);
+/* Real field: every entry = value (set_unit(f, value) of a Field<RealD>); with a
+ * selection (n = sites * multiplicity bytes, site-major, nonzero = selected)
+ * only the selected entries: `f[sel] = value`. */
+int qgb_field_fill(qgb_field* f, double value, const uint8_t* mask, int64_t n);
+/* `dst[sel] = src[sel]` with a boolean selection of the (site, component)
+ * entries as above; fields of one kind, multiplicity, lattice and precision. */
+int qgb_field_set_selected(qgb_field* dst, const qgb_field* src, const uint8_t* mask, int64_t n);
+
 /* ---- force-kernel autotuner (no counterpart in the reference) ---------- */
 
 /* The force kernels (set_gm_force and its fused HMC / flow consumers) exist

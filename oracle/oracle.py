@@ -104,6 +104,15 @@ def lib():
                                                        ctypes.c_int, ctypes.c_double]),
             "or_run_hmc_evolve_leapfrog": (ctypes.c_double, [_dbl_p, _dbl_p, _int4, ctypes.c_double,
                                                              ctypes.c_double, ctypes.c_int, ctypes.c_double]),
+            "or_field_set_u_rand": (None, [_dbl_p, _int4, ctypes.c_int, R, ctypes.c_double, ctypes.c_double]),
+            "or_field_set_g_rand": (None, [_dbl_p, _int4, ctypes.c_int, R, ctypes.c_double, ctypes.c_double]),
+            "or_set_rand_gauge_momentum_fa": (None, [_dbl_p, _dbl_p, _int4, R]),
+            "or_gm_hamilton_node_fa": (ctypes.c_double, [_dbl_p, _dbl_p, _int4]),
+            "or_gf_evolve_fa": (None, [_dbl_p, _dbl_p, _dbl_p, _int4, ctypes.c_double, ctypes.c_int]),
+            "or_set_gm_force_dual": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
+            "or_project_gauge_transform": (ctypes.c_double, [_dbl_p, _dbl_p, _dbl_p, _dbl_p, _int4]),
+            "or_set_gauge_transform_momentum": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
+            "or_dot_gauge_momentum": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_make_matrix_exp": (None, [_dbl_p, _dbl_p, ctypes.c_int]),
             "or_unitarize": (None, [_dbl_p]),
             "or_make_tr_less_anti_herm": (None, [_dbl_p, _dbl_p]),
@@ -284,6 +293,60 @@ def clf_topology_field_5_terms(gf, total_site) -> np.ndarray:
 def gf_topology(gf, total_site) -> float:
     """topology.pyx:98-108: the 5-loop improved charge."""
     return lib().or_gf_topology(_p(gf), _dims(total_site))
+
+
+# ---- field-accelerated HMC (hmc.cpp:121-201, 330-396, 492-645) ----------------
+# mass fields: float64 arrays of shape (V, 4); +inf freezes a link
+
+
+def field_set_u_rand(f: np.ndarray, total_site, rs: RngState, upper: float = 1.0, lower: float = 0.0) -> None:
+    """set_u_rand (core.h:1585-1603): f is (V, n) float64 or (V, m, 3, 3) complex128."""
+    n = f.size // volume(total_site) * (2 if f.dtype == np.complex128 else 1)
+    lib().or_field_set_u_rand(_p(f), _dims(total_site), n, rs.ptr, upper, lower)
+
+
+def field_set_g_rand(f: np.ndarray, total_site, rs: RngState, center: float = 0.0, sigma: float = 1.0) -> None:
+    """set_g_rand (core.h:1617-1636)."""
+    n = f.size // volume(total_site) * (2 if f.dtype == np.complex128 else 1)
+    lib().or_field_set_g_rand(_p(f), _dims(total_site), n, rs.ptr, center, sigma)
+
+
+def set_rand_gauge_momentum_fa(gm, mf, total_site, rs: RngState) -> None:
+    lib().or_set_rand_gauge_momentum_fa(_p(gm), _p(mf), _dims(total_site), rs.ptr)
+
+
+def gm_hamilton_node_fa(gm, mf, total_site) -> float:
+    return lib().or_gm_hamilton_node_fa(_p(gm), _p(mf), _dims(total_site))
+
+
+def gf_evolve_fa(gf, gm, mf, total_site, step_size: float) -> None:
+    lib().or_gf_evolve_fa(_p(gf), _p(gm), _p(mf), _dims(total_site), step_size, 0)
+
+
+def gf_evolve_fa_dual(gf, gm_dual, mf_dual, total_site, step_size: float) -> None:
+    lib().or_gf_evolve_fa(_p(gf), _p(gm_dual), _p(mf_dual), _dims(total_site), step_size, 1)
+
+
+def gf_evolve_dual(gf, gm_dual, total_site, step_size: float) -> None:
+    lib().or_gf_evolve_fa(_p(gf), _p(gm_dual), None, _dims(total_site), step_size, 1)
+
+
+def set_gm_force_dual(fd, gf, f, total_site) -> None:
+    lib().or_set_gm_force_dual(_p(fd), _p(gf), _p(f), _dims(total_site))
+
+
+def project_gauge_transform(gm, gm_dual, mf, mf_dual, total_site) -> float:
+    return lib().or_project_gauge_transform(_p(gm), _p(gm_dual), _p(mf), _p(mf_dual), _dims(total_site))
+
+
+def set_gauge_transform_momentum(gm, gm_dual, gtm, total_site) -> None:
+    lib().or_set_gauge_transform_momentum(_p(gm), _p(gm_dual), _p(gtm), _dims(total_site))
+
+
+def dot_gauge_momentum(gm1, gm2, total_site) -> np.ndarray:
+    f = np.zeros((volume(total_site), 4), dtype=np.float64)
+    lib().or_dot_gauge_momentum(_p(f), _p(gm1), _p(gm2), _dims(total_site))
+    return f
 
 
 def run_hmc_evolve(gm, gf, total_site, beta, c1, n_step, md_time=1.0, integrator="force-gradient") -> float:

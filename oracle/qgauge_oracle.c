@@ -1087,6 +1087,210 @@ double or_run_hmc_evolve_leapfrog(double* gm, double* gf, const int dims[4], dou
   return delta_h;
 }
 
+/* ------------------------------------------------------------------ */
+/* field-accelerated HMC                                                */
+
+/* rng-state.h:71-76 newtype + rng-state.cpp:38-45 set_type */
+static void rng_newtype(or_rng* out, const or_rng* rs, uint64_t type)
+{
+  *out = *rs;
+  out->type = type;
+  out->cacheAvail = 0;
+  out->gaussianAvail = 0;
+}
+
+/* core.h:1585-1603 */
+void or_field_set_u_rand(double* f, const int dims[4], int n_per_site, const or_rng* rs, double upper, double lower)
+{
+  const geo_t g = mk_geo(dims);
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    or_rng rsi;
+    rng_newtype(&rsi, rs, (uint64_t)i);
+    for (int m = 0; m < n_per_site; ++m) f[i * n_per_site + m] = or_u_rand_gen(&rsi, upper, lower);
+  }
+}
+
+/* core.h:1617-1636 */
+void or_field_set_g_rand(double* f, const int dims[4], int n_per_site, const or_rng* rs, double center, double sigma)
+{
+  const geo_t g = mk_geo(dims);
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    or_rng rsi;
+    rng_newtype(&rsi, rs, (uint64_t)i);
+    for (int m = 0; m < n_per_site; ++m) f[i * n_per_site + m] = or_g_rand_gen(&rsi, center, sigma);
+  }
+}
+
+/* hmc.cpp:121-149 */
+void or_set_rand_gauge_momentum_fa(double* gm, const double* mf, const int dims[4], const or_rng* rs)
+{
+  or_set_rand_gauge_momentum(gm, dims, rs, 1.0);
+  const geo_t g = mk_geo(dims);
+  for (long i = 0; i < g.vol; ++i)
+    for (int m = 0; m < 4; ++m) {
+      double* p = gm + (i * 4 + m) * 18;
+      const double v = mf[i * 4 + m];
+      if (v != INFINITY) {
+        const double s = sqrt(v);
+        for (int k = 0; k < 18; ++k) p[k] *= s;
+      } else {
+        for (int k = 0; k < 18; ++k) p[k] = 0.0;
+      }
+    }
+}
+
+/* hmc.cpp:175-201 */
+double or_gm_hamilton_node_fa(const double* gm, const double* mf, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+  double sum = 0.0;
+  for (long i = 0; i < g.vol; ++i) {
+    double s = 0.0;
+    for (int mu = 0; mu < 4; ++mu) {
+      cm p;
+      memcpy(&p, gm + (i * 4 + mu) * 18, sizeof(cm));
+      s += neg_half_tr_square(&p) / mf[i * 4 + mu];
+    }
+    sum += s;
+  }
+  return sum;
+}
+
+/* hmc.cpp:311-396 with matrix_evolve / matrix_evolve_dual (matrix-hmc.h:178-200) */
+void or_gf_evolve_fa(double* gf, const double* gm, const double* mf, const int dims[4], double step_size, int dual)
+{
+  const geo_t g = mk_geo(dims);
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    for (int mu = 0; mu < 4; ++mu) {
+      cm u, p;
+      memcpy(&u, gf + (i * 4 + mu) * 18, sizeof(cm));
+      memcpy(&p, gm + (i * 4 + mu) * 18, sizeof(cm));
+      const double dt_m = mf ? step_size / mf[i * 4 + mu] : step_size;
+      cm r;
+      if (!dual) {
+        r = matrix_evolve(&u, &p, dt_m);
+      } else {
+        cm t = m_rscale(-dt_m, &p);
+        cm e = make_matrix_exp(&t, 20);
+        r = m_mul(&u, &e);
+        unitarize_cm(&r);
+      }
+      put_link(gf, i, mu, &r);
+    }
+  }
+}
+
+/* hmc.cpp:492-513: -U^+ F U, evaluated as ((-U^+) F) U */
+void or_set_gm_force_dual(double* fd, const double* gf, const double* f, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+  for (long i = 0; i < g.vol; ++i)
+    for (int mu = 0; mu < 4; ++mu) {
+      cm u, x;
+      memcpy(&u, gf + (i * 4 + mu) * 18, sizeof(cm));
+      memcpy(&x, f + (i * 4 + mu) * 18, sizeof(cm));
+      cm a = m_adj(&u);
+      a = m_rscale(-1.0, &a);
+      cm t = m_mul(&a, &x);
+      t = m_mul(&t, &u);
+      put_link(fd, i, mu, &t);
+    }
+}
+
+/* hmc.cpp:515-589 */
+double or_project_gauge_transform(double* gm, double* gmd, const double* mf, const double* mfd, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+  cm* ag = (cm*)malloc(sizeof(cm) * (size_t)g.vol);
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    cm sum = m_zero();
+    for (int m = 0; m < 4; ++m) {
+      int xm[4] = {x[0], x[1], x[2], x[3]};
+      xm[m] -= 1;
+      const long im = index_from_coor(&g, xm);
+      const double m1 = mf[i * 4 + m];
+      const double m2 = mfd[im * 4 + m];
+      cm c1, c2;
+      memcpy(&c1, gm + (i * 4 + m) * 18, sizeof(cm));
+      memcpy(&c2, gmd + (im * 4 + m) * 18, sizeof(cm));
+      if (m1 != INFINITY) {
+        cm t = m_rscale(1.0 / sqrt(m1), &c1);
+        m_add_to(&sum, &t);
+      }
+      if (m2 != INFINITY) {
+        cm t = m_rscale(1.0 / sqrt(m2), &c2);
+        m_add_to(&sum, &t);
+      }
+    }
+    ag[i] = m_rscale(1.0 / 8.0, &sum);
+  }
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    for (int m = 0; m < 4; ++m) {
+      int xp[4] = {x[0], x[1], x[2], x[3]};
+      xp[m] += 1;
+      const long ip = index_from_coor(&g, xp);
+      if (mf[i * 4 + m] != INFINITY) {
+        cm v;
+        memcpy(&v, gm + (i * 4 + m) * 18, sizeof(cm));
+        cm t = m_rscale(sqrt(mf[i * 4 + m]), &ag[i]);
+        m_sub_to(&v, &t);
+        put_link(gm, i, m, &v);
+      }
+      if (mfd[i * 4 + m] != INFINITY) {
+        cm v;
+        memcpy(&v, gmd + (i * 4 + m) * 18, sizeof(cm));
+        cm t = m_rscale(sqrt(mfd[i * 4 + m]), &ag[ip]);
+        m_sub_to(&v, &t);
+        put_link(gmd, i, m, &v);
+      }
+    }
+  }
+  double qn = 0.0;
+  for (long i = 0; i < g.vol; ++i) {
+    const double* p = (const double*)ag[i].p;
+    double s = 0.0;
+    for (int k = 0; k < 9; ++k) s += p[2 * k] * p[2 * k] + p[2 * k + 1] * p[2 * k + 1];
+    qn += s;
+  }
+  free(ag);
+  return qn / (double)g.vol;
+}
+
+/* hmc.cpp:591-626 */
+void or_set_gauge_transform_momentum(double* gm, double* gmd, const double* gtm, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    for (int m = 0; m < 4; ++m) {
+      int xp[4] = {x[0], x[1], x[2], x[3]};
+      xp[m] += 1;
+      const long ip = index_from_coor(&g, xp);
+      memcpy(gm + (i * 4 + m) * 18, gtm + i * 18, sizeof(cm));
+      memcpy(gmd + (i * 4 + m) * 18, gtm + ip * 18, sizeof(cm));
+    }
+  }
+}
+
+/* hmc.cpp:628-645 with qnorm(m1, m2) (matrix.h:209-217, complex.h:153-156) */
+void or_dot_gauge_momentum(double* f, const double* gm1, const double* gm2, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+  for (long i = 0; i < g.vol * 4; ++i) {
+    double s = 0.0;
+    for (int k = 0; k < 9; ++k) s += gm1[i * 18 + 2 * k] * gm2[i * 18 + 2 * k] + gm1[i * 18 + 2 * k + 1] * gm2[i * 18 + 2 * k + 1];
+    f[i] = s;
+  }
+}
+
 void or_make_matrix_exp(double out[18], const double a[18], int max_order)
 {
   cm x;

@@ -82,6 +82,21 @@ double or_run_hmc_evolve_fg(double* gm, double* gf, const int dims[4], double be
  * per step gf_evolve(dt/2), gm += dt F, gf_evolve(dt/2); returns delta_h. */
 double or_run_hmc_evolve_leapfrog(double* gm, double* gf, const int dims[4], double beta, double c1,
                                   int n_step, double md_time);
+/* Field-accelerated HMC (hmc.cpp:121-201, 330-396, 492-645).  A mass field mf
+ * holds 4 doubles per site (one per link), +inf freezing a link. */
+/* set_u_rand / set_g_rand of a field (core.h:1585-1636): per site
+ * rs.newtype(site index), n_per_site draws in memory order. */
+void or_field_set_u_rand(double* f, const int dims[4], int n_per_site, const or_rng* rs, double upper, double lower);
+void or_field_set_g_rand(double* f, const int dims[4], int n_per_site, const or_rng* rs, double center, double sigma);
+void or_set_rand_gauge_momentum_fa(double* gm, const double* mf, const int dims[4], const or_rng* rs);
+double or_gm_hamilton_node_fa(const double* gm, const double* mf, const int dims[4]);
+/* dual = 0: U = unitarize(exp(dt/m P) U); dual = 1: U = unitarize(U exp(-dt/m P));
+ * mf NULL: m = 1 (the overloads without a mass field). */
+void or_gf_evolve_fa(double* gf, const double* gm, const double* mf, const int dims[4], double step_size, int dual);
+void or_set_gm_force_dual(double* fd, const double* gf, const double* f, const int dims[4]);
+double or_project_gauge_transform(double* gm, double* gmd, const double* mf, const double* mfd, const int dims[4]);
+void or_set_gauge_transform_momentum(double* gm, double* gmd, const double* gtm, const int dims[4]);
+void or_dot_gauge_momentum(double* f, const double* gm1, const double* gm2, const int dims[4]);
 /* Single-matrix helpers used by the tests. */
 void or_make_matrix_exp(double out[18], const double a[18], int max_order);
 void or_unitarize(double m[18]);

@@ -20,6 +20,9 @@ from .batch import ChainBatch
 from .flowed_hmc import (FlowInfo, FlowStepInfo, gf_flow, gf_flow_and_ln_det_node, gf_flow_inv, gf_hamilton_flowed,
                          gf_hamilton_flowed_node, gm_evolve_fg_flowed, mk_flow_info_step, run_flowed_hmc,
                          run_hmc_evolve_flowed, set_gm_force_flowed)
+from .hmc_fa import (MomentumAutoCorr, dot_gauge_momentum, gf_evolve_dual, gf_evolve_fa, gf_evolve_fa_dual,
+                     gm_hamilton_node_fa, project_gauge_transform, run_hmc_fa, set_gauge_transform_momentum,
+                     set_gm_force_dual, set_rand_gauge_momentum_fa)
 from .flow_adjoint import (FlowedWilsonAction, gf_flow_action, gf_flow_action_grad, gf_wilson_flow_vjp,
                            run_flowed_hmc_pure_gauge, set_anti_hermitian_matrix_from_basis,
                            set_basis_from_anti_hermitian_matrix)

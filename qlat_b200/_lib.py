@@ -46,6 +46,19 @@ SIGNATURES = {
                                     c_dbl_p, c_dbl_p],
     "qgb_set_gm_force_flowed": [c_field, c_field, ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_int32,
                                 ctypes.c_int32],
+    "qgb_set_rand_gauge_momentum_fa": [c_field, c_field, c_u32_p],
+    "qgb_gm_hamilton_node_fa": [c_field, c_field, c_dbl_p],
+    "qgb_gf_evolve_fa": [c_field, c_field, c_field, ctypes.c_double],
+    "qgb_gf_evolve_dual": [c_field, c_field, ctypes.c_double],
+    "qgb_gf_evolve_fa_dual": [c_field, c_field, c_field, ctypes.c_double],
+    "qgb_set_gm_force_dual": [c_field, c_field, c_field],
+    "qgb_project_gauge_transform": [c_field, c_field, c_field, c_field, c_dbl_p],
+    "qgb_set_gauge_transform_momentum": [c_field, c_field, c_field],
+    "qgb_dot_gauge_momentum": [c_field, c_field, c_field],
+    "qgb_field_set_u_rand": [c_field, c_u32_p, ctypes.c_double, ctypes.c_double],
+    "qgb_field_set_g_rand": [c_field, c_u32_p, ctypes.c_double, ctypes.c_double],
+    "qgb_field_fill": [c_field, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64],
+    "qgb_field_set_selected": [c_field, c_field, ctypes.c_void_p, ctypes.c_int64],
     "qgb_field_info": [c_field, i32x4, c_i32_p, c_i32_p, c_i32_p],
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],

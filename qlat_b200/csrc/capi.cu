@@ -533,7 +533,7 @@ static int check_vjp_args(const qgb_field* gf, const qgb_field* a, const char* w
 
 namespace qgb
 {
-// Internal accessors for the other translation units (flowed.cu).
+// Internal accessors for the other translation units (flowed.cu, fa.cu).
 void* field_data(const qgb_field* f) { return f ? f->d : nullptr; }
 int library_stream(cudaStream_t* st)
 {
@@ -544,6 +544,18 @@ int library_stream(cudaStream_t* st)
 
 // Lets the allocation-free entry point (noalloc.cu) report through qgb_last_error.
 void set_last_error(const std::string& msg) { g_err = msg; }
+// The library's reusable device buffers (zeroed when first allocated).
+int scratch_buffer(size_t bytes, int tag, void** out)
+{
+  QGB_CTX();
+  return get_scratch(bytes, tag, out);
+}
+// Kernel launches made outside the profiled entry points (qgb_launch_count).
+void add_launches(int64_t n)
+{
+  std::lock_guard<std::recursive_mutex> lock(g_mu);
+  g_launches += n;
+}
 }  // namespace qgb
 
 // ========================================================================

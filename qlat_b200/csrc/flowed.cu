@@ -871,7 +871,7 @@ int qgb_gf_flow_and_ln_det_node(qgb_field* gf, const qgb_field* gf0, const qgb_f
   DevBuf C, L, S;
   FL_CUDA(C.alloc(c.bytes / 4));
   FL_CUDA(L.alloc(c.V * sizeof(double)));
-  FL_CUDA(S.alloc(16 * sizeof(double)));
+  FL_CUDA(S.alloc((size_t)(n > 0 ? n : 1) * sizeof(double)));
   void* U = qgb::field_data(gf);
   for (int i = 0; i < n; ++i) {
     const qgb_flow_step& f = steps[i];
@@ -887,8 +887,8 @@ int qgb_gf_flow_and_ln_det_node(qgb_field* gf, const qgb_field* gf0, const qgb_f
                                               f.epsilon, 0, 0);
     FL_CUDA(cudaGetLastError());
   }
-  double sums[16] = {0};
-  if (n > 0) FL_CUDA(cudaMemcpyAsync(sums, S.p, n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  std::vector<double> sums((size_t)(n > 0 ? n : 1), 0.0);
+  if (n > 0) FL_CUDA(cudaMemcpyAsync(sums.data(), S.p, n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
   FL_CUDA(cudaStreamSynchronize(c.st));
   double t = 0.0;
   for (int i = 0; i < n; ++i) t += sums[i];

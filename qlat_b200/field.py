@@ -63,6 +63,13 @@ class Geometry:
     def show(self):
         return repr(self)
 
+    def xg_arr(self) -> np.ndarray:
+        """Global coordinates of the sites, shape (V, 4) int32, x fastest
+        (Geometry.xg_arr, geometry.pyx)."""
+        X, Y, Z, T = self.total_site
+        i = np.arange(self.total_volume, dtype=np.int64)
+        return np.stack([i % X, (i // X) % Y, (i // (X * Y)) % Z, i // (X * Y * Z)], axis=1).astype(np.int32)
+
 
 class RngState:
     """qlat.RngState (rng-state.h:38-99): a SHA-256 counter RNG; the state is
@@ -109,6 +116,17 @@ class RngState:
         o = ctypes.c_double()
         call("qgb_rng_g_rand_gen", self._v, center, sigma, ctypes.byref(o))
         return o.value
+
+    def c_rand_gen(self, size) -> Coordinate:
+        """c_rand_gen (coordinate.h:305-310): the coordinate of site
+        rand_gen() % volume(size), x fastest."""
+        size = Coordinate(size)
+        ri = self.rand_gen() % size.volume()
+        x = []
+        for n in size:
+            x.append(ri % n)
+            ri //= n
+        return Coordinate(x)
 
     def export(self) -> np.ndarray:
         return np.array(list(self._v), dtype=np.uint32)
@@ -259,6 +277,58 @@ class Field:
     def download_device(self, ptr: int) -> None:
         call("qgb_field_download_device", self.handle, ctypes.c_void_p(ptr))
 
+    def set_rand(self, rng: RngState, upper: float = 1.0, lower: float = 0.0):
+        """set_u_rand (field_types.pyx.in:194-196, core.h:1585-1603): per site
+        rng.newtype(site index), one uniform draw in [lower, upper) per real."""
+        call("qgb_field_set_u_rand", self.handle, rng.c, float(upper), float(lower))
+
+    def set_rand_g(self, rng: RngState, center: float = 0.0, sigma: float = 1.0):
+        """set_g_rand (field_types.pyx.in:198-200, core.h:1617-1636)."""
+        call("qgb_field_set_g_rand", self.handle, rng.c, float(center), float(sigma))
+
+    def _selection(self, sel) -> np.ndarray | None:
+        """A boolean selection of the (site, component) entries as one byte per
+        entry, or None for other indexes."""
+        if isinstance(sel, np.ndarray) and sel.dtype == np.bool_ and sel.shape == (self.geo.total_volume,
+                                                                                   self.multiplicity):
+            return np.ascontiguousarray(sel, dtype=np.uint8)
+        return None
+
+    def __getitem__(self, idx):
+        """``field[idx]``: a copy of the indexed entries of the reference
+        memory image (numpy indexing on the downloaded field)."""
+        return self.to_numpy()[idx]
+
+    def __setitem__(self, idx, value):
+        """``field[idx] = value``.  A boolean selection of (site, component)
+        entries with a scalar (real fields) or with ``other.selected(sel)``
+        runs on the GPU; other indexes edit the downloaded image and upload
+        it."""
+        mask = self._selection(idx)
+        if mask is not None and isinstance(value, _Selected) and value.sel is idx:
+            call("qgb_field_set_selected", self.handle, value.field.handle, mask.ctypes.data_as(ctypes.c_void_p),
+                 mask.size)
+            return
+        if mask is not None and self.kind == KIND_REAL and np.isscalar(value):
+            call("qgb_field_fill", self.handle, float(value), mask.ctypes.data_as(ctypes.c_void_p), mask.size)
+            return
+        if isinstance(value, _Selected):
+            value = value.field.to_numpy()[value.sel]
+        a = self.to_numpy()
+        a[idx] = value
+        self.from_numpy(a)
+
+    def selected(self, sel) -> "_Selected":
+        """The entries of a boolean selection, for ``dst[sel] = src.selected(sel)``
+        (a GPU copy of the selected entries)."""
+        return _Selected(self, sel)
+
+
+class _Selected:
+    def __init__(self, field: Field, sel):
+        self.field = field
+        self.sel = sel
+
 
 class FieldColorMatrix(Field):
     _kind = KIND_COLOR_MATRIX
@@ -342,9 +412,17 @@ class GaugeMomentum(FieldColorMatrix):
     def set_rand(self, rng: RngState, sigma: float = 1.0):
         call("qgb_set_rand_gauge_momentum", self.handle, float(sigma), rng.c)
 
+    def set_rand_fa(self, mf: "FieldRealD", rng: RngState):
+        """set_rand_gauge_momentum(gm, mf, rs) (hmc.pyx:51-52, hmc.cpp:121-149)."""
+        call("qgb_set_rand_gauge_momentum_fa", self.handle, mf.handle, rng.c)
+
 
 def set_unit(gf: Field, coef: float = 1.0):
-    """field.h set_unit (everything.pxd:187) for color-matrix fields."""
+    """field.h set_unit (everything.pxd:187): coef times the unit matrix in
+    every entry of a color-matrix field, coef in every entry of a real field."""
+    if gf.kind == KIND_REAL:
+        call("qgb_field_fill", gf.handle, float(coef), None, 0)
+        return
     call("qgb_set_unit", gf.handle)
     if coef != 1.0:
         gf *= coef

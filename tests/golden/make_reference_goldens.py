@@ -10,6 +10,7 @@ Run in a checkout that has the reference source tree (default
   examples-py/hmc-pure-gauge-test.log.json    Python HMC from a unit start, plaq per trajectory
   examples-py/flow-and-smear.log.json         Wilson flow steps and energies
   examples-py/gf-utils.log.json               hot-start plaquette, clover and 5-loop charges along the flow
+  examples-py/hmc-pure-gauge-fa-sym.log.json  field-accelerated HMC, five jobs, plaq per trajectory
 """
 
 import json
@@ -68,6 +69,20 @@ def main():
                        "topo_5li_terms_sum": {str(t): g[f"t={t} topo_5li sum(topo_terms)"][0]
                                               for t in ("0", "1.0", "2.0", "3.0", "4.0", "5.0")},
                        "eps_topo": 1e-9}
+    # field-accelerated HMC: the log holds, per job of the script's default
+    # job list (in that order), the job's parameters then 'run_hmc: {traj} plaq'
+    src = open(os.path.join(ref, "examples-py/hmc-pure-gauge-fa-sym.py")).read()
+    tags = re.findall(r'"([^"]+)"', re.search(r"job_tag_list_default = \[(.*?)\]", src, re.S).group(1))
+    jobs = []
+    for e in json.load(open(os.path.join(ref, "examples-py/hmc-pure-gauge-fa-sym.log.json"))):
+        if len(e) == 1:
+            jobs.append({"job_tag": tags[len(jobs)], "params": json.loads(e[0]), "plaq": []})
+        else:
+            m = re.match(r"run_hmc: (\d+) plaq", e[0])
+            assert m and int(m.group(1)) == len(jobs[-1]["plaq"]) + 1
+            jobs[-1]["plaq"].append(e[1])
+    out["py_hmc_fa_sym"] = {"source": "examples-py/hmc-pure-gauge-fa-sym.log.json", "jobs": jobs,
+                            "reference_check_eps": 1e-5}
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "reference_goldens.json"), "w") as f:
         json.dump(out, f, indent=1)
