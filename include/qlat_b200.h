@@ -335,6 +335,47 @@ int qgb_gf_hamilton_flowed_node(const qgb_field* gf0, double beta, double c1, co
 int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double beta, double c1,
                             const qgb_flow_step* steps, int32_t n, int32_t with_det);
 
+/* ---- topology measurement: flows and site fields (instanton_map.py,
+ * qcd.cpp:33-62, 295-341, 391-414, wilson-flow.cpp:164-236) ----------------- */
+
+#define QGB_FLOW_TOPO_C1 0       /* gf_wilson_flow_step with the action's c1 (Wilson 0, Iwasaki -0.331, DBW2 -1.4008) */
+#define QGB_FLOW_TOPO_SHRINK 1   /* plaquette weight 0.005 / (1 - p + 0.005) + 0.5 */
+#define QGB_FLOW_TOPO_FREEZE 2   /* 1 - p */
+#define QGB_FLOW_TOPO_LOCALIZE 3 /* 0.002 / (1 - p + 0.002) + 50 (1 - p) */
+#define QGB_FLOW_TOPO_PRESERVE 4 /* max(1, 50 (1 - p)) */
+#define QGB_FLOW_INTEGRATOR_EULER 0
+#define QGB_FLOW_INTEGRATOR_RUNGE_KUTTA 1
+
+/* gf_plaq_field (qcd.cpp:295-341; qcd.pyx:209-213): f_plaq, an FP64 real field
+ * of multiplicity 6, gets Re tr P / 3 of the plaquettes at each site in the
+ * planes (0,1) (0,2) (0,3) (1,2) (1,3) (2,3). */
+int qgb_gf_plaq_field(qgb_field* f_plaq, const qgb_field* gf);
+/* clf_plaq_action_density_field (spatial = 0) / clf_spatial_plaq_action_density_field
+ * (spatial = 1) (qcd.cpp:33-62, 391-414; topology.pyx:26-75): per site, sum over
+ * the planes (spatial: (0,1) (0,2) (1,2)) of 1 - Re tr C / 3, C the clover
+ * average of the four plaquettes with a corner at the site; paf: FP64 real,
+ * multiplicity 1. */
+int qgb_gf_plaq_action_density_field(qgb_field* paf, const qgb_field* gf, int32_t spatial);
+/* set_plaq_flow_z (wilson-flow.cpp:164-236; gf_plaq_flow_force, wilson_flow.pyx:65-75):
+ * the Wilson-flow force with each plaquette weighted by plaq_factor (FP64 real,
+ * multiplicity 6, planes as in qgb_gf_plaq_field). */
+int qgb_set_plaq_flow_z(qgb_field* z, const qgb_field* gf, const qgb_field* plaq_factor);
+/* gf_flow_topo(gf, step_size, flow_type, integrator) (instanton_map.py:91-191):
+ * QGB_FLOW_TOPO_C1 takes one gf_wilson_flow_step with c1 and the integrator;
+ * the plaquette-weighted kinds take one Euler step of step_size / norm along the
+ * weighted force, norm the weight's extreme over the lattice.  advance (may be
+ * NULL) = the flow time taken, step_size / norm. */
+int qgb_gf_flow_topo(qgb_field* gf, double step_size, int32_t flow_kind, double c1, int32_t integrator,
+                     double* advance);
+/* glb_min / glb_max of each component of a real field (either output may be
+ * NULL; each holds multiplicity values). */
+int qgb_field_glb_min_max(const qgb_field* f, double* mins, double* maxs);
+/* glb_sum_tslice (field_base.pyx:750-762): out[t * multiplicity + m] = sum over
+ * the sites with coordinate t in direction t_dir of component m (real field). */
+int qgb_field_glb_sum_tslice(const qgb_field* f, int32_t t_dir, double* out);
+/* f = |f| entrywise (real field). */
+int qgb_field_abs(qgb_field* f);
+
 /* ---- field-accelerated HMC: per-link masses and dual momenta (hmc.h:20-80) */
 
 /* A mass field is an FP64 real field of multiplicity 4 (Field<RealD>, one mass

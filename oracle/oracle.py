@@ -113,6 +113,10 @@ def lib():
             "or_project_gauge_transform": (ctypes.c_double, [_dbl_p, _dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_set_gauge_transform_momentum": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_dot_gauge_momentum": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
+            "or_gf_plaq_field": (None, [_dbl_p, _dbl_p, _int4]),
+            "or_clf_plaq_action_density_field": (None, [_dbl_p, _dbl_p, _int4, ctypes.c_int]),
+            "or_set_plaq_flow_z": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
+            "or_gf_flow_topo_plaq": (ctypes.c_double, [_dbl_p, _int4, ctypes.c_double, ctypes.c_int]),
             "or_make_matrix_exp": (None, [_dbl_p, _dbl_p, ctypes.c_int]),
             "or_unitarize": (None, [_dbl_p]),
             "or_make_tr_less_anti_herm": (None, [_dbl_p, _dbl_p]),
@@ -347,6 +351,42 @@ def dot_gauge_momentum(gm1, gm2, total_site) -> np.ndarray:
     f = np.zeros((volume(total_site), 4), dtype=np.float64)
     lib().or_dot_gauge_momentum(_p(f), _p(gm1), _p(gm2), _dims(total_site))
     return f
+
+
+# ---- topology-measurement flows (qcd.cpp, wilson-flow.cpp:164-236, instanton_map.py) ----
+
+PLAQ_FLOW_KINDS = {"Shrink": 1, "Freeze": 2, "Localize": 3, "Preserve": 4}
+
+
+def gf_plaq_field(gf, total_site) -> np.ndarray:
+    """qcd.cpp:295-341: (V, 6)."""
+    f = np.zeros((volume(total_site), 6), dtype=np.float64)
+    lib().or_gf_plaq_field(_p(f), _p(gf), _dims(total_site))
+    return f
+
+
+def clf_plaq_action_density_field(gf, total_site, spatial: bool = False) -> np.ndarray:
+    """qcd.cpp:33-62, 391-414: (V,)."""
+    f = np.zeros(volume(total_site), dtype=np.float64)
+    lib().or_clf_plaq_action_density_field(_p(f), _p(gf), _dims(total_site), int(spatial))
+    return f
+
+
+def set_plaq_flow_z(gf, plaq_factor, total_site) -> np.ndarray:
+    z = new_field(total_site)
+    lib().or_set_plaq_flow_z(_p(z), _p(gf), _p(np.ascontiguousarray(plaq_factor)), _dims(total_site))
+    return z
+
+
+def gf_flow_topo(gf, total_site, step_size: float, flow_type=None, integrator: str = "euler") -> float:
+    """instanton_map.py:91-191 on the oracle: returns the flow time taken."""
+    if flow_type is None:
+        flow_type = "Wilson"
+    if flow_type in PLAQ_FLOW_KINDS:
+        return lib().or_gf_flow_topo_plaq(_p(gf), _dims(total_site), step_size, PLAQ_FLOW_KINDS[flow_type])
+    c1 = {"Wilson": 0.0, "Iwasaki": -0.331, "DBW2": -1.4008}.get(flow_type, flow_type)
+    gf_wilson_flow_step(gf, total_site, step_size, float(c1), integrator)
+    return step_size
 
 
 def run_hmc_evolve(gm, gf, total_site, beta, c1, n_step, md_time=1.0, integrator="force-gradient") -> float:

@@ -1291,6 +1291,141 @@ void or_dot_gauge_momentum(double* f, const double* gm1, const double* gm2, cons
   }
 }
 
+/* ------------------------------------------------------------------ */
+/* topology-measurement flows                                           */
+
+static const int PLANE_A[6] = {0, 0, 0, 1, 1, 2};
+static const int PLANE_B[6] = {1, 2, 3, 2, 3, 3};
+
+/* qcd.cpp:84-91 gf_plaq_no_comm: Re tr(U_a(x) U_b(x+a) (U_b(x) U_a(x+b))^+) / 3 */
+static double plaq_at(const double* gf, const geo_t* g, const int x[4], int a, int b)
+{
+  int xa[4] = {x[0], x[1], x[2], x[3]}, xb[4] = {x[0], x[1], x[2], x[3]};
+  xa[a] += 1;
+  xb[b] += 1;
+  cm ua = get_link(gf, g, x, a), ub = get_link(gf, g, x, b);
+  cm ub_a = get_link(gf, g, xa, b), ua_b = get_link(gf, g, xb, a);
+  cm l = m_mul(&ua, &ub_a);
+  cm r = m_mul(&ub, &ua_b);
+  cm ra = m_adj(&r);
+  cm p = m_mul(&l, &ra);
+  return m_trace(&p).re / 3.0;
+}
+
+/* qcd.cpp:298-325 */
+void or_gf_plaq_field(double* f_plaq, const double* gf, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    for (int p = 0; p < 6; ++p) f_plaq[i * 6 + p] = plaq_at(gf, &g, x, PLANE_A[p], PLANE_B[p]);
+  }
+}
+
+/* qcd.cpp:33-62 with the clover leaves of qcd.cpp:10-31 */
+void or_clf_plaq_action_density_field(double* paf, const double* gf, const int dims[4], int spatial)
+{
+  const geo_t g = mk_geo(dims);
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    double sum = 0.0;
+    for (int p = 0; p < 6; ++p) {
+      if (spatial && (p == 2 || p == 4 || p == 5)) continue;
+      cm c = clover_leaf(gf, &g, x, PLANE_A[p], PLANE_B[p]);
+      sum += 1.0 - 1.0 / 3.0 * m_trace(&c).re;
+    }
+    paf[i] = sum;
+  }
+}
+
+static int plane_index(int mu, int nu)
+{
+  const int a = mu < nu ? mu : nu, b = mu < nu ? nu : mu;
+  for (int p = 0; p < 6; ++p)
+    if (PLANE_A[p] == a && PLANE_B[p] == b) return p;
+  return -1;
+}
+
+/* wilson-flow.cpp:164-207 */
+void or_set_plaq_flow_z(double* z, const double* gf, const double* plaq_factor, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    for (int mu = 0; mu < 4; ++mu) {
+      cm acc = m_zero();
+      for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        int xn[4] = {x[0], x[1], x[2], x[3]};
+        xn[nu] -= 1;
+        const long in = index_from_coor(&g, xn);
+        const int m = plane_index(mu, nu);
+        const int p1[3] = {nu, mu, -nu - 1};
+        const int p2[3] = {-nu - 1, mu, nu};
+        cm w1 = wilson_line(gf, &g, x, p1, 3);
+        cm w2 = wilson_line(gf, &g, x, p2, 3);
+        cm t1 = m_rscale(plaq_factor[i * 6 + m], &w1);
+        m_add_to(&acc, &t1);
+        cm t2 = m_rscale(plaq_factor[in * 6 + m], &w2);
+        m_add_to(&acc, &t2);
+      }
+      cm ad = m_adj(&acc);
+      cm u = get_link(gf, &g, x, mu);
+      cm f = m_mul(&u, &ad);
+      f = m_rscale(-1.0, &f);
+      cm r = make_tr_less_anti_herm(&f);
+      put_link(z, i, mu, &r);
+    }
+  }
+}
+
+/* instanton_map.py:162-190 */
+double or_gf_flow_topo_plaq(double* gf, const int dims[4], double step_size, int kind)
+{
+  const geo_t g = mk_geo(dims);
+  double* fp = (double*)malloc(sizeof(double) * 6 * (size_t)g.vol);
+  double* pf = (double*)malloc(sizeof(double) * 6 * (size_t)g.vol);
+  double* z = (double*)malloc(sizeof(double) * 72 * (size_t)g.vol);
+  or_gf_plaq_field(fp, gf, dims);
+  double pmin = fp[0], pmax = fp[0];
+  for (long i = 0; i < 6 * g.vol; ++i) {
+    if (fp[i] < pmin) pmin = fp[i];
+    if (fp[i] > pmax) pmax = fp[i];
+  }
+  double norm = 1.0;
+  for (long i = 0; i < 6 * g.vol; ++i) {
+    const double p = fp[i];
+    double v;
+    if (kind == 1) v = 0.005 / (1 - p + 0.005) + 0.5;
+    else if (kind == 2) v = 1 - p;
+    else if (kind == 3) v = 0.002 / (1 - p + 0.002) + (50 * (1 - p));
+    else { v = 50 * (1 - p); if (v < 1) v = 1; }
+    pf[i] = v;
+  }
+  if (kind == 1) norm = 0.005 / (1 - pmax + 0.005) + 0.5;
+  else if (kind == 2) norm = 1 - pmin;
+  else if (kind == 3) {
+    const double a = 0.002 / (1 - pmax + 0.002) + (50 * (1 - pmax));
+    const double b = 0.002 / (1 - pmin + 0.002) + (50 * (1 - pmin));
+    norm = a > b ? a : b;
+  } else {
+    norm = 50 * (1 - pmin);
+    if (norm < 1) norm = 1;
+  }
+  or_set_plaq_flow_z(z, gf, pf, dims);
+  or_gf_evolve(gf, z, dims, step_size / norm);
+  free(fp);
+  free(pf);
+  free(z);
+  return step_size / norm;
+}
+
 void or_make_matrix_exp(double out[18], const double a[18], int max_order)
 {
   cm x;

@@ -97,6 +97,15 @@ void or_set_gm_force_dual(double* fd, const double* gf, const double* f, const i
 double or_project_gauge_transform(double* gm, double* gmd, const double* mf, const double* mfd, const int dims[4]);
 void or_set_gauge_transform_momentum(double* gm, double* gmd, const double* gtm, const int dims[4]);
 void or_dot_gauge_momentum(double* f, const double* gm1, const double* gm2, const int dims[4]);
+/* Topology-measurement flows (qcd.cpp:33-62, 295-341; wilson-flow.cpp:164-236;
+ * instanton_map.py:91-191).  Plaquette fields hold 6 doubles per site, planes
+ * (0,1) (0,2) (0,3) (1,2) (1,3) (2,3). */
+void or_gf_plaq_field(double* f_plaq, const double* gf, const int dims[4]);
+void or_clf_plaq_action_density_field(double* paf, const double* gf, const int dims[4], int spatial);
+void or_set_plaq_flow_z(double* z, const double* gf, const double* plaq_factor, const int dims[4]);
+/* one step of a plaquette-weighted flow: kind 1 Shrink, 2 Freeze, 3 Localize,
+ * 4 Preserve; returns step_size / norm */
+double or_gf_flow_topo_plaq(double* gf, const int dims[4], double step_size, int kind);
 /* Single-matrix helpers used by the tests. */
 void or_make_matrix_exp(double out[18], const double a[18], int max_order);
 void or_unitarize(double m[18]);

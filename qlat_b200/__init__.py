@@ -23,6 +23,9 @@ from .flowed_hmc import (FlowInfo, FlowStepInfo, gf_flow, gf_flow_and_ln_det_nod
 from .hmc_fa import (MomentumAutoCorr, dot_gauge_momentum, gf_evolve_dual, gf_evolve_fa, gf_evolve_fa_dual,
                      gm_hamilton_node_fa, project_gauge_transform, run_hmc_fa, set_gauge_transform_momentum,
                      set_gm_force_dual, set_rand_gauge_momentum_fa)
+from .topo_measure import (gf_energy_derivative_density_field_topo, gf_flow_topo, gf_plaq_action_density,
+                           gf_plaq_action_density_field, gf_plaq_field, gf_plaq_flow_force,
+                           gf_spatial_plaq_action_density, gf_spatial_plaq_action_density_field, smear_measure_topo)
 from .flow_adjoint import (FlowedWilsonAction, gf_flow_action, gf_flow_action_grad, gf_wilson_flow_vjp,
                            run_flowed_hmc_pure_gauge, set_anti_hermitian_matrix_from_basis,
                            set_basis_from_anti_hermitian_matrix)

@@ -59,6 +59,13 @@ SIGNATURES = {
     "qgb_field_set_g_rand": [c_field, c_u32_p, ctypes.c_double, ctypes.c_double],
     "qgb_field_fill": [c_field, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64],
     "qgb_field_set_selected": [c_field, c_field, ctypes.c_void_p, ctypes.c_int64],
+    "qgb_gf_plaq_field": [c_field, c_field],
+    "qgb_gf_plaq_action_density_field": [c_field, c_field, ctypes.c_int32],
+    "qgb_set_plaq_flow_z": [c_field, c_field, c_field],
+    "qgb_gf_flow_topo": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, c_dbl_p],
+    "qgb_field_glb_min_max": [c_field, c_dbl_p, c_dbl_p],
+    "qgb_field_glb_sum_tslice": [c_field, ctypes.c_int32, c_dbl_p],
+    "qgb_field_abs": [c_field],
     "qgb_field_info": [c_field, i32x4, c_i32_p, c_i32_p, c_i32_p],
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],

@@ -338,7 +338,22 @@ class FieldRealD(Field):
     _kind = KIND_REAL
 
     def glb_sum(self) -> np.ndarray:
-        return self.to_numpy().sum(axis=0, keepdims=True)
+        """Sum over the lattice of each component, shape (1, multiplicity)."""
+        from .topo_measure import glb_sum
+        return glb_sum(self)
+
+    def glb_sum_tslice(self, *, t_dir: int = 3) -> np.ndarray:
+        """Per-timeslice sums (field_base.pyx:750-762), shape (T, multiplicity)."""
+        from .topo_measure import glb_sum_tslice
+        return glb_sum_tslice(self, t_dir=t_dir)
+
+    def glb_min(self) -> np.ndarray:
+        from .topo_measure import glb_min
+        return glb_min(self)
+
+    def glb_max(self) -> np.ndarray:
+        from .topo_measure import glb_max
+        return glb_max(self)
 
 
 class GaugeField(FieldColorMatrix):

@@ -11,6 +11,7 @@ Run in a checkout that has the reference source tree (default
   examples-py/flow-and-smear.log.json         Wilson flow steps and energies
   examples-py/gf-utils.log.json               hot-start plaquette, clover and 5-loop charges along the flow
   examples-py/hmc-pure-gauge-fa-sym.log.json  field-accelerated HMC, five jobs, plaq per trajectory
+  examples-py/gf-flow-topo.log.json           Wilson and plaquette-weighted flows: plaq, plaq_min, flow time, signatures
 """
 
 import json
@@ -60,6 +61,8 @@ def main():
                    "c1_plaq": {str(c1): g[f"gf_wilson_flow_step c1={c1} plaq"][0] for c1 in (0.0, -0.331, -1.4008)},
                    "flow3_energy": g["gf_wilson_flow energy_list"][0]["value"],
                    "flow3_plaq": g["gf_wilson_flow final plaq"][0],
+                   "flow_topo": {k[len("gf_flow_topo "):-len(" plaq")]: v[0] for k, v in g.items()
+                                 if k.startswith("gf_flow_topo ")},
                    "eps": 1e-10}
     g = load("gf-utils.log.json")
     out["gf_utils"] = {"source": "examples-py/gf-utils.log.json",
@@ -83,6 +86,19 @@ def main():
             jobs[-1]["plaq"].append(e[1])
     out["py_hmc_fa_sym"] = {"source": "examples-py/hmc-pure-gauge-fa-sym.log.json", "jobs": jobs,
                             "reference_check_eps": 1e-5}
+    # gf_flow_topo stages: (name, value) in log order; complex signature
+    # entries as [re, im] pairs
+    rows = []
+    for e in json.load(open(os.path.join(ref, "examples-py/gf-flow-topo.log.json"))):
+        if len(e) != 3:
+            continue
+        v = e[1]
+        if isinstance(v, dict):
+            v = [[x["real"], x["imag"]] if isinstance(x, dict) else x for x in v["value"]]
+        rows.append([e[0], v])
+    out["gf_flow_topo"] = {"source": "examples-py/gf-flow-topo.log.json", "rows": rows, "eps": 1e-10,
+                           "flow_order": [None, "Freeze", "Shrink", "Localize", "Preserve"], "n_step": 5,
+                           "step_size": 0.1}
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "reference_goldens.json"), "w") as f:
         json.dump(out, f, indent=1)
