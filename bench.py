@@ -287,25 +287,35 @@ def our_arm(args):
     del g_a, g_b, m_a, m_b
 
     # end to end through the public API: host gauge configuration in pinned
-    # memory uploaded every step, trajectory, delta_h + plaquette read back
+    # memory uploaded every step, trajectory, delta_h + plaquette read back.
+    # The uploads go through qgb_field_upload_pipelined: each step commits its
+    # configuration (prefetched by the step before; the first is copied when
+    # it is committed) and starts the next step's host-to-device copy, which
+    # then runs on the copy engine under the trajectory.  Every copy is inside
+    # the timed region.
     e2e = None
     if not args.no_e2e:
         host = torch.empty((V, 4, 3, 3), dtype=torch.complex128, pin_memory=True)
         host.numpy()[...] = gf.to_numpy()
-        n_e2e = max(2, min(args.steps, 5))
+        n_e2e = max(2, min(args.steps, 10))
+        # allocate the two staging slots outside the timed region (no prefetch left pending)
+        gf.upload_host_pipelined(host.data_ptr(), host.data_ptr())
+        gf.upload_host_pipelined(host.data_ptr(), None)
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for i in range(n_e2e):
-            gf.upload_host(host.data_ptr())
+            gf.upload_host_pipelined(host.data_ptr(), host.data_ptr() if i + 1 < n_e2e else None)
             dh, fl = trajectory(traj + 1 + i, "mixed")
             _ = q.gf_avg_plaq(gf)
         e1.record(stream)
         torch.cuda.synchronize()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
-        e2e = {"value": job_throughput(world, n_e2e, ms_e2e), "unit": "traj/s",
-               "h2d_bytes_per_step": V * 4 * 9 * 16, "d2h_bytes_per_step": 8 * 2 + 8 * 6}
+        e2e = {"value": job_throughput(world, n_e2e, ms_e2e), "unit": "traj/s", "steps": n_e2e,
+               "h2d_bytes_per_step": V * 4 * 9 * 16, "d2h_bytes_per_step": 8 * 2 + 8 * 6,
+               "h2d": "pinned host, one full FP64 configuration per step; each step's copy overlaps the "
+                      "previous trajectory (copy stream, two staging slots), the first one is not overlapped"}
 
     if rank != 0:
         if dist is not None:

@@ -83,6 +83,14 @@ int qgb_field_info(const qgb_field* f, int32_t total_site[4], int32_t* multiplic
  * Color-matrix fields take complex128 (double pairs); real fields take double. */
 int qgb_field_upload(qgb_field* f, const double* host);
 int qgb_field_download(const qgb_field* f, double* host);
+/* Stream a sequence of host configurations into f, overlapping each copy with
+ * the work queued after it: copy host_now into f (from the library's staging
+ * copy if an earlier call prefetched it, else now), then start the
+ * host-to-device copy of host_next (may be NULL) on a library copy stream, to
+ * be committed by the next call with host_now = host_next.  The prefetch reads
+ * host_next when the copy engine reaches it: keep that buffer unchanged until
+ * the next call.  Overlap needs pinned host memory. */
+int qgb_field_upload_pipelined(qgb_field* f, const double* host_now, const double* host_next);
 /* Same, from / into a device buffer in the reference memory image. */
 int qgb_field_upload_device(qgb_field* f, const double* dev);
 int qgb_field_download_device(const qgb_field* f, double* dev);

@@ -70,6 +70,7 @@ SIGNATURES = {
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],
     "qgb_field_upload_device": [c_field, ctypes.c_void_p],
+    "qgb_field_upload_pipelined": [c_field, ctypes.c_void_p, ctypes.c_void_p],
     "qgb_field_download_device": [c_field, ctypes.c_void_p],
     "qgb_field_copy": [c_field, c_field],
     "qgb_field_set_zero": [c_field],

@@ -79,6 +79,18 @@ struct Ctx {
   bool prof_on = false;
   std::map<std::string, ProfEntry> prof;
   std::vector<cudaEvent_t> event_pool;
+  // pipelined host uploads (qgb_field_upload_pipelined): a copy stream and two
+  // device staging slots; slot i holds the copy of up_host[i] once up_ready[i]
+  // has fired, and up_order[i] orders its next copy after the work queued on
+  // the library stream (the conversion that last read the slot included)
+  cudaStream_t copy_stream = nullptr;
+  void* up_buf[2] = {nullptr, nullptr};
+  size_t up_cap[2] = {0, 0};
+  const double* up_host[2] = {nullptr, nullptr};
+  size_t up_bytes[2] = {0, 0};
+  cudaEvent_t up_ready[2] = {nullptr, nullptr};
+  cudaEvent_t up_order[2] = {nullptr, nullptr};
+  int up_next = 0;
 };
 
 Ctx g_ctx;
@@ -688,6 +700,57 @@ int qgb_field_upload(qgb_field* f, const double* host)
   QGB_RC(ensure_staging(bytes));
   QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.staging, host, bytes, cudaMemcpyHostToDevice, g_ctx.stream));
   QGB_RC(upload_from_device_aos(f, g_ctx.staging));
+  return QGB_OK;
+}
+
+// Copy `bytes` from `host` into staging slot `i` on the copy stream, after the
+// work queued so far on the library stream.
+static int up_start(int i, const double* host, size_t bytes)
+{
+  if (!g_ctx.copy_stream) {
+    QGB_TRY_CUDA(cudaStreamCreateWithFlags(&g_ctx.copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+      QGB_TRY_CUDA(cudaEventCreateWithFlags(&g_ctx.up_ready[k], cudaEventDisableTiming));
+      QGB_TRY_CUDA(cudaEventCreateWithFlags(&g_ctx.up_order[k], cudaEventDisableTiming));
+    }
+  }
+  if (g_ctx.up_cap[i] < bytes) {
+    // a queued conversion may still read the old buffer
+    QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+    if (g_ctx.up_buf[i]) QGB_TRY_CUDA(cudaFree(g_ctx.up_buf[i]));
+    g_ctx.up_buf[i] = nullptr;
+    g_ctx.up_cap[i] = 0;
+    QGB_TRY_CUDA(cudaMalloc(&g_ctx.up_buf[i], bytes));
+    g_ctx.up_cap[i] = bytes;
+  }
+  QGB_TRY_CUDA(cudaEventRecord(g_ctx.up_order[i], g_ctx.stream));
+  QGB_TRY_CUDA(cudaStreamWaitEvent(g_ctx.copy_stream, g_ctx.up_order[i], 0));
+  QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.up_buf[i], host, bytes, cudaMemcpyHostToDevice, g_ctx.copy_stream));
+  QGB_TRY_CUDA(cudaEventRecord(g_ctx.up_ready[i], g_ctx.copy_stream));
+  g_ctx.up_host[i] = host;
+  g_ctx.up_bytes[i] = bytes;
+  return QGB_OK;
+}
+
+int qgb_field_upload_pipelined(qgb_field* f, const double* host_now, const double* host_next)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_upload_pipelined"));
+  QGB_CHECK(host_now, QGB_ERR_INVALID_ARG, "qgb_field_upload_pipelined: null host buffer");
+  const size_t bytes = (size_t)n_reals(f) * sizeof(double);
+  int i = -1;
+  for (int k = 0; k < 2; ++k)
+    if (g_ctx.up_host[k] == host_now && g_ctx.up_bytes[k] == bytes) i = k;
+  if (i < 0) {  // not prefetched: copy it now
+    i = g_ctx.up_next;
+    QGB_RC(up_start(i, host_now, bytes));
+  }
+  QGB_TRY_CUDA(cudaStreamWaitEvent(g_ctx.stream, g_ctx.up_ready[i], 0));
+  QGB_RC(upload_from_device_aos(f, (const double*)g_ctx.up_buf[i]));
+  g_ctx.up_host[i] = nullptr;
+  g_ctx.up_bytes[i] = 0;
+  g_ctx.up_next = 1 - i;
+  if (host_next) QGB_RC(up_start(1 - i, host_next, bytes));
   return QGB_OK;
 }
 

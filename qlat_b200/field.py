@@ -269,6 +269,13 @@ class Field:
         in the reference memory image."""
         call("qgb_field_upload", self.handle, ctypes.cast(ctypes.c_void_p(ptr), _lib.c_dbl_p))
 
+    def upload_host_pipelined(self, ptr_now: int, ptr_next: int | None = None) -> None:
+        """Copy the host image at ``ptr_now`` into the field and start copying the
+        one at ``ptr_next`` to the GPU behind the work that follows, for the next
+        call to commit (``qgb_field_upload_pipelined``; pinned host memory)."""
+        call("qgb_field_upload_pipelined", self.handle, ctypes.c_void_p(ptr_now),
+             None if ptr_next is None else ctypes.c_void_p(ptr_next))
+
     def upload_device(self, ptr: int) -> None:
         """Copy from a device buffer (e.g. a torch CUDA tensor's data_ptr) in
         the reference memory image."""

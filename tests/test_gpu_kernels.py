@@ -214,3 +214,31 @@ def test_every_force_variant(q, oracle, prec):
     finally:
         q.force_set_variant(P, False, 0)
         q.force_set_variant(P, True, 0)
+
+
+@pytest.mark.gpu
+def test_upload_pipelined(q):
+    """qgb_field_upload_pipelined: each call leaves the field equal to host_now,
+    whether it was prefetched by the call before or not (pinned and pageable
+    buffers, changing buffers, FP64 and FP32 fields)."""
+    import torch
+    geo = q.Geometry((4, 4, 4, 8))
+    V = geo.total_volume
+    rng = np.random.default_rng(11)
+    bufs = []
+    for pinned in (True, True, False):
+        t = torch.empty((V, 4, 3, 3), dtype=torch.complex128, pin_memory=pinned)
+        t.numpy()[...] = rng.standard_normal((V, 4, 3, 3)) + 1j * rng.standard_normal((V, 4, 3, 3))
+        bufs.append(t)
+    for prec in (q.F64, q.F32):
+        gf = q.GaugeField(geo, precision=prec)
+        tol = 0 if prec == q.F64 else 1e-6
+        order = [0, 1, 0, 2, 2, 1]
+        for k, i in enumerate(order):
+            nxt = bufs[order[k + 1]].data_ptr() if k + 1 < len(order) else None
+            gf.upload_host_pipelined(bufs[i].data_ptr(), nxt)
+            assert np.abs(np.asarray(gf) - bufs[i].numpy()).max() <= tol * 10, (prec, k)
+        # a prefetch that is not committed next is dropped, not applied
+        gf.upload_host_pipelined(bufs[0].data_ptr(), bufs[1].data_ptr())
+        gf.upload_host_pipelined(bufs[2].data_ptr(), None)
+        assert np.abs(np.asarray(gf) - bufs[2].numpy()).max() <= tol * 10
