@@ -405,3 +405,37 @@ def test_run_hmc_fa_reference_log(q, goldens):
         recs = q.run_hmc_fa(job["params"], job["job_tag"])
         for rec, b in zip(recs, job["plaq"]):
             assert abs(rec["plaq"] - b) <= GOLDEN_EPS * abs(b), (job["job_tag"], rec["traj"], rec["plaq"], b)
+
+
+@pytest.mark.gpu
+def test_gpu_fa_odd_lattice(q, oracle):
+    """3x4x5x6 (V = 360, not a multiple of the 32-site blocks): projection,
+    dual force and both evolutions against the oracle, masses with +inf."""
+    o = oracle
+    ts = (3, 4, 5, 6)
+    _, gf0, mf, mfd, gm, gmd = seeded_inputs(o, ts, "fa-odd")
+    geo = q.Geometry(ts)
+    up = lambda a, f: (f.from_numpy(a), f)[1]  # noqa: E731
+    qmf, qmfd = up(mf, q.FieldRealD(geo, 4)), up(mfd, q.FieldRealD(geo, 4))
+    qgm, qgmd = up(gm, q.GaugeMomentum(geo)), up(gmd, q.GaugeMomentum(geo))
+    qgf = up(gf0, q.GaugeField(geo))
+    a, b = qgm.copy(), qgmd.copy()
+    ch = q.project_gauge_transform(a, b, qmf, qmfd)
+    ra, rb = gm.copy(), gmd.copy()
+    assert abs(ch - o.project_gauge_transform(ra, rb, mf, mfd, ts)) < 1e-13 * ch
+    assert np.abs(np.asarray(a) - ra).max() < 1e-14 and np.abs(np.asarray(b) - rb).max() < 1e-14
+    g = qgf.copy()
+    q.gf_evolve_fa(g, qgm, qmf, DT)
+    q.gf_evolve_fa_dual(g, qgmd, qmfd, DT)
+    r = gf0.copy()
+    o.gf_evolve_fa(r, gm, mf, ts, DT)
+    o.gf_evolve_fa_dual(r, gmd, mfd, ts, DT)
+    assert np.abs(np.asarray(g) - r).max() < 1e-14
+    F, Fd = q.GaugeMomentum(geo), q.GaugeMomentum(geo)
+    q.set_gm_force(F, qgf, q.GaugeAction(BETA, C1))
+    q.set_gm_force_dual(Fd, qgf, F)
+    rfd = o.new_field(ts)
+    o.set_gm_force_dual(rfd, gf0, np.asarray(F), ts)
+    assert np.abs(np.asarray(Fd) - rfd).max() < 1e-13
+    assert abs(q.gm_hamilton_node_fa(qgm, qmf) - o.gm_hamilton_node_fa(gm, mf, ts)) < 1e-12 * o.gm_hamilton_node_fa(
+        gm, mf, ts)

@@ -266,3 +266,31 @@ def test_gpu_smear_measure_topo_matches_oracle(q, oracle, tmp_path):
     assert (tmp_path / "info" / "info.pickle").exists()
     assert (tmp_path / "df" / "smear-step-0" / "topo.npy").exists()
     assert math.isclose(topo[-1]["flow_time"], topo_r[-1]["flow_time"], rel_tol=1e-13)
+
+
+@pytest.mark.gpu
+def test_gpu_odd_lattice(q, oracle):
+    """3x4x5x6 (V = 360, padded 32-site blocks, odd extents): plaquette field,
+    action densities, weighted flow step and per-timeslice sums."""
+    o = oracle
+    ts = (3, 4, 5, 6)
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("odd").split("gf-init"), 0.4, 2)
+    ref = o.new_field(ts)
+    o.gf_set_rand(ref, ts, o.RngState("odd").split("gf-init"), 0.4, 2)
+    fp = q.gf_plaq_field(gf)
+    assert np.abs(fp.to_numpy() - o.gf_plaq_field(ref, ts)).max() < 1e-14
+    for spatial in (False, True):
+        f = q.gf_spatial_plaq_action_density_field(gf) if spatial else q.gf_plaq_action_density_field(gf)
+        assert np.abs(f.to_numpy()[:, 0] - o.clf_plaq_action_density_field(ref, ts, spatial)).max() < 1e-13
+    a = fp.to_numpy()
+    xg = q.Geometry(ts).xg_arr()
+    for t_dir in range(4):
+        want = np.stack([a[xg[:, t_dir] == t].sum(axis=0) for t in range(ts[t_dir])])
+        assert np.abs(fp.glb_sum_tslice(t_dir=t_dir) - want).max() < 1e-12
+    assert np.array_equal(fp.glb_min(), a.min(axis=0, keepdims=True))
+    for kind in ("Localize", "Shrink"):
+        g, r = gf.copy(), ref.copy()
+        adv = q.gf_flow_topo(g, 0.1, kind)
+        assert abs(adv - o.gf_flow_topo(r, ts, 0.1, kind)) < 1e-13 * adv
+        assert np.abs(np.asarray(g) - r).max() < 1e-12, kind
