@@ -66,6 +66,7 @@ SIGNATURES = {
     "qgb_field_glb_min_max": [c_field, c_dbl_p, c_dbl_p],
     "qgb_field_glb_sum_tslice": [c_field, ctypes.c_int32, c_dbl_p],
     "qgb_field_abs": [c_field],
+    "qgb_fp32_fma_rate": [ctypes.c_int32, ctypes.c_int32, c_dbl_p],
     "qgb_field_info": [c_field, i32x4, c_i32_p, c_i32_p, c_i32_p],
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],

@@ -25,7 +25,7 @@ LIB = os.path.join(HERE, "libqlat_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-Xptxas", "-O3"]
-SOURCES = ["kernels.cu", "force_f64.cu", "force_f32.cu", "force_variants.cu", "noalloc.cu", "nersc_io.cu", "flowed.cu", "fa.cu", "topo_flow.cu", "batch.cu", "adjoint.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "force_f64.cu", "force_f32.cu", "force_variants.cu", "noalloc.cu", "nersc_io.cu", "flowed.cu", "fa.cu", "topo_flow.cu", "probes.cu", "batch.cu", "adjoint.cu", "capi.cu"]
 
 
 def nvcc() -> str:

@@ -4,6 +4,8 @@
         time every force-kernel launch variant (FP64 / FP32, Wilson / Iwasaki)
     python -m qlat_b200.kernel_bench force-profile --variants 0,7 [--lattice 24,24,24,48]
         one set_gm_force launch per variant and precision (Iwasaki), for ncu -k regex:k_force
+    python -m qlat_b200.kernel_bench fma-peak [--reps 5]
+        FP32 FMA rate of the device: scalar FFMA chains and packed f32x2 chains
     python -m qlat_b200.kernel_bench flow [--lattice 32,32,32,32] [--steps 80] [--every 4]
         gradient flow (RK3, eps = 0.05) with t^2 E(t) and the clover charge Q measured every
         `every` steps, FP64 and FP32 storage; prints timings and the FP32 errors
@@ -59,6 +61,20 @@ def force_profile(args):
             q.set_gm_force(F, g, ga)
     q.synchronize()
     print(json.dumps({"lattice": list(ts), "variants": variants, "launches": 2 * len(variants)}))
+
+
+def fma_peak(args):
+    import ctypes
+
+    import torch
+    from qlat_b200._lib import call
+    torch.cuda.set_device(0)
+    out = {}
+    for name, packed in (("scalar_ffma", 0), ("packed_ffma2", 1)):
+        t = ctypes.c_double()
+        call("qgb_fp32_fma_rate", packed, int(args.reps), ctypes.byref(t))
+        out[name + "_tflops"] = t.value
+    print(json.dumps(out))
 
 
 def flow(args):
@@ -270,9 +286,11 @@ def main():
     e.add_argument("--hmc-steps", type=int, default=20)
     e.add_argument("--hmc-flow-steps", type=int, default=2)
     e.add_argument("--hmc-warmup", type=int, default=10)
+    f = sub.add_parser("fma-peak")
+    f.add_argument("--reps", type=int, default=5)
     args = ap.parse_args()
     {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch,
-     "flow-adjoint": flow_adjoint}[args.cmd](args)
+     "flow-adjoint": flow_adjoint, "fma-peak": fma_peak}[args.cmd](args)
 
 
 if __name__ == "__main__":
