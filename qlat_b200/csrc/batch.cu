@@ -1,7 +1,7 @@
 // batch.cu -- many independent pure-gauge HMC chains advanced together.
 //
 // The chains (each with its own lattice, beta and c1) are concatenated into
-// one structure-of-arrays field of Vtot sites; every phase of a trajectory --
+// one field of Vtot sites (blocked layout of gauge_common.cuh); every phase of a trajectory --
 // momentum refresh, Hamiltonians, forces, exponentials -- is one launch over
 // all chains.  The whole trajectory is recorded once as a CUDA graph per
 // (n_step, md_time, integrator, precision) and replayed, so a trajectory of

@@ -1,12 +1,11 @@
 // kernels.cu -- CUDA kernels of the pure-gauge hot path for sm_100a.
 //
-// Memory layout in HBM: a color-matrix field with multiplicity m over V sites
-// is stored structure-of-arrays, element (site, mu, k) of the 3x3 matrix at
-// Cx<R>[(mu * 9 + k) * V + site], sites in the reference's order (x fastest,
-// coordinate.h:182-188).  A warp touches 32 consecutive sites per component,
-// so every load and store is a fully coalesced 512-byte (FP64) or 256-byte
-// (FP32) transaction.  Neighbour links come through L1/L2; the lattice is
-// periodic.
+// Memory layout in HBM (gauge_common.cuh): sites in the reference's order (x
+// fastest, coordinate.h:182-188) cut into blocks of 32; entry k of the 3x3
+// matrix of component mu at site s is Cx<R>[((mu * nblk + s / 32) * 9 + k) *
+// 32 + s % 32].  A warp touching 32 consecutive sites reads one fully coalesced
+// 512-byte (FP64) or 256-byte (FP32) segment per matrix entry.  Neighbour
+// links come through L1/L2; the lattice is periodic.
 //
 // Kernels use one thread per link (site, mu) for link-local work and force
 // evaluation, and one thread per site for the site reductions.  Reductions
