@@ -358,6 +358,14 @@ int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double be
  * of multiplicity 6, gets Re tr P / 3 of the plaquettes at each site in the
  * planes (0,1) (0,2) (0,3) (1,2) (1,3) (2,3). */
 int qgb_gf_plaq_field(qgb_field* f_plaq, const qgb_field* gf);
+/* gf_energy_density_dir_field (wilson-flow.cpp:53-95; wilson_flow.pyx:49-63):
+ * per site and plane (planes as in qgb_gf_plaq_field) -Re tr(G G), G the
+ * traceless anti-Hermitian part of the clover; the six sum to
+ * gf_energy_density_field.  fd: FP64 real, multiplicity 6. */
+int qgb_gf_energy_density_dir_field(qgb_field* fd, const qgb_field* gf);
+/* topology_charge_5 (qcd.cpp:376-389): the lattice sum of the 5-loop improved
+ * charge density (same as qgb_gf_topology). */
+int qgb_topology_charge_5(const qgb_field* gf, double* out);
 /* clf_plaq_action_density_field (spatial = 0) / clf_spatial_plaq_action_density_field
  * (spatial = 1) (qcd.cpp:33-62, 391-414; topology.pyx:26-75): per site, sum over
  * the planes (spatial: (0,1) (0,2) (1,2)) of 1 - Re tr C / 3, C the clover

@@ -114,6 +114,7 @@ def lib():
             "or_set_gauge_transform_momentum": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_dot_gauge_momentum": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_gf_plaq_field": (None, [_dbl_p, _dbl_p, _int4]),
+            "or_gf_energy_density_dir_field": (None, [_dbl_p, _dbl_p, _int4]),
             "or_clf_plaq_action_density_field": (None, [_dbl_p, _dbl_p, _int4, ctypes.c_int]),
             "or_set_plaq_flow_z": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_gf_flow_topo_plaq": (ctypes.c_double, [_dbl_p, _int4, ctypes.c_double, ctypes.c_int]),
@@ -362,6 +363,13 @@ def gf_plaq_field(gf, total_site) -> np.ndarray:
     """qcd.cpp:295-341: (V, 6)."""
     f = np.zeros((volume(total_site), 6), dtype=np.float64)
     lib().or_gf_plaq_field(_p(f), _p(gf), _dims(total_site))
+    return f
+
+
+def gf_energy_density_dir_field(gf, total_site) -> np.ndarray:
+    """wilson-flow.cpp:53-95: (V, 6)."""
+    f = np.zeros((volume(total_site), 6), dtype=np.float64)
+    lib().or_gf_energy_density_dir_field(_p(f), _p(gf), _dims(total_site))
     return f
 
 

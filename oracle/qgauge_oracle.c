@@ -1324,6 +1324,22 @@ void or_gf_plaq_field(double* f_plaq, const double* gf, const int dims[4])
   }
 }
 
+/* wilson-flow.cpp:53-95 */
+void or_gf_energy_density_dir_field(double* fd, const double* gf, const int dims[4])
+{
+  const geo_t g = mk_geo(dims);
+#pragma omp parallel for
+  for (long i = 0; i < g.vol; ++i) {
+    int x[4];
+    coor_from_index(&g, i, x);
+    for (int p = 0; p < 6; ++p) {
+      cm c = clover_leaf(gf, &g, x, PLANE_A[p], PLANE_B[p]);
+      cm gmn = make_tr_less_anti_herm(&c);
+      fd[i * 6 + p] = -m_trace2(&gmn, &gmn).re;
+    }
+  }
+}
+
 /* qcd.cpp:33-62 with the clover leaves of qcd.cpp:10-31 */
 void or_clf_plaq_action_density_field(double* paf, const double* gf, const int dims[4], int spatial)
 {

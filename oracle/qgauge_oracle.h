@@ -101,6 +101,8 @@ void or_dot_gauge_momentum(double* f, const double* gm1, const double* gm2, cons
  * instanton_map.py:91-191).  Plaquette fields hold 6 doubles per site, planes
  * (0,1) (0,2) (0,3) (1,2) (1,3) (2,3). */
 void or_gf_plaq_field(double* f_plaq, const double* gf, const int dims[4]);
+/* wilson-flow.cpp:53-95: per site and plane -Re tr(G G), G = TA(clover); 6 per site */
+void or_gf_energy_density_dir_field(double* fd, const double* gf, const int dims[4]);
 void or_clf_plaq_action_density_field(double* paf, const double* gf, const int dims[4], int spatial);
 void or_set_plaq_flow_z(double* z, const double* gf, const double* plaq_factor, const int dims[4]);
 /* one step of a plaquette-weighted flow: kind 1 Shrink, 2 Freeze, 3 Localize,

@@ -29,7 +29,8 @@ from .topo_measure import (gf_energy_derivative_density_field_topo, gf_flow_topo
 from .flow_adjoint import (FlowedWilsonAction, gf_flow_action, gf_flow_action_grad, gf_wilson_flow_vjp,
                            run_flowed_hmc_pure_gauge, set_anti_hermitian_matrix_from_basis,
                            set_basis_from_anti_hermitian_matrix)
-from .wilson_flow import (gf_energy_density, gf_energy_density_field, gf_energy_derivative_density_field,
+from .wilson_flow import (gf_energy_density_dir_field, topology_charge_5,
+                          gf_energy_density, gf_energy_density_field, gf_energy_derivative_density_field,
                           gf_topology, gf_topology_clf, gf_topology_field, gf_topology_field_clf, gf_topology_terms,
                           gf_topology_terms_field, gf_wilson_flow, gf_wilson_flow_force,
                           gf_wilson_flow_step)

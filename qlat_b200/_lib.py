@@ -60,6 +60,8 @@ SIGNATURES = {
     "qgb_field_fill": [c_field, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64],
     "qgb_field_set_selected": [c_field, c_field, ctypes.c_void_p, ctypes.c_int64],
     "qgb_gf_plaq_field": [c_field, c_field],
+    "qgb_gf_energy_density_dir_field": [c_field, c_field],
+    "qgb_topology_charge_5": [c_field, c_dbl_p],
     "qgb_gf_plaq_action_density_field": [c_field, c_field, ctypes.c_int32],
     "qgb_set_plaq_flow_z": [c_field, c_field, c_field],
     "qgb_gf_flow_topo": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, c_dbl_p],

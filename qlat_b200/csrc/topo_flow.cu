@@ -143,6 +143,38 @@ __global__ void __launch_bounds__(TF_BS) k_plaq_flow_z(Geo g, const Cx<R>* Up, c
   WField<R>{Z, g.V}.st(s, mu, traceless_antiherm(scale((R)-1, fz)));
 }
 
+// gf_energy_density_dir_field (wilson-flow.cpp:53-95): per site and plane
+// (a, b) in plane_of order, -Re tr(G G) with G = TA(C), C the clover average
+// of the four plaquettes with a corner at the site, each walked from the site
+// as in gf_clover_leaf_no_comm (qcd.cpp:10-31).
+template <typename R>
+__global__ void __launch_bounds__(TF_BS) k_energy_density_dir(Geo g, const Cx<R>* Up, double* out)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.V) return;
+  const CField<R> U{Up, g.V};
+  const Coord x = coord_of(g, s);
+#pragma unroll 1
+  for (int p = 0; p < 6; ++p) {
+    const int a = p < 3 ? 0 : (p < 5 ? 1 : 2);
+    const int b = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
+    const long xa = site_rt(g, x, a, 1, b, 0), xb = site_rt(g, x, a, 0, b, 1);
+    const long xma = site_rt(g, x, a, -1, b, 0), xmb = site_rt(g, x, a, 0, b, -1);
+    const long xmab = site_rt(g, x, a, -1, b, -1), xmab2 = site_rt(g, x, a, -1, b, 1),
+               xamb = site_rt(g, x, a, 1, b, -1);
+    // (a, b, -a, -b): U_a(x) U_b(x+a) U_a(x+b)^+ U_b(x)^+
+    M3<R> c = mul_adj(mul_adj(mul(U.ld(s, a), U.ld(xa, b)), U.ld(xb, a)), U.ld(s, b));
+    // (-a, -b, a, b): U_a(x-a)^+ U_b(x-a-b)^+ U_a(x-a-b) U_b(x-b)
+    add_to(c, mul(mul(adj_mul(U.ld(xma, a), adj(U.ld(xmab, b))), U.ld(xmab, a)), U.ld(xmb, b)));
+    // (b, -a, -b, a): U_b(x) U_a(x-a+b)^+ U_b(x-a)^+ U_a(x-a)
+    add_to(c, mul(mul_adj(mul_adj(U.ld(s, b), U.ld(xmab2, a)), U.ld(xma, b)), U.ld(xma, a)));
+    // (-b, a, b, -a): U_b(x-b)^+ U_a(x-b) U_b(x-b+a) U_a(x)^+
+    add_to(c, mul_adj(mul(adj_mul(U.ld(xmb, b), U.ld(xmb, a)), U.ld(xamb, b)), U.ld(s, a)));
+    const M3<R> G = traceless_antiherm(scale(R(0.25), c));
+    out[lay_index<1>(g.V, p, 0, s)] = -(double)re_tr_mul(G, G);
+  }
+}
+
 // per-block min and max of each component of a real field (blockDim TF_BS)
 template <typename R>
 __global__ void __launch_bounds__(TF_BS) k_min_max(long V, int mult, const R* f, double* part)
@@ -371,6 +403,26 @@ int qgb_gf_plaq_field(qgb_field* f_plaq, const qgb_field* gf_)
   TF_RC(qgb::library_stream(&st));
   return plaq_field_dev(st, gf, (double*)f.d);
 }
+
+int qgb_gf_energy_density_dir_field(qgb_field* fd, const qgb_field* gf_)
+{
+  const char* what = "qgb_gf_energy_density_dir_field";
+  Meta gf, f;
+  TF_RC(meta_of(gf_, gf, what));
+  TF_RC(meta_of(fd, f, what));
+  TF_RC(check_gauge(gf, what));
+  TF_RC(check_real(f, gf, 6, what));
+  cudaStream_t st;
+  TF_RC(qgb::library_stream(&st));
+  if (gf.prec == QGB_F64)
+    k_energy_density_dir<double><<<blocks_of(gf.g.V), TF_BS, 0, st>>>(gf.g, (const Cx<double>*)gf.d, (double*)f.d);
+  else
+    k_energy_density_dir<float><<<blocks_of(gf.g.V), TF_BS, 0, st>>>(gf.g, (const Cx<float>*)gf.d, (double*)f.d);
+  TF_LAUNCHED();
+  return QGB_OK;
+}
+
+int qgb_topology_charge_5(const qgb_field* gf, double* out) { return qgb_gf_topology(gf, out); }
 
 int qgb_gf_plaq_action_density_field(qgb_field* paf, const qgb_field* gf_, int32_t spatial)
 {

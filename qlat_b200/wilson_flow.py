@@ -62,6 +62,22 @@ def gf_wilson_flow(gf: GaugeField, flow_time: float, steps: int, *, c1: float = 
     return out
 
 
+def gf_energy_density_dir_field(gf: GaugeField) -> FieldRealD:
+    """wilson_flow.pyx:49-63 -> gf_energy_density_dir_field (wilson-flow.cpp:53-95):
+    -Re tr(G G) per plane (0,1) (0,2) (0,3) (1,2) (1,3) (2,3), G = TA(clover);
+    multiplicity 6, summing to gf_energy_density_field."""
+    fd = FieldRealD(gf.geo, 6)
+    call("qgb_gf_energy_density_dir_field", fd.handle, gf.handle)
+    return fd
+
+
+def topology_charge_5(gf: GaugeField) -> float:
+    """topology_charge_5 (qcd.cpp:376-389): the 5-loop improved charge."""
+    o = ctypes.c_double()
+    call("qgb_topology_charge_5", gf.handle, ctypes.byref(o))
+    return o.value
+
+
 def gf_energy_derivative_density_field(gf: GaugeField, *, epsilon: float = 0.0125, c1: float = 0.0,
                                        wilson_flow_integrator_type: str | None = None) -> FieldRealD:
     """wilson_flow.pyx:96-108: central difference of the energy density field."""

@@ -294,3 +294,25 @@ def test_gpu_odd_lattice(q, oracle):
         adv = q.gf_flow_topo(g, 0.1, kind)
         assert abs(adv - o.gf_flow_topo(r, ts, 0.1, kind)) < 1e-13 * adv
         assert np.abs(np.asarray(g) - r).max() < 1e-12, kind
+
+
+def test_oracle_energy_density_dir_sums_to_density(oracle):
+    o = oracle
+    gf = o.new_field(TS)
+    o.gf_set_rand(gf, TS, o.RngState("edir").split("gf-init"), 0.4, 2)
+    d = o.gf_energy_density_dir_field(gf, TS)
+    assert np.abs(d.sum(axis=1) - o.gf_energy_density_field(gf, TS)).max() < 1e-13
+
+
+@pytest.mark.gpu
+def test_gpu_energy_density_dir_and_charge_5(q, oracle):
+    o = oracle
+    for ts in (TS, (3, 4, 5, 6)):
+        gf = q.GaugeField(q.Geometry(ts))
+        gf.set_rand(q.RngState("edir").split("gf-init"), 0.4, 2)
+        ref = o.new_field(ts)
+        o.gf_set_rand(ref, ts, o.RngState("edir").split("gf-init"), 0.4, 2)
+        d = q.gf_energy_density_dir_field(gf).to_numpy()
+        assert np.abs(d - o.gf_energy_density_dir_field(ref, ts)).max() < 1e-13
+        assert np.abs(d.sum(axis=1) - q.gf_energy_density_field(gf).to_numpy()[:, 0]).max() < 1e-13
+        assert q.topology_charge_5(gf) == q.gf_topology(gf)
