@@ -442,6 +442,32 @@ int qgb_field_fill(qgb_field* f, double value, const uint8_t* mask, int64_t n);
  * entries as above; fields of one kind, multiplicity, lattice and precision. */
 int qgb_field_set_selected(qgb_field* dst, const qgb_field* src, const uint8_t* mask, int64_t n);
 
+/* ---- time-slab decomposition (the reference's domain decomposition,
+ * field-expand.h / hmc.cpp:466-490 refresh_expanded, restricted to the time
+ * direction) ------------------------------------------------------------- */
+
+/* A rank holds the slab of T / R time slices it owns plus h halo slices on each
+ * side as an ordinary field of extent T / R + 2 h in direction 3.  The halo
+ * slices are copied from the neighbouring ranks (pack / unpack below, sent by
+ * the caller's communication library); the owned sites are the contiguous
+ * local site range [h X Y Z, (h + T / R) X Y Z). */
+/* Sums over the local sites [s0, s1) only: gm_hamilton_node, the plaquette and
+ * rectangle sums of gf_sum_re_tr_*_node (out[1] = 0 unless rect), and
+ * gf_hamilton_node. */
+int qgb_gm_hamilton_node_sites(const qgb_field* gm, int64_t s0, int64_t s1, double* out);
+int qgb_gf_action_sums_sites(const qgb_field* gf, int32_t rect, int64_t s0, int64_t s1, double out[2]);
+int qgb_gf_hamilton_node_sites(const qgb_field* gf, double beta, double c1, int64_t s0, int64_t s1, double* out);
+/* set_rand_gauge_momentum / set_g_rand_color_matrix_field with the per-site
+ * streams of global site (local site + site_offset). */
+int qgb_set_rand_gauge_momentum_sites(qgb_field* gm, double sigma, const uint32_t rs[24], int64_t site_offset);
+int qgb_gf_set_rand_sites(qgb_field* gf, const uint32_t rs[24], double sigma, int32_t n_step, int64_t site_offset);
+/* Copy the time slices [t0, t0 + nt) of every component of f into a device
+ * buffer of qgb_field_tslice_bytes(f, nt) bytes, or back; X Y Z must be a
+ * multiple of 32.  Asynchronous on the library stream. */
+int qgb_field_tslice_bytes(const qgb_field* f, int32_t nt, int64_t* bytes);
+int qgb_field_pack_tslices(const qgb_field* f, int32_t t0, int32_t nt, void* dev);
+int qgb_field_unpack_tslices(qgb_field* f, int32_t t0, int32_t nt, const void* dev);
+
 /* ---- force-kernel autotuner (no counterpart in the reference) ---------- */
 
 /* The force kernels (set_gm_force and its fused HMC / flow consumers) exist

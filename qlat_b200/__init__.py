@@ -26,6 +26,7 @@ from .hmc_fa import (MomentumAutoCorr, dot_gauge_momentum, gf_evolve_dual, gf_ev
 from .topo_measure import (gf_energy_derivative_density_field_topo, gf_flow_topo, gf_plaq_action_density,
                            gf_plaq_action_density_field, gf_plaq_field, gf_plaq_flow_force,
                            gf_spatial_plaq_action_density, gf_spatial_plaq_action_density_field, smear_measure_topo)
+from .slabs import TimeSlabs, run_hmc_evolve_slabs, run_hmc_pure_gauge_slabs
 from .flow_adjoint import (FlowedWilsonAction, gf_flow_action, gf_flow_action_grad, gf_wilson_flow_vjp,
                            run_flowed_hmc_pure_gauge, set_anti_hermitian_matrix_from_basis,
                            set_basis_from_anti_hermitian_matrix)

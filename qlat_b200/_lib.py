@@ -69,6 +69,15 @@ SIGNATURES = {
     "qgb_field_glb_sum_tslice": [c_field, ctypes.c_int32, c_dbl_p],
     "qgb_field_abs": [c_field],
     "qgb_fp32_fma_rate": [ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+    "qgb_gm_hamilton_node_sites": [c_field, ctypes.c_int64, ctypes.c_int64, c_dbl_p],
+    "qgb_gf_action_sums_sites": [c_field, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, c_dbl_p],
+    "qgb_gf_hamilton_node_sites": [c_field, ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int64,
+                                   c_dbl_p],
+    "qgb_set_rand_gauge_momentum_sites": [c_field, ctypes.c_double, c_u32_p, ctypes.c_int64],
+    "qgb_gf_set_rand_sites": [c_field, c_u32_p, ctypes.c_double, ctypes.c_int32, ctypes.c_int64],
+    "qgb_field_tslice_bytes": [c_field, ctypes.c_int32, c_i64_p],
+    "qgb_field_pack_tslices": [c_field, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p],
+    "qgb_field_unpack_tslices": [c_field, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p],
     "qgb_field_info": [c_field, i32x4, c_i32_p, c_i32_p, c_i32_p],
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],

@@ -969,6 +969,136 @@ int qgb_gf_hamilton_node(const qgb_field* gf, double beta, double c1, double* ou
   return QGB_OK;
 }
 
+// ---- sub-lattices of a time-slab decomposition ----------------------------
+
+int qgb_gm_hamilton_node_sites(const qgb_field* gm, int64_t s0, int64_t s1, double* out)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_gm_hamilton_node_sites"));
+  QGB_CHECK(out && gm->mult == 4 && s0 >= 0 && s0 <= s1 && s1 <= gm->V, QGB_ERR_INVALID_ARG,
+            "qgb_gm_hamilton_node_sites: bad argument");
+  Geo g = geo_of(gm);
+  g.r0 = s0;
+  g.r1 = s1;
+  const int nb = qgb::reduce_blocks(g);
+  QGB_RC(ensure_partials((size_t)nb));
+  if (gm->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_gm_hamilton<double>(g, gm->d, g_ctx.partials, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_gm_hamilton<float>(g, gm->d, g_ctx.partials, g_ctx.stream));
+  QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 0, g_ctx.stream));
+  g_launches += 2;
+  return read_results(0, 1, out);
+}
+
+int qgb_gf_action_sums_sites(const qgb_field* gf, int32_t rect, int64_t s0, int64_t s1, double out[2])
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_action_sums_sites"));
+  QGB_CHECK(out && gf->mult == 4 && s0 >= 0 && s0 <= s1 && s1 <= gf->V, QGB_ERR_INVALID_ARG,
+            "qgb_gf_action_sums_sites: bad argument");
+  Geo g = geo_of(gf);
+  g.r0 = s0;
+  g.r1 = s1;
+  const int nb = qgb::reduce_blocks(g);
+  QGB_RC(ensure_partials((size_t)nb * 2));
+  if (gf->prec == QGB_F64) QGB_TRY_CUDA(qgb::launch_action<double>(g, gf->d, rect, g_ctx.partials, g_ctx.stream));
+  else QGB_TRY_CUDA(qgb::launch_action<float>(g, gf->d, rect, g_ctx.partials, g_ctx.stream));
+  QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, rect ? 2 : 1, nb, g_ctx.results, 0, g_ctx.stream));
+  g_launches += 2;
+  out[1] = 0.0;
+  return read_results(0, rect ? 2 : 1, out);
+}
+
+int qgb_gf_hamilton_node_sites(const qgb_field* gf, double beta, double c1, int64_t s0, int64_t s1, double* out)
+{
+  QGB_CHECK(out, QGB_ERR_INVALID_ARG, "qgb_gf_hamilton_node_sites: null output");
+  double r[2] = {0.0, 0.0};
+  QGB_RC(qgb_gf_action_sums_sites(gf, c1 != 0.0, s0, s1, r));
+  *out = gf_hamilton_from(r[0], r[1], beta, c1);
+  return QGB_OK;
+}
+
+int qgb_set_rand_gauge_momentum_sites(qgb_field* gm, double sigma, const uint32_t rs[24], int64_t site_offset)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_set_rand_gauge_momentum_sites"));
+  QGB_CHECK(gm->mult == 4 && rs, QGB_ERR_INVALID_ARG, "qgb_set_rand_gauge_momentum_sites: bad argument");
+  Geo g = geo_of(gm);
+  g.rng_off = site_offset;
+  Prof p("rng");
+  if (gm->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_rand_momentum<double>(g, gm->d, rs, sigma, g_ctx.ambiguous, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_rand_momentum<float>(g, gm->d, rs, sigma, g_ctx.ambiguous, g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_gf_set_rand_sites(qgb_field* gf, const uint32_t rs[24], double sigma, int32_t n_step, int64_t site_offset)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_set_rand_sites"));
+  QGB_CHECK(gf->mult == 4 && rs, QGB_ERR_INVALID_ARG, "qgb_gf_set_rand_sites: bad argument");
+  Geo g = geo_of(gf);
+  g.rng_off = site_offset;
+  Prof p("rng");
+  if (gf->prec == QGB_F64)
+    QGB_TRY_CUDA(qgb::launch_hot_start<double>(g, gf->d, rs, sigma, n_step, g_ctx.ambiguous, g_ctx.stream));
+  else
+    QGB_TRY_CUDA(qgb::launch_hot_start<float>(g, gf->d, rs, sigma, n_step, g_ctx.ambiguous, g_ctx.stream));
+  return QGB_OK;
+}
+
+// The time slices [t0, t0 + nt) of every component are whole 32-site blocks
+// when X Y Z is a multiple of 32: one contiguous chunk per component.
+static int tslice_chunks(const qgb_field* f, int32_t t0, int32_t nt, size_t* block_bytes, long* b0, long* nb_t)
+{
+  const long spatial = (long)f->dims[0] * f->dims[1] * f->dims[2];
+  QGB_CHECK(spatial % 32 == 0, QGB_ERR_BAD_GEOMETRY, "time slices: X * Y * Z must be a multiple of 32");
+  QGB_CHECK(t0 >= 0 && nt >= 0 && t0 + nt <= f->dims[3], QGB_ERR_INVALID_ARG, "time slices: range outside the field");
+  *block_bytes = (size_t)32 * elem_reals(f) * (f->prec == QGB_F64 ? 8 : 4);
+  *b0 = (long)t0 * spatial / 32;
+  *nb_t = (long)nt * spatial / 32;
+  return QGB_OK;
+}
+
+int qgb_field_tslice_bytes(const qgb_field* f, int32_t nt, int64_t* bytes)
+{
+  QGB_RC(check_field(f, -1, "qgb_field_tslice_bytes"));
+  QGB_CHECK(bytes, QGB_ERR_INVALID_ARG, "qgb_field_tslice_bytes: null output");
+  size_t bb;
+  long b0, nb;
+  QGB_RC(tslice_chunks(f, 0, nt, &bb, &b0, &nb));
+  *bytes = (int64_t)f->mult * nb * (int64_t)bb;
+  return QGB_OK;
+}
+
+static int tslice_copy(qgb_field* f, int32_t t0, int32_t nt, void* buf, bool pack, const char* what)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, what));
+  QGB_CHECK(buf, QGB_ERR_INVALID_ARG, std::string(what) + ": null buffer");
+  size_t bb;
+  long b0, nb;
+  QGB_RC(tslice_chunks(f, t0, nt, &bb, &b0, &nb));
+  const long nblk = qgb::site_blocks(f->V);
+  for (int m = 0; m < f->mult; ++m) {
+    char* field = (char*)f->d + ((size_t)m * nblk + b0) * bb;
+    char* packed = (char*)buf + (size_t)m * nb * bb;
+    if (pack) QGB_TRY_CUDA(cudaMemcpyAsync(packed, field, nb * bb, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    else QGB_TRY_CUDA(cudaMemcpyAsync(field, packed, nb * bb, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  }
+  return QGB_OK;
+}
+
+int qgb_field_pack_tslices(const qgb_field* f, int32_t t0, int32_t nt, void* dev)
+{
+  return tslice_copy(const_cast<qgb_field*>(f), t0, nt, dev, true, "qgb_field_pack_tslices");
+}
+
+int qgb_field_unpack_tslices(qgb_field* f, int32_t t0, int32_t nt, const void* dev)
+{
+  return tslice_copy(f, t0, nt, const_cast<void*>(dev), false, "qgb_field_unpack_tslices");
+}
+
 int qgb_gf_avg_plaq(const qgb_field* gf, double* out)
 {
   QGB_CTX();

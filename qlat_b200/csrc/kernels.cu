@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(RED_BS) k_gm_hamilton(Geo g, const Cx<R>* P, d
 {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
-  if (s < g.V) {
+  if (s < g.V && in_reduce(g, s)) {
     const CField<R> Pf{P, g.V};
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) v[0] += neg_half_tr_square(Pf.ld(s, mu));
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(RED_BS) k_action(Geo g, const Cx<R>* Up, doubl
 {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  if (s < g.V) {
+  if (s < g.V && in_reduce(g, s)) {
     const CField<R> U{Up, g.V};
     const Coord x = coord_of(g, s);
 #pragma unroll 1
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(RED_BS) k_clover(Geo g, const Cx<R>* Up, R* ef
 {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  if (s < g.V) {
+  if (s < g.V && in_reduce(g, s)) {
     const CField<R> U{Up, g.V};
     const Coord x = coord_of(g, s);
     double e = 0.0, q = 0.0;
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(128) k_rand_momentum(Geo g, RngArg ra, double 
   const bool active = s < g.V;
   Rng base, rs;
   rng_import(base, ra.v);
-  if (active) rng_split_long(rs, base, (int64_t)s);
+  if (active) rng_split_long(rs, base, (int64_t)(s + g.rng_off));
   int amb = 0;
   const WField<R> Pf{P, g.V};
   double b[8];
@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(128) k_hot_start(Geo g, RngArg ra, double s_si
   if (s >= g.V) return;
   Rng base, rs;
   rng_import(base, ra.v);
-  rng_split_long(rs, base, (int64_t)s);
+  rng_split_long(rs, base, (int64_t)(s + g.rng_off));
   int amb = 0;
   const WField<R> Uf{U, g.V};
   for (int mu = 0; mu < 4; ++mu) {

@@ -16,7 +16,14 @@ struct Geo {
   int d[4];      // X, Y, Z, T
   long V;        // sites of this lattice
   long off = 0;  // index of its first site in a field holding several lattices
+  // a sub-lattice of a larger one (time-slab decomposition): the site
+  // reductions sum over the sites [r0, r1) only (r1 < 0: all), and the
+  // per-site random streams of site s are those of global site s + rng_off
+  long r0 = 0, r1 = -1;
+  long rng_off = 0;
 };
+
+__host__ __device__ inline bool in_reduce(const Geo& g, long s) { return s >= g.r0 && (g.r1 < 0 || s < g.r1); }
 
 // One chain of a batch: its lattice, offset in the concatenated field and action.
 struct ChainInfo {

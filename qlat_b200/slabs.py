@@ -1,0 +1,215 @@
+"""Time-slab domain decomposition of pure-gauge HMC over ranks.
+
+The reference runs its fields on MPI ranks with halo ("expanded") copies of
+the neighbouring ranks' sites, refreshed before each force evaluation
+(refresh_expanded, field-expand.h; hmc.cpp:466-490), and sums the Hamiltonians
+over ranks (glb_sum).  Here the lattice is cut along the time direction: with R
+ranks each rank owns T / R time slices and holds them with ``halo`` slices of
+its two neighbours on either side, as one ordinary GPU field of time extent
+T / R + 2 halo.  The library's kernels run unchanged on that field; the owned
+sites are correct as long as the halo slices are fresh copies:
+
+- the Iwasaki force reaches two slices, so a force-gradient momentum update
+  (the force at U, the shifted U' = exp(eps F) U, the force at U') is right on
+  the owned slices when the halo is 4 slices deep and was refreshed just before
+  it: one exchange per update;
+- the link updates are site-local and need no exchange;
+- the Hamiltonians sum over the owned sites only and are then summed over
+  ranks in FP64;
+- momenta and hot starts use the per-site random streams of the global site
+  index, so every owned site draws exactly what a single-GPU run draws.
+
+The halo exchange packs the boundary slices of every component into one
+contiguous buffer (qgb_field_pack_tslices) and sends it with torch.distributed
+point-to-point operations: over NCCL from device buffers, over gloo through
+host memory.  Communication is plumbing; all arithmetic stays in the
+library's kernels.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+from ._lib import call
+from .field import GaugeAction, GaugeField, GaugeMomentum, Geometry, RngState
+from .hmc import gf_evolve, gm_evolve_fg_pure_gauge, metropolis_accept, unitarize
+
+
+class TimeSlabs:
+    """The local slab of a lattice cut into ``world`` time slabs (rank ``rank``).
+
+    ``geo`` is the geometry of the local field (time extent nt + 2 halo);
+    ``owned`` the local site range [s0, s1) of the owned slices;
+    ``site_offset`` the global index of local site 0 (the owned site s is
+    global site s + site_offset)."""
+
+    def __init__(self, total_site, *, halo: int = 4, group=None):
+        import torch.distributed as dist
+        self._dist = dist if dist.is_available() and dist.is_initialized() else None
+        self.group = group
+        self.world = self._dist.get_world_size(group) if self._dist else 1
+        self.rank = self._dist.get_rank(group) if self._dist else 0
+        X, Y, Z, T = (int(v) for v in total_site)
+        if T % self.world:
+            raise ValueError(f"TimeSlabs: T = {T} is not divisible by {self.world} ranks")
+        self.nt = T // self.world
+        if self.nt < halo:
+            raise ValueError(f"TimeSlabs: {self.nt} owned slices per rank, fewer than the halo depth {halo}")
+        self.spatial = X * Y * Z
+        if self.spatial % 32:
+            raise ValueError("TimeSlabs: X * Y * Z must be a multiple of 32")
+        self.halo = halo
+        self.total_site = (X, Y, Z, T)
+        self.total_volume = X * Y * Z * T
+        self.geo = Geometry((X, Y, Z, self.nt + 2 * halo))
+        self.t0 = self.rank * self.nt
+        self.owned = (halo * self.spatial, (halo + self.nt) * self.spatial)
+        self.site_offset = (self.t0 - halo) * self.spatial
+        self.backend = self._dist.get_backend(group) if self._dist else None
+        self._bufs = {}
+
+    # ---- communication ----------------------------------------------------------------
+
+    def _buffer(self, key, nbytes, device):
+        import torch
+        b = self._bufs.get((key, nbytes, device))
+        if b is None:
+            b = torch.empty(nbytes, dtype=torch.uint8, device=device)
+            self._bufs[(key, nbytes, device)] = b
+        return b
+
+    def exchange(self, f) -> None:
+        """Refresh the halo slices of f from the neighbouring ranks (the ring
+        of time slabs is periodic)."""
+        import torch
+        from . import synchronize
+        h, nt = self.halo, self.nt
+        n = ctypes.c_int64()
+        call("qgb_field_tslice_bytes", f.handle, h, ctypes.byref(n))
+        nbytes = n.value
+        up_dev = self._buffer("send_up", nbytes, "cuda")
+        dn_dev = self._buffer("send_dn", nbytes, "cuda")
+        call("qgb_field_pack_tslices", f.handle, nt, h, ctypes.c_void_p(up_dev.data_ptr()))  # top owned slices
+        call("qgb_field_pack_tslices", f.handle, h, h, ctypes.c_void_p(dn_dev.data_ptr()))   # bottom owned slices
+        synchronize()
+        if self.world == 1:
+            rbot, rtop = up_dev, dn_dev
+        else:
+            on_host = self.backend != "nccl"
+            rbot, rtop = self._swap(up_dev.cpu() if on_host else up_dev, dn_dev.cpu() if on_host else dn_dev)
+            if on_host:
+                rbot = rbot.to("cuda")
+                rtop = rtop.to("cuda")
+            torch.cuda.current_stream().synchronize()
+        call("qgb_field_unpack_tslices", f.handle, 0, h, ctypes.c_void_p(rbot.data_ptr()))
+        call("qgb_field_unpack_tslices", f.handle, nt + h, h, ctypes.c_void_p(rtop.data_ptr()))
+        synchronize()
+
+    def _swap(self, send_up, send_dn):
+        """Send this rank's packed top slices up the ring and its bottom slices
+        down; returns what arrives for the bottom halo (the lower neighbour's
+        top slices) and for the top halo (the upper neighbour's bottom slices)."""
+        dist = self._dist
+        rbot = self._buffer("recv_bot", send_up.numel(), send_up.device.type)
+        rtop = self._buffer("recv_top", send_dn.numel(), send_dn.device.type)
+        up, dn = (self.rank + 1) % self.world, (self.rank - 1) % self.world
+        # posted in the same order on every rank: NCCL pairs the operations
+        # between two ranks in order, gloo by tag
+        ops = [dist.P2POp(dist.isend, send_up, up, self.group, 0),
+               dist.P2POp(dist.isend, send_dn, dn, self.group, 1),
+               dist.P2POp(dist.irecv, rbot, dn, self.group, 0),
+               dist.P2POp(dist.irecv, rtop, up, self.group, 1)]
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+        return rbot, rtop
+
+    def glb_sum(self, x: float) -> float:
+        """glb_sum (mpi.h:273-308): FP64 sum over the ranks."""
+        if self.world == 1:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
+        self._dist.all_reduce(t, group=self.group)
+        return float(t.item())
+
+    # ---- fields on the slab -------------------------------------------------------------
+
+    def gauge_field(self) -> GaugeField:
+        return GaugeField(self.geo)
+
+    def gauge_momentum(self) -> GaugeMomentum:
+        return GaugeMomentum(self.geo)
+
+    def set_rand(self, gf: GaugeField, rng: RngState, sigma: float = 0.5, n_step: int = 1) -> None:
+        """GaugeField.set_rand on the slab: the owned sites get the links a
+        single-GPU field of the whole lattice gets; then the halo is filled."""
+        call("qgb_gf_set_rand_sites", gf.handle, rng.c, float(sigma), int(n_step), self.site_offset)
+        self.exchange(gf)
+
+    def set_rand_momentum(self, gm: GaugeMomentum, rng: RngState, sigma: float = 1.0) -> None:
+        call("qgb_set_rand_gauge_momentum_sites", gm.handle, float(sigma), rng.c, self.site_offset)
+
+    def gm_hamilton(self, gm: GaugeMomentum) -> float:
+        o = ctypes.c_double()
+        call("qgb_gm_hamilton_node_sites", gm.handle, self.owned[0], self.owned[1], ctypes.byref(o))
+        return self.glb_sum(o.value)
+
+    def gf_hamilton(self, gf: GaugeField, ga: GaugeAction) -> float:
+        """The gauge action over the whole lattice; the halo must be fresh."""
+        o = ctypes.c_double()
+        call("qgb_gf_hamilton_node_sites", gf.handle, ga.beta(), ga.c1(), self.owned[0], self.owned[1],
+             ctypes.byref(o))
+        return self.glb_sum(o.value)
+
+    def plaq(self, gf: GaugeField) -> float:
+        """gf_avg_plaq over the whole lattice; the halo must be fresh."""
+        out = (ctypes.c_double * 2)()
+        call("qgb_gf_action_sums_sites", gf.handle, 0, self.owned[0], self.owned[1], out)
+        return 1.0 + self.glb_sum(out[0]) / (18.0 * self.total_volume)
+
+    def owned_slices(self, a):
+        """The owned part of a local field's numpy image (sites, ...)."""
+        return a[self.owned[0]:self.owned[1]]
+
+
+# ---- HMC on the slabs (hmc.pyx:157-216) ----------------------------------------------------
+
+
+def run_hmc_evolve_slabs(slabs: TimeSlabs, gm: GaugeMomentum, gf: GaugeField, ga: GaugeAction, n_step: int,
+                         md_time: float = 1.0) -> float:
+    """run_hmc_evolve_pure_gauge (hmc.pyx:169-188) on time slabs: the same
+    Omelyan force-gradient steps, a halo exchange before each momentum update
+    and before the closing Hamiltonian; returns the global delta_h."""
+    slabs.exchange(gf)
+    energy = slabs.gm_hamilton(gm) + slabs.gf_hamilton(gf, ga)
+    dt = md_time / n_step
+    lam = 0.5 * (1.0 - 1.0 / math.sqrt(3.0))
+    theta = (2.0 - math.sqrt(3.0)) / 48.0
+    ttheta = theta * dt * dt * dt
+    gf_evolve(gf, gm, lam * dt)
+    for i in range(n_step):
+        slabs.exchange(gf)
+        gm_evolve_fg_pure_gauge(gm, gf, ga, 4.0 * ttheta / dt, 0.5 * dt)
+        gf_evolve(gf, gm, (1.0 - 2.0 * lam) * dt)
+        slabs.exchange(gf)
+        gm_evolve_fg_pure_gauge(gm, gf, ga, 4.0 * ttheta / dt, 0.5 * dt)
+        gf_evolve(gf, gm, (2.0 if i < n_step - 1 else 1.0) * lam * dt)
+    unitarize(gf)
+    slabs.exchange(gf)
+    return slabs.gm_hamilton(gm) + slabs.gf_hamilton(gf, ga) - energy
+
+
+def run_hmc_pure_gauge_slabs(slabs: TimeSlabs, gf: GaugeField, ga: GaugeAction, traj: int, rs: RngState, *,
+                             n_step: int = 6, md_time: float = 1.0, is_always_accept: bool = False):
+    """run_hmc_pure_gauge (hmc.pyx:190-216) on time slabs; every rank takes the
+    same Metropolis decision from the global delta_h.  Returns (flag, delta_h)."""
+    rs = rs.split(f"{traj}")
+    gf0 = gf.copy()
+    gm = slabs.gauge_momentum()
+    slabs.set_rand_momentum(gm, rs.split("set_rand_gauge_momentum"), 1.0)
+    delta_h = run_hmc_evolve_slabs(slabs, gm, gf0, ga, n_step, md_time)
+    flag, _ = metropolis_accept(delta_h, traj, rs.split("metropolis_accept"))
+    if flag or is_always_accept:
+        gf @= gf0
+    return flag, delta_h

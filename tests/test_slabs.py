@@ -1,0 +1,150 @@
+"""Time-slab decomposition of pure-gauge HMC (qlat_b200.slabs).
+
+CPU: the slab geometry and its checks; the halo message pattern of the ring
+on 2 and 3 gloo ranks (the library's own _swap, with CPU buffers).
+GPU: a one-rank slab (its halo is its own periodic copy) and two ranks run as
+two processes on one GPU, exchanging halos through host memory over gloo (no
+kernel waits on another rank), both against the single-GPU trajectory of the
+whole lattice: the same links on every owned site, the same delta_h and the
+same accept / reject decisions.
+"""
+
+import json
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TS = (4, 4, 4, 16)
+BETA, C1 = 2.13, -0.331
+N_TRAJ, N_STEP = 3, 4
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_slab_geometry():
+    sys.path.insert(0, ROOT)
+    from qlat_b200.slabs import TimeSlabs
+    s = TimeSlabs(TS)
+    assert s.world == 1 and s.nt == 16 and tuple(s.geo.total_site) == (4, 4, 4, 24)
+    assert s.owned == (4 * 64, 20 * 64) and s.site_offset == -4 * 64
+    with pytest.raises(ValueError):
+        TimeSlabs((4, 4, 4, 2))  # fewer owned slices than the halo
+    with pytest.raises(ValueError):
+        TimeSlabs((3, 4, 5, 8))  # X Y Z not a multiple of 32
+
+
+def _swap_main(rank, world, port, out_dir):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from qlat_b200.slabs import TimeSlabs
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        s = TimeSlabs((4, 4, 4, 12))
+        up = torch.full((64,), 10 * rank + 1, dtype=torch.uint8)
+        dn = torch.full((64,), 10 * rank + 2, dtype=torch.uint8)
+        rbot, rtop = s._swap(up, dn)
+        with open(os.path.join(out_dir, f"swap{rank}.json"), "w") as f:
+            json.dump({"t0": s.t0, "bot": rbot.unique().tolist(), "top": rtop.unique().tolist()}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_halo_ring_on_gloo_ranks(tmp_path, world):
+    import torch.multiprocessing as mp
+    mp.start_processes(_swap_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for r in range(world):
+        g = json.load(open(tmp_path / f"swap{r}.json"))
+        assert g["t0"] == r * (12 // world)
+        assert g["bot"] == [10 * ((r - 1) % world) + 1]  # the lower neighbour's top slices
+        assert g["top"] == [10 * ((r + 1) % world) + 2]  # the upper neighbour's bottom slices
+
+
+# ---- GPU ------------------------------------------------------------------------------------
+
+
+def _global_run(q):
+    """The single-GPU reference: hot start and N_TRAJ trajectories of the whole lattice."""
+    ga = q.GaugeAction(BETA, C1)
+    rs = q.RngState("slabs")
+    gf = q.GaugeField(q.Geometry(TS))
+    gf.set_rand(rs.split("gf-init"), 0.3, 1)
+    rows = []
+    for traj in range(1, N_TRAJ + 1):
+        flag, dh = q.run_hmc_pure_gauge(gf, ga, traj, rs.split("hmc"), n_step=N_STEP, is_always_accept=traj < 2)
+        rows.append([bool(flag), dh, q.gf_avg_plaq(gf)])
+    return rows, np.asarray(gf)
+
+
+def _slab_run(q, slabs):
+    ga = q.GaugeAction(BETA, C1)
+    rs = q.RngState("slabs")
+    gf = slabs.gauge_field()
+    slabs.set_rand(gf, rs.split("gf-init"), 0.3, 1)
+    rows = []
+    for traj in range(1, N_TRAJ + 1):
+        flag, dh = q.run_hmc_pure_gauge_slabs(slabs, gf, ga, traj, rs.split("hmc"), n_step=N_STEP,
+                                              is_always_accept=traj < 2)
+        slabs.exchange(gf)
+        rows.append([bool(flag), dh, slabs.plaq(gf)])
+    return rows, slabs.owned_slices(np.asarray(gf))
+
+
+def _compare(rows, ref_rows, links, ref_links, t0, nt):
+    V3 = TS[0] * TS[1] * TS[2]
+    for (f, dh, p), (rf, rdh, rp) in zip(rows, ref_rows):
+        assert f == rf
+        assert abs(dh - rdh) < 1e-9, (dh, rdh)
+        assert abs(p - rp) < 1e-12, (p, rp)
+    assert np.abs(links - ref_links[t0 * V3:(t0 + nt) * V3]).max() < 1e-12
+
+
+@pytest.mark.gpu
+def test_one_rank_slab_matches_global(q):
+    slabs = q.TimeSlabs(TS)
+    rows, links = _slab_run(q, slabs)
+    ref_rows, ref_links = _global_run(q)
+    _compare(rows, ref_rows, links, ref_links, 0, TS[3])
+
+
+def _slab_main(rank, world, port, out_dir):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    torch.cuda.set_device(0)  # both ranks share the one GPU; halos go through host memory
+    import qlat_b200 as q
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        slabs = q.TimeSlabs(TS)
+        rows, links = _slab_run(q, slabs)
+        np.save(os.path.join(out_dir, f"links{rank}.npy"), links)
+        with open(os.path.join(out_dir, f"rows{rank}.json"), "w") as f:
+            json.dump({"t0": slabs.t0, "nt": slabs.nt, "rows": rows}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_two_rank_slabs_match_global(q, tmp_path):
+    import torch.multiprocessing as mp
+    mp.start_processes(_slab_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    ref_rows, ref_links = _global_run(q)
+    for r in range(2):
+        g = json.load(open(tmp_path / f"rows{r}.json"))
+        _compare(g["rows"], ref_rows, np.load(tmp_path / f"links{r}.npy"), ref_links, g["t0"], g["nt"])
