@@ -1,7 +1,9 @@
 """Time-slab decomposition of pure-gauge HMC (qlat_b200.slabs).
 
 CPU: the slab geometry and its checks; the halo message pattern of the ring
-on 2 and 3 gloo ranks (the library's own _swap, with CPU buffers).
+on 2 and 3 gloo ranks (the library's own _swap, with CPU buffers); a rank that
+leaves between steps makes the other rank's exchange fail with an error
+instead of waiting for ever.
 GPU: a one-rank slab (its halo is its own periodic copy) and two ranks run as
 two processes on one GPU, exchanging halos through host memory over gloo (no
 kernel waits on another rank), both against the single-GPU trajectory of the
@@ -148,3 +150,37 @@ def test_two_rank_slabs_match_global(q, tmp_path):
     for r in range(2):
         g = json.load(open(tmp_path / f"rows{r}.json"))
         _compare(g["rows"], ref_rows, np.load(tmp_path / f"links{r}.npy"), ref_links, g["t0"], g["nt"])
+
+
+def _leaving_rank_main(rank, world, port, out_dir):
+    """Rank 1 leaves right after joining; rank 0's halo exchange must end with
+    an error (not wait forever) within the process group's timeout."""
+    import datetime
+    import time
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from qlat_b200.slabs import TimeSlabs
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    s = TimeSlabs((4, 4, 4, 12))
+    if rank == 1:
+        return  # leaves between steps, with nothing in flight
+    t = time.time()
+    err = None
+    try:
+        s._swap(torch.zeros(64, dtype=torch.uint8), torch.zeros(64, dtype=torch.uint8))
+    except Exception as e:  # the peer is gone
+        err = type(e).__name__
+    with open(os.path.join(out_dir, "leave.json"), "w") as f:
+        json.dump({"error": err, "seconds": time.time() - t}, f)
+
+
+def test_leaving_rank_is_reported(tmp_path):
+    import torch.multiprocessing as mp
+    mp.start_processes(_leaving_rank_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    g = json.load(open(tmp_path / "leave.json"))
+    assert g["error"] is not None
+    assert g["seconds"] < 60
