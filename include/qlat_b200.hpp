@@ -18,6 +18,7 @@
 
 #include <stdint.h>
 
+#include <cstdio>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -299,6 +300,219 @@ inline long load_gauge_field(GaugeField& gf, const std::string& path)
   int64_t n = 0;
   check(qgb_load_gauge_field(gf.handle(), path.c_str(), &checks, &n));
   return (long)n;
+}
+
+/* ---- field-accelerated HMC (hmc.h:20-80): per-link masses, dual momenta --- */
+
+inline void set_rand_gauge_momentum(GaugeMomentum& gm, const FieldRealD& mf, const RngState& rs)
+{
+  if (!gm.initialized()) gm.init(mf.geo());
+  check(qgb_set_rand_gauge_momentum_fa(gm.handle(), mf.handle(), rs.v));
+}
+inline double gm_hamilton_node(const GaugeMomentum& gm, const FieldRealD& mf)
+{
+  double r;
+  check(qgb_gm_hamilton_node_fa(gm.handle(), mf.handle(), &r));
+  return r;
+}
+inline void gf_evolve(GaugeField& gf, const GaugeMomentum& gm, const FieldRealD& mf, double step_size)
+{
+  check(qgb_gf_evolve_fa(gf.handle(), gm.handle(), mf.handle(), step_size));
+}
+inline void gf_evolve_dual(GaugeField& gf, const GaugeMomentum& gm_dual, double step_size)
+{
+  check(qgb_gf_evolve_dual(gf.handle(), gm_dual.handle(), step_size));
+}
+inline void gf_evolve_dual(GaugeField& gf, const GaugeMomentum& gm_dual, const FieldRealD& mf_dual, double step_size)
+{
+  check(qgb_gf_evolve_fa_dual(gf.handle(), gm_dual.handle(), mf_dual.handle(), step_size));
+}
+inline void set_gm_force_dual(GaugeMomentum& gm_force_dual, const GaugeField& gf, const GaugeMomentum& gm_force)
+{
+  if (!gm_force_dual.initialized()) gm_force_dual.init(gf.geo());
+  check(qgb_set_gm_force_dual(gm_force_dual.handle(), gf.handle(), gm_force.handle()));
+}
+inline double project_gauge_transform(GaugeMomentum& gm, GaugeMomentum& gm_dual, const FieldRealD& mf,
+                                      const FieldRealD& mf_dual)
+{
+  double r;
+  check(qgb_project_gauge_transform(gm.handle(), gm_dual.handle(), mf.handle(), mf_dual.handle(), &r));
+  return r;
+}
+inline void set_gauge_transform_momentum(GaugeMomentum& gm, GaugeMomentum& gm_dual, const FieldColorMatrix& gtm)
+{
+  if (!gm.initialized()) gm.init(gtm.geo());
+  if (!gm_dual.initialized()) gm_dual.init(gtm.geo());
+  check(qgb_set_gauge_transform_momentum(gm.handle(), gm_dual.handle(), gtm.handle()));
+}
+inline void dot_gauge_momentum(FieldRealD& f, const GaugeMomentum& gm1, const GaugeMomentum& gm2)
+{
+  f.init(gm1.geo(), 4);
+  check(qgb_dot_gauge_momentum(f.handle(), gm1.handle(), gm2.handle()));
+}
+/* set_u_rand / set_g_rand of a real field (core.h:1585-1636) */
+inline void set_u_rand(FieldRealD& f, const RngState& rs, double upper = 1.0, double lower = -1.0)
+{
+  check(qgb_field_set_u_rand(f.handle(), rs.v, upper, lower));
+}
+inline void set_g_rand(FieldRealD& f, const RngState& rs, double center = 0.0, double sigma = 1.0)
+{
+  check(qgb_field_set_g_rand(f.handle(), rs.v, center, sigma));
+}
+
+/* ---- fields of the flow and the topology (qcd.h, wilson-flow.h, qcd-topology.h) */
+
+inline void gf_plaq_field(FieldRealD& f_plaq, const GaugeField& gf)
+{
+  f_plaq.init(gf.geo(), 6);
+  check(qgb_gf_plaq_field(f_plaq.handle(), gf.handle()));
+}
+inline void gf_energy_density_field(FieldRealD& fd, const GaugeField& gf)
+{
+  fd.init(gf.geo(), 1);
+  check(qgb_gf_energy_density_field(fd.handle(), gf.handle()));
+}
+inline void gf_energy_density_dir_field(FieldRealD& fd, const GaugeField& gf)
+{
+  fd.init(gf.geo(), 6);
+  check(qgb_gf_energy_density_dir_field(fd.handle(), gf.handle()));
+}
+inline void set_wilson_flow_z(GaugeMomentum& z, const GaugeField& gf, double c1)
+{
+  if (!z.initialized()) z.init(gf.geo());
+  check(qgb_set_wilson_flow_z(z.handle(), gf.handle(), c1));
+}
+inline void set_plaq_flow_z(GaugeMomentum& z, const GaugeField& gf, const FieldRealD& plaq_factor)
+{
+  if (!z.initialized()) z.init(gf.geo());
+  check(qgb_set_plaq_flow_z(z.handle(), gf.handle(), plaq_factor.handle()));
+}
+inline void gf_wilson_flow_step_euler(GaugeField& gf, double epsilon, double c1 = 0.0)
+{
+  check(qgb_gf_wilson_flow_step_euler(gf.handle(), epsilon, c1));
+}
+inline void clf_plaq_action_density_field(FieldRealD& paf, const GaugeField& gf)
+{
+  paf.init(gf.geo(), 1);
+  check(qgb_gf_plaq_action_density_field(paf.handle(), gf.handle(), 0));
+}
+inline void clf_spatial_plaq_action_density_field(FieldRealD& paf, const GaugeField& gf)
+{
+  paf.init(gf.geo(), 1);
+  check(qgb_gf_plaq_action_density_field(paf.handle(), gf.handle(), 1));
+}
+inline void clf_topology_field(FieldRealD& topf, const GaugeField& gf)
+{
+  topf.init(gf.geo(), 1);
+  check(qgb_clf_topology_field(topf.handle(), gf.handle()));
+}
+inline void clf_topology_field_5(FieldRealD& topf, const GaugeField& gf)
+{
+  topf.init(gf.geo(), 1);
+  check(qgb_clf_topology_field_5(topf.handle(), gf.handle()));
+}
+inline double topology_charge_5(const GaugeField& gf)
+{
+  double r;
+  check(qgb_topology_charge_5(gf.handle(), &r));
+  return r;
+}
+
+/* ---- flowed HMC with masked invertible flows (flowed-hmc.h) ----------------- */
+
+/* FlowStepInfo (flowed-hmc.h:26-41) */
+struct FlowStepInfo {
+  int mask = 0, mu = 0;
+  double epsilon = 0.0;
+  int flow_size = 1;
+};
+/* FlowInfo (flowed-hmc.h:43-46) */
+struct FlowInfo {
+  std::vector<FlowStepInfo> v;
+};
+
+inline std::vector<qgb_flow_step> flow_steps(const FlowInfo& fi)
+{
+  std::vector<qgb_flow_step> s(fi.v.size());
+  for (size_t i = 0; i < s.size(); ++i) {
+    s[i].mask = fi.v[i].mask;
+    s[i].mu = fi.v[i].mu;
+    s[i].epsilon = fi.v[i].epsilon;
+    s[i].flow_size = fi.v[i].flow_size;
+  }
+  return s;
+}
+
+/* show(FlowInfo) (flowed-hmc.h:48-62): one line per step */
+inline std::string show(const FlowInfo& fi)
+{
+  std::string out;
+  char buf[128];
+  for (size_t i = 0; i < fi.v.size(); ++i) {
+    const FlowStepInfo& f = fi.v[i];
+    std::snprintf(buf, sizeof(buf), "flow step %d: mask=%d mu=%d epsilon=%.17g flow_size=%d\n", (int)i, f.mask,
+                  f.mu, f.epsilon, f.flow_size);
+    out += buf;
+  }
+  return out;
+}
+
+/* mk_flow_info_step(rs, epsilon) and (rs, epsilon, epsilon2) (flowed-hmc.cpp:21-69) */
+inline FlowInfo mk_flow_info_step(const RngState& rs, double epsilon)
+{
+  qgb_flow_step s[16];
+  int32_t n = 0;
+  check(qgb_flow_info_step(rs.v, epsilon, 0.0, 0, s, &n));
+  FlowInfo fi;
+  for (int i = 0; i < n; ++i) fi.v.push_back(FlowStepInfo{s[i].mask, s[i].mu, s[i].epsilon, s[i].flow_size});
+  return fi;
+}
+inline FlowInfo mk_flow_info_step(const RngState& rs, double epsilon, double epsilon2)
+{
+  qgb_flow_step s[16];
+  int32_t n = 0;
+  check(qgb_flow_info_step(rs.v, epsilon, epsilon2, 1, s, &n));
+  FlowInfo fi;
+  for (int i = 0; i < n; ++i) fi.v.push_back(FlowStepInfo{s[i].mask, s[i].mu, s[i].epsilon, s[i].flow_size});
+  return fi;
+}
+
+/* vector_append (qlat-utils vector.h) */
+template <class T>
+inline void vector_append(std::vector<T>& v, const std::vector<T>& w)
+{
+  v.insert(v.end(), w.begin(), w.end());
+}
+
+/* gf_flow / gf_flow_inv (flowed-hmc.cpp:540-594) */
+inline void gf_flow(GaugeField& gf, const GaugeField& gf0, const FlowInfo& fi)
+{
+  if (!gf.initialized()) gf.init(gf0.geo());
+  const std::vector<qgb_flow_step> s = flow_steps(fi);
+  check(qgb_gf_flow(gf.handle(), gf0.handle(), s.data(), (int32_t)s.size()));
+}
+inline void gf_flow_inv(GaugeField& gf, const GaugeField& gf1, const FlowInfo& fi)
+{
+  if (!gf.initialized()) gf.init(gf1.geo());
+  const std::vector<qgb_flow_step> s = flow_steps(fi);
+  check(qgb_gf_flow_inv(gf.handle(), gf1.handle(), s.data(), (int32_t)s.size()));
+}
+/* gf_hamilton_flowed_node (flowed-hmc.cpp:1301-1321): the action of the flowed
+ * field minus the log-determinant of the flow */
+inline double gf_hamilton_flowed_node(const GaugeField& gf0, const GaugeAction& ga, const FlowInfo& fi)
+{
+  const std::vector<qgb_flow_step> s = flow_steps(fi);
+  double act = 0.0, ln_det = 0.0;
+  check(qgb_gf_hamilton_flowed_node(gf0.handle(), ga.beta, ga.c1, s.data(), (int32_t)s.size(), &act, &ln_det));
+  return act - ln_det;
+}
+/* set_gm_force_flowed (flowed-hmc.cpp:1500-1509) */
+inline void set_gm_force_flowed(GaugeMomentum& gm_force, const GaugeField& gf0, const GaugeAction& ga,
+                                const FlowInfo& fi)
+{
+  if (!gm_force.initialized()) gm_force.init(gf0.geo());
+  const std::vector<qgb_flow_step> s = flow_steps(fi);
+  check(qgb_set_gm_force_flowed(gm_force.handle(), gf0.handle(), ga.beta, ga.c1, s.data(), (int32_t)s.size(), 1));
 }
 
 }  // namespace qlat_b200
