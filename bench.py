@@ -37,6 +37,25 @@ SEED = "b200-c2-24x64-iwasaki"
 METRIC = "24^3x64 Iwasaki HMC traj/s (force-gradient, 8 steps/traj; mixed FP32/FP64)"
 
 
+def workload_config(lattice, world):
+    """The `config` of the bench line, the same for both arms."""
+    V = 1
+    for v in lattice:
+        V *= v
+    return {"workload": f"{'x'.join(map(str, lattice))} Iwasaki beta=2.13 c1=-0.331, force-gradient "
+                        f"n_step=8 md_time=1, one chain per GPU", "lattice": list(lattice), "sites": V,
+            "l2_policy": f"inputs larger than L2 (FP64 links {V * 576 / 1e6:.1f} MB, FP32 "
+                         f"{V * 288 / 1e6:.1f} MB per chain; L2 126 MB)",
+            "parallelism": f"replicas x{world}"}
+
+
+def metric_for(lattice):
+    """The metric's name for a lattice (the default lattice gives METRIC)."""
+    X, Y, Z, T = lattice
+    head = f"{X}^3x{T}" if X == Y == Z else f"{X}x{Y}x{Z}x{T}"
+    return METRIC.replace("24^3x64", head, 1)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -90,11 +109,10 @@ def reference_arm(args):
     sample = (f"{r['samples']} x (set_gm_force + gf_evolve) on {'x'.join(map(str, lattice))} + one set of "
               f"trajectory ends (momentum refresh, 2 x H, unitarize); traj time = 32 pairs + ends")
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": 0,
+        "impl": "reference", "metric": metric_for(lattice), "value": value, "unit": "traj/s", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": traj_s * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded hot start set_rand(sigma=0.3)",
-        "config": {"workload": f"{'x'.join(map(str, lattice))} Iwasaki beta=2.13 FG n_step=8 (reference CPU, FP64)",
-                   "lattice": list(lattice), "sites": r["sites"]},
+        "config": workload_config(lattice, 1),
         "cpu_baseline": {"value": value, "unit": "traj/s", "cores": r["threads"], "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -349,14 +367,11 @@ def our_arm(args):
         except Exception:
             traffic = None
     out = {
-        "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_for(lattice), "value": value, "unit": "traj/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (MD) + f64 (H, unitarize)",
         "data": "synthetic: seeded hot start set_rand(RngState('b200-c2-24x64-iwasaki').split('gf-init'), 0.3)",
-        "config": {"workload": f"{'x'.join(map(str, lattice))} Iwasaki beta=2.13 c1=-0.331, force-gradient "
-                               f"n_step=8 md_time=1, one chain per GPU", "lattice": list(lattice), "sites": V,
-                   "l2_policy": "inputs larger than L2 (FP64 links 509.6 MB, FP32 254.8 MB per chain)",
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(lattice, world),
         "fp64_traj_per_s": fp64_value, "mixed_over_fp64": value / fp64_value,
         "link_updates_per_s": value * 4 * V * N_STEP,
         "delta_h": {"mixed_mean": statistics.fmean(dh_mixed), "fp64_mean": statistics.fmean(dh_fp64),
