@@ -342,6 +342,11 @@ int qgb_gf_hamilton_flowed_node(const qgb_field* gf0, double beta, double c1, co
  * set_gm_force_flowed_no_det of set_gm_force of the flowed field). */
 int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double beta, double c1,
                             const qgb_flow_step* steps, int32_t n, int32_t with_det);
+/* set_gm_force_flowed_no_det (flowed-hmc.cpp:1511-1520): gm_force_pre, a force
+ * on the flowed field, propagated back through the steps to gf0 without the
+ * determinant term. */
+int qgb_set_gm_force_flowed_no_det(qgb_field* gm_force, const qgb_field* gm_force_pre, const qgb_field* gf0,
+                                   const qgb_flow_step* steps, int32_t n);
 
 /* ---- topology measurement: flows and site fields (instanton_map.py,
  * qcd.cpp:33-62, 295-341, 391-414, wilson-flow.cpp:164-236) ----------------- */

@@ -18,6 +18,7 @@ from .hmc import (gf_avg_plaq, gf_evolve, gf_hamilton, gf_hamilton_node, gf_sum_
                   set_gm_force, set_rand_gauge_momentum, unitarize)
 from .batch import ChainBatch
 from .flowed_hmc import (FlowInfo, FlowStepInfo, gf_flow, gf_flow_and_ln_det_node, gf_flow_inv, gf_hamilton_flowed,
+                         set_gm_force_flowed_no_det,
                          gf_hamilton_flowed_node, gm_evolve_fg_flowed, mk_flow_info_step, run_flowed_hmc,
                          run_hmc_evolve_flowed, set_gm_force_flowed)
 from .hmc_fa import (MomentumAutoCorr, dot_gauge_momentum, gf_evolve_dual, gf_evolve_fa, gf_evolve_fa_dual,

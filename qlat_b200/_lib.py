@@ -46,6 +46,7 @@ SIGNATURES = {
                                     c_dbl_p, c_dbl_p],
     "qgb_set_gm_force_flowed": [c_field, c_field, ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_int32,
                                 ctypes.c_int32],
+    "qgb_set_gm_force_flowed_no_det": [c_field, c_field, c_field, ctypes.c_void_p, ctypes.c_int32],
     "qgb_set_rand_gauge_momentum_fa": [c_field, c_field, c_u32_p],
     "qgb_gm_hamilton_node_fa": [c_field, c_field, c_dbl_p],
     "qgb_gf_evolve_fa": [c_field, c_field, c_field, ctypes.c_double],

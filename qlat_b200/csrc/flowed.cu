@@ -913,8 +913,15 @@ int qgb_gf_hamilton_flowed_node(const qgb_field* gf0, double beta, double c1, co
   return QGB_OK;
 }
 
-int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double beta, double c1,
-                            const qgb_flow_step* steps, int32_t n, int32_t with_det)
+}  // extern "C"
+
+namespace
+{
+// The force on gf0 of a force F on the flowed field, propagated back through
+// the steps with (with_det) or without the log-determinants' force.  F is the
+// action's force on the flowed field (pre == nullptr) or the given field.
+int flowed_force(qgb_field* gm_force, const qgb_field* gf0, const qgb_field* pre, double beta, double c1,
+                 const qgb_flow_step* steps, int32_t n, int32_t with_det)
 {
   FlowCtx c;
   FL_RC(setup(c, gf0, n, steps));
@@ -933,13 +940,17 @@ int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double be
     FL_CUDA(cudaMemcpyAsync(G[i + 1].p, G[i].p, c.bytes, cudaMemcpyDeviceToDevice, c.st));
     FL_RC(flow_step_dev(c, G[i + 1].p, C.p, steps[i], false));
   }
-  // the force of the action on the flowed field (set_gm_force, hmc.cpp:466-490)
-  qgb_field* gfl = nullptr;
-  FL_RC(qgb_field_create(&gfl, ts, 4, QGB_KIND_COLOR_MATRIX, QGB_F64));
-  FL_CUDA(cudaMemcpyAsync(qgb::field_data(gfl), G[n].p, c.bytes, cudaMemcpyDeviceToDevice, c.st));
-  int rc = qgb_set_gm_force(gm_force, gfl, beta, c1);
-  qgb_field_destroy(gfl);
-  FL_RC(rc);
+  if (pre) {
+    FL_RC(qgb_field_copy(gm_force, pre));
+  } else {
+    // the force of the action on the flowed field (set_gm_force, hmc.cpp:466-490)
+    qgb_field* gfl = nullptr;
+    FL_RC(qgb_field_create(&gfl, ts, 4, QGB_KIND_COLOR_MATRIX, QGB_F64));
+    FL_CUDA(cudaMemcpyAsync(qgb::field_data(gfl), G[n].p, c.bytes, cudaMemcpyDeviceToDevice, c.st));
+    int rc = qgb_set_gm_force(gm_force, gfl, beta, c1);
+    qgb_field_destroy(gfl);
+    FL_RC(rc);
+  }
   void* F = qgb::field_data(gm_force);
   // back through the steps (set_gm_force_propagated_det_from_flow, flowed-hmc.cpp:1456-1477)
   for (int i = n - 1; i >= 0; --i) {
@@ -958,6 +969,22 @@ int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double be
   }
   FL_CUDA(cudaStreamSynchronize(c.st));
   return QGB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int qgb_set_gm_force_flowed(qgb_field* gm_force, const qgb_field* gf0, double beta, double c1,
+                            const qgb_flow_step* steps, int32_t n, int32_t with_det)
+{
+  return flowed_force(gm_force, gf0, nullptr, beta, c1, steps, n, with_det);
+}
+
+int qgb_set_gm_force_flowed_no_det(qgb_field* gm_force, const qgb_field* gm_force_pre, const qgb_field* gf0,
+                                   const qgb_flow_step* steps, int32_t n)
+{
+  if (!gm_force_pre) return ffail(QGB_ERR_INVALID_ARG, "qgb_set_gm_force_flowed_no_det: null force");
+  return flowed_force(gm_force, gf0, gm_force_pre, 0.0, 0.0, steps, n, 0);
 }
 
 }  // extern "C"

@@ -33,10 +33,24 @@ class FlowStepInfo:
 
 
 class FlowInfo:
-    """FlowInfo (flowed-hmc.h:43-45): the flow steps in order."""
+    """FlowInfo (flowed-hmc.h:43-45; qlat.fthmc.FlowInfo, fthmc.py:14-36): the
+    flow steps in order."""
 
     def __init__(self, v=None):
         self.v = list(v or [])
+
+    def add_flow(self, eo: int, mu: int, epsilon: float, flow_size: int = 1) -> None:
+        """Append one step (fthmc.py:21-22): mask eo (1 or 2) of direction mu."""
+        self.v.append(FlowStepInfo(int(eo), int(mu), float(epsilon), int(flow_size)))
+
+    def add_rand_order_flow(self, rng: RngState, epsilon: float, *args) -> None:
+        """Append mk_flow_info_step(rng, epsilon[, epsilon2]) (fthmc.py:24-31)."""
+        if len(args) > 1:
+            raise ValueError("add_rand_order_flow: at most one second epsilon")
+        self.v.extend(mk_flow_info_step(rng, epsilon, *args).v)
+
+    def show(self) -> str:
+        return repr(self)
 
     def _c(self):
         arr = (_Step * max(1, len(self.v)))()
@@ -58,20 +72,34 @@ def mk_flow_info_step(rs: RngState, epsilon: float, epsilon2: float | None = Non
     return FlowInfo(FlowStepInfo(out[i].mask, out[i].mu, out[i].epsilon, out[i].flow_size) for i in range(n.value))
 
 
-def gf_flow(gf0: GaugeField, fi: FlowInfo) -> GaugeField:
-    """gf_flow(gf, gf0, fi) (flowed-hmc.cpp:540-566): the flowed field."""
-    gf = GaugeField(gf0.geo)
+def _flow(name, args):
+    if len(args) == 3:  # (gf, gf0, fi): into gf, which may be gf0 itself
+        gf, gf0, fi = args
+        if gf._h is None:
+            gf.init(gf0.geo)
+        out = gf if gf is not gf0 else GaugeField(gf0.geo)
+    elif len(args) == 2:  # (gf0, fi): a new field
+        gf0, fi = args
+        gf = out = GaugeField(gf0.geo)
+    else:
+        raise TypeError(f"{name}: (gf, gf0, fi) or (gf0, fi)")
     arr, n = fi._c()
-    call("qgb_gf_flow", gf.handle, gf0.handle, arr, n)
-    return gf
+    call("qgb_" + name, out.handle, gf0.handle, arr, n)
+    if out is not gf:
+        gf @= out
+    return None if len(args) == 3 else gf
 
 
-def gf_flow_inv(gf1: GaugeField, fi: FlowInfo) -> GaugeField:
-    """gf_flow_inv(gf, gf1, fi) (flowed-hmc.cpp:568-594)."""
-    gf = GaugeField(gf1.geo)
-    arr, n = fi._c()
-    call("qgb_gf_flow_inv", gf.handle, gf1.handle, arr, n)
-    return gf
+def gf_flow(*args):
+    """gf_flow(gf, gf0, fi) (flowed-hmc.cpp:540-566; fthmc.py:38-42): gf = the
+    flow of gf0.  gf_flow(gf0, fi) returns a new field."""
+    return _flow("gf_flow", args)
+
+
+def gf_flow_inv(*args):
+    """gf_flow_inv(gf, gf1, fi) (flowed-hmc.cpp:568-594; fthmc.py:44-48): gf =
+    the inverse flow of gf1.  gf_flow_inv(gf1, fi) returns a new field."""
+    return _flow("gf_flow_inv", args)
 
 
 def gf_flow_and_ln_det_node(gf0: GaugeField, fi: FlowInfo):
@@ -104,6 +132,15 @@ def set_gm_force_flowed(gm_force: GaugeMomentum, gf0: GaugeField, ga: GaugeActio
     force of the flowed field propagated back without the determinant term."""
     arr, n = fi._c()
     call("qgb_set_gm_force_flowed", gm_force.handle, gf0.handle, ga.beta(), ga.c1(), arr, n, int(bool(with_det)))
+
+
+def set_gm_force_flowed_no_det(gm_force: GaugeMomentum, gm_force_pre: GaugeMomentum, gf0: GaugeField,
+                               fi: FlowInfo) -> None:
+    """set_gm_force_flowed_no_det (flowed-hmc.cpp:1511-1520; fthmc.py:62-67):
+    gm_force_pre, a force on the flowed field, propagated back to gf0 without
+    the determinant term."""
+    arr, n = fi._c()
+    call("qgb_set_gm_force_flowed_no_det", gm_force.handle, gm_force_pre.handle, gf0.handle, arr, n)
 
 
 def gm_evolve_fg_flowed(gm: GaugeMomentum, gf_init: GaugeField, ga: GaugeAction, fi: FlowInfo, fg_dt: float,

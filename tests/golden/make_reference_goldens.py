@@ -12,6 +12,8 @@ Run in a checkout that has the reference source tree (default
   examples-py/gf-utils.log.json               hot-start plaquette, clover and 5-loop charges along the flow
   examples-py/hmc-pure-gauge-fa-sym.log.json  field-accelerated HMC, five jobs, plaq per trajectory
   examples-py/gf-flow-topo.log.json           Wilson and plaquette-weighted flows: plaq, plaq_min, flow time, signatures
+  examples-py/hmc-pure-gauge-symmetric.log.json  HMC with a dual momentum (gf_evolve + gf_evolve_dual), plaq per trajectory
+  examples-py/hmc-pure-gauge-flowed.log.json  flowed HMC (add_rand_order_flow), plaq per trajectory
 """
 
 import json
@@ -86,6 +88,17 @@ def main():
             jobs[-1]["plaq"].append(e[1])
     out["py_hmc_fa_sym"] = {"source": "examples-py/hmc-pure-gauge-fa-sym.log.json", "jobs": jobs,
                             "reference_check_eps": 1e-5}
+    # single-job HMC examples: the job's parameters, then 'run_hmc: {traj} plaq'
+    for key, name in (("py_hmc_symmetric", "hmc-pure-gauge-symmetric"), ("py_hmc_flowed", "hmc-pure-gauge-flowed")):
+        log = json.load(open(os.path.join(ref, "examples-py", name + ".log.json")))
+        params = json.loads(log[0][0])
+        plaq = []
+        for e in log[1:]:
+            m = re.match(r"run_hmc: (\d+) plaq", e[0])
+            assert m and int(m.group(1)) == len(plaq) + 1
+            plaq.append(e[1])
+        out[key] = {"source": f"examples-py/{name}.log.json", "job_tag": params["job_tag"],
+                    "total_site": params["total_site"], "hmc": params["hmc"], "plaq": plaq}
     # gf_flow_topo stages: (name, value) in log order; complex signature
     # entries as [re, im] pairs
     rows = []
