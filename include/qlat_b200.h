@@ -368,6 +368,10 @@ int qgb_gf_plaq_field(qgb_field* f_plaq, const qgb_field* gf);
  * traceless anti-Hermitian part of the clover; the six sum to
  * gf_energy_density_field.  fd: FP64 real, multiplicity 6. */
 int qgb_gf_energy_density_dir_field(qgb_field* fd, const qgb_field* gf);
+/* gf_avg_wilson_loop_normalized_tr(gf, l, t) (qcd-utils.cpp:359-400; qcd.pyx:250-254):
+ * Re tr / 3 of the l x t Wilson loop (l links along a spatial direction, t along
+ * direction 3), averaged over the sites and the three spatial directions. */
+int qgb_gf_avg_wilson_loop_normalized_tr(const qgb_field* gf, int32_t l, int32_t t, double* out);
 /* topology_charge_5 (qcd.cpp:376-389): the lattice sum of the 5-loop improved
  * charge density (same as qgb_gf_topology). */
 int qgb_topology_charge_5(const qgb_field* gf, double* out);

@@ -115,6 +115,7 @@ def lib():
             "or_dot_gauge_momentum": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_gf_plaq_field": (None, [_dbl_p, _dbl_p, _int4]),
             "or_gf_energy_density_dir_field": (None, [_dbl_p, _dbl_p, _int4]),
+            "or_gf_avg_wilson_loop_normalized_tr": (ctypes.c_double, [_dbl_p, _int4, ctypes.c_int, ctypes.c_int]),
             "or_clf_plaq_action_density_field": (None, [_dbl_p, _dbl_p, _int4, ctypes.c_int]),
             "or_set_plaq_flow_z": (None, [_dbl_p, _dbl_p, _dbl_p, _int4]),
             "or_gf_flow_topo_plaq": (ctypes.c_double, [_dbl_p, _int4, ctypes.c_double, ctypes.c_int]),
@@ -371,6 +372,11 @@ def gf_energy_density_dir_field(gf, total_site) -> np.ndarray:
     f = np.zeros((volume(total_site), 6), dtype=np.float64)
     lib().or_gf_energy_density_dir_field(_p(f), _p(gf), _dims(total_site))
     return f
+
+
+def gf_avg_wilson_loop_normalized_tr(gf, total_site, l: int, t: int) -> float:
+    """qcd-utils.cpp:359-400"""
+    return lib().or_gf_avg_wilson_loop_normalized_tr(_p(gf), _dims(total_site), int(l), int(t))
 
 
 def clf_plaq_action_density_field(gf, total_site, spatial: bool = False) -> np.ndarray:

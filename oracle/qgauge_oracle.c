@@ -1324,6 +1324,30 @@ void or_gf_plaq_field(double* f_plaq, const double* gf, const int dims[4])
   }
 }
 
+/* qcd-utils.cpp:359-400 (make_wilson_loop_path: l along +i, t along +3, l along -i, t along -3) */
+double or_gf_avg_wilson_loop_normalized_tr(const double* gf, const int dims[4], int l, int t)
+{
+  const geo_t g = mk_geo(dims);
+  int path[256];
+  double tot = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    int n = 0;
+    for (int k = 0; k < l && n < 256; ++k) path[n++] = i;
+    for (int k = 0; k < t && n < 256; ++k) path[n++] = 3;
+    for (int k = 0; k < l && n < 256; ++k) path[n++] = -i - 1;
+    for (int k = 0; k < t && n < 256; ++k) path[n++] = -4;
+    cd sum = {0.0, 0.0};
+    for (long s = 0; s < g.vol; ++s) {
+      int x[4];
+      coor_from_index(&g, s, x);
+      cm w = wilson_line(gf, &g, x, path, n);
+      sum = c_add(sum, m_trace(&w));
+    }
+    tot += sum.re / (double)g.vol;
+  }
+  return tot / 3.0 / 3.0;
+}
+
 /* wilson-flow.cpp:53-95 */
 void or_gf_energy_density_dir_field(double* fd, const double* gf, const int dims[4])
 {

@@ -101,6 +101,8 @@ void or_dot_gauge_momentum(double* f, const double* gm1, const double* gm2, cons
  * instanton_map.py:91-191).  Plaquette fields hold 6 doubles per site, planes
  * (0,1) (0,2) (0,3) (1,2) (1,3) (2,3). */
 void or_gf_plaq_field(double* f_plaq, const double* gf, const int dims[4]);
+/* qcd-utils.cpp:359-400: Re tr / 3 of the l x t Wilson loop averaged over sites and spatial directions */
+double or_gf_avg_wilson_loop_normalized_tr(const double* gf, const int dims[4], int l, int t);
 /* wilson-flow.cpp:53-95: per site and plane -Re tr(G G), G = TA(clover); 6 per site */
 void or_gf_energy_density_dir_field(double* fd, const double* gf, const int dims[4]);
 void or_clf_plaq_action_density_field(double* paf, const double* gf, const int dims[4], int spatial);

@@ -12,7 +12,7 @@ the first call loads the built libqlat_b200.so and raises if it is missing
 from ._lib import QlatB200Error, load as _load
 from .field import (F32, F64, Coordinate, Field, FieldColorMatrix, FieldRealD, GaugeAction, GaugeField,
                     GaugeMomentum, Geometry, RngState, read_gauge_field_header, set_unit)
-from .hmc import (gf_avg_plaq, gf_evolve, gf_hamilton, gf_hamilton_node, gf_sum_re_tr_plaq_node_no_comm,
+from .hmc import (gf_avg_wilson_loop_normalized_tr, gf_avg_plaq, gf_evolve, gf_hamilton, gf_hamilton_node, gf_sum_re_tr_plaq_node_no_comm,
                   gf_sum_re_tr_rect_node_no_comm, glb_sum_double, gm_evolve_fg_pure_gauge, gm_hamilton_node,
                   metropolis_accept, metropolis_accept_cpp, run_hmc_evolve_pure_gauge, run_hmc_pure_gauge,
                   set_gm_force, set_rand_gauge_momentum, unitarize)

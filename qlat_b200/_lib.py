@@ -63,6 +63,7 @@ SIGNATURES = {
     "qgb_gf_plaq_field": [c_field, c_field],
     "qgb_gf_energy_density_dir_field": [c_field, c_field],
     "qgb_topology_charge_5": [c_field, c_dbl_p],
+    "qgb_gf_avg_wilson_loop_normalized_tr": [c_field, ctypes.c_int32, ctypes.c_int32, c_dbl_p],
     "qgb_gf_plaq_action_density_field": [c_field, c_field, ctypes.c_int32],
     "qgb_set_plaq_flow_z": [c_field, c_field, c_field],
     "qgb_gf_flow_topo": [c_field, ctypes.c_double, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, c_dbl_p],

@@ -42,6 +42,37 @@ using namespace qgb;
 
 constexpr int TF_BS = 256;
 
+// fixed-order block sum of one value per thread into partials[blockIdx.x]
+__device__ __forceinline__ void block_sum_store_tf(double v, double* partials)
+{
+  __shared__ double sm[TF_BS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < TF_BS / 32; ++i) t += sm[i];
+    partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_sum_partials_tf(const double* partials, int n, double* out)
+{
+  __shared__ double sm[32];
+  double t = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) t += partials[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sm[i];
+    *out = r;
+  }
+}
+
 // plane index of (mu, nu), mu != nu: (0,1) (0,2) (0,3) (1,2) (1,3) (2,3)
 // (gf_plaq_field_no_comm, qcd.cpp:312-317; the table of wilson-flow.cpp:170-181)
 __host__ __device__ __forceinline__ int plane_of(int mu, int nu)
@@ -173,6 +204,46 @@ __global__ void __launch_bounds__(TF_BS) k_energy_density_dir(Geo g, const Cx<R>
     const M3<R> G = traceless_antiherm(scale(R(0.25), c));
     out[lay_index<1>(g.V, p, 0, s)] = -(double)re_tr_mul(G, G);
   }
+}
+
+// gf_avg_wilson_loop (qcd-utils.cpp:359-400): per site, the sum over the
+// spatial directions i of Re tr of the l x t loop from the site: l links along
+// +i, t along +3, l along -i, t along -3, multiplied in that order as
+// gf_avg_wilson_line walks its path segments.
+template <typename R>
+__global__ void __launch_bounds__(TF_BS) k_wilson_loop(Geo g, const Cx<R>* Up, int l, int t, double* partials)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (s < g.V) {
+    const CField<R> U{Up, g.V};
+    const Coord x0 = coord_of(g, s);
+    for (int i = 0; i < 3; ++i) {
+      int c[4] = {x0.c[0], x0.c[1], x0.c[2], x0.c[3]};
+      auto site = [&]() {
+        return (long)c[0] + (long)g.d[0] * ((long)c[1] + (long)g.d[1] * ((long)c[2] + (long)g.d[2] * (long)c[3]));
+      };
+      M3<R> m = m3_unit<R>();
+      for (int k = 0; k < l; ++k) {
+        m = mul(m, U.ld(site(), i));
+        c[i] = c[i] + 1 == g.d[i] ? 0 : c[i] + 1;
+      }
+      for (int k = 0; k < t; ++k) {
+        m = mul(m, U.ld(site(), 3));
+        c[3] = c[3] + 1 == g.d[3] ? 0 : c[3] + 1;
+      }
+      for (int k = 0; k < l; ++k) {
+        c[i] = c[i] == 0 ? g.d[i] - 1 : c[i] - 1;
+        m = mul_adj(m, U.ld(site(), i));
+      }
+      for (int k = 0; k < t; ++k) {
+        c[3] = c[3] == 0 ? g.d[3] - 1 : c[3] - 1;
+        m = mul_adj(m, U.ld(site(), 3));
+      }
+      v += (double)re_tr(m);
+    }
+  }
+  block_sum_store_tf(v, partials);
 }
 
 // per-block min and max of each component of a real field (blockDim TF_BS)
@@ -318,7 +389,7 @@ int check_real(const Meta& f, const Meta& gf, int mult, const char* what)
   return QGB_OK;
 }
 
-enum { TAG_PLAQ = 0x7B000, TAG_Z64, TAG_Z32, TAG_MM_PART, TAG_MM_OUT, TAG_TS_OUT };
+enum { TAG_PLAQ = 0x7B000, TAG_Z64, TAG_Z32, TAG_MM_PART, TAG_MM_OUT, TAG_TS_OUT, TAG_WL_PART, TAG_WL_OUT };
 
 unsigned blocks_of(long V) { return (unsigned)((V + TF_BS - 1) / TF_BS); }
 
@@ -423,6 +494,34 @@ int qgb_gf_energy_density_dir_field(qgb_field* fd, const qgb_field* gf_)
 }
 
 int qgb_topology_charge_5(const qgb_field* gf, double* out) { return qgb_gf_topology(gf, out); }
+
+int qgb_gf_avg_wilson_loop_normalized_tr(const qgb_field* gf_, int32_t l, int32_t t, double* out)
+{
+  const char* what = "qgb_gf_avg_wilson_loop_normalized_tr";
+  Meta gf;
+  TF_RC(meta_of(gf_, gf, what));
+  TF_RC(check_gauge(gf, what));
+  if (!out || l < 0 || t < 0) return tfail(QGB_ERR_INVALID_ARG, std::string(what) + ": bad argument");
+  cudaStream_t st;
+  TF_RC(qgb::library_stream(&st));
+  const unsigned nb = blocks_of(gf.g.V);
+  void *part = nullptr, *res = nullptr;
+  TF_RC(qgb::scratch_buffer((size_t)nb * sizeof(double), TAG_WL_PART, &part));
+  TF_RC(qgb::scratch_buffer(sizeof(double), TAG_WL_OUT, &res));
+  if (gf.prec == QGB_F64)
+    k_wilson_loop<double><<<nb, TF_BS, 0, st>>>(gf.g, (const Cx<double>*)gf.d, l, t, (double*)part);
+  else
+    k_wilson_loop<float><<<nb, TF_BS, 0, st>>>(gf.g, (const Cx<float>*)gf.d, l, t, (double*)part);
+  TF_LAUNCHED();
+  k_sum_partials_tf<<<1, 1024, 0, st>>>((const double*)part, (int)nb, (double*)res);
+  TF_LAUNCHED();
+  double h = 0.0;
+  TF_CUDA(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, st));
+  TF_CUDA(cudaStreamSynchronize(st));
+  // average over the sites and the three spatial directions, Re tr / 3
+  *out = h / (3.0 * (double)gf.g.V) / 3.0;
+  return QGB_OK;
+}
 
 int qgb_gf_plaq_action_density_field(qgb_field* paf, const qgb_field* gf_, int32_t spatial)
 {

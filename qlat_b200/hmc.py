@@ -72,6 +72,15 @@ def gf_avg_plaq(gf: GaugeField) -> float:
     return o.value
 
 
+def gf_avg_wilson_loop_normalized_tr(gf: GaugeField, l: int, t: int) -> float:
+    """qcd.pyx:250-254 -> gf_avg_wilson_loop (qcd-utils.cpp:359-400): Re tr / 3 of
+    the l x t Wilson loop (spatial side l, time side t), averaged over sites and
+    the three spatial directions."""
+    o = _d()
+    call("qgb_gf_avg_wilson_loop_normalized_tr", gf.handle, int(l), int(t), ctypes.byref(o))
+    return o.value
+
+
 def gf_evolve(gf: GaugeField, gm: GaugeMomentum, step_size: float):
     """hmc.cpp:311-328: U <- unitarize(exp(step_size P) U)"""
     call("qgb_gf_evolve", gf.handle, gm.handle, float(step_size))

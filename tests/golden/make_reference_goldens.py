@@ -14,6 +14,7 @@ Run in a checkout that has the reference source tree (default
   examples-py/gf-flow-topo.log.json           Wilson and plaquette-weighted flows: plaq, plaq_min, flow time, signatures
   examples-py/hmc-pure-gauge-symmetric.log.json  HMC with a dual momentum (gf_evolve + gf_evolve_dual), plaq per trajectory
   examples-py/hmc-pure-gauge-flowed.log.json  flowed HMC (add_rand_order_flow), plaq per trajectory
+  examples-py/hmc-pure-gauge-flowed-test.log.json  flowed HMC, plaq and 1x1 Wilson loop per trajectory
 """
 
 import json
@@ -99,6 +100,11 @@ def main():
             plaq.append(e[1])
         out[key] = {"source": f"examples-py/{name}.log.json", "job_tag": params["job_tag"],
                     "total_site": params["total_site"], "hmc": params["hmc"], "plaq": plaq}
+    g = load("hmc-pure-gauge-flowed-test.log.json")
+    out["py_hmc_flowed_test"] = {"source": "examples-py/hmc-pure-gauge-flowed-test.log.json",
+                                 "rows": [[t, g[f"beta=2.31_c1=-0.331 traj={t} plaq"][0],
+                                           g[f"beta=2.31_c1=-0.331 traj={t} wilson_loop"][0]] for t in (1, 2, 3)],
+                                 "eps": 1e-10}
     # gf_flow_topo stages: (name, value) in log order; complex signature
     # entries as [re, im] pairs
     rows = []

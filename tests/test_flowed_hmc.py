@@ -107,7 +107,11 @@ def test_flowed_hmc_reference_log(q, goldens):
     gf.set_unit()
     gf.set_rand(q.RngState(), 1.0, 1)
     rs = q.RngState("test_hmc-4x4x4x8")
+    wl = {t: w for t, _, w in goldens["py_hmc_flowed_test"]["rows"]}
     for traj, plaq_ref, _ in g["rows"]:
         q.run_flowed_hmc(gf, ga, traj, rs.split(f"hmc-{traj}"))
         p = q.gf_avg_plaq(gf)
         assert abs(p - plaq_ref) <= 1e-11 * abs(plaq_ref), (traj, p, plaq_ref)
+        # examples-py/hmc-pure-gauge-flowed-test.py: the same chain, with the 1 x 1 Wilson loop
+        w = q.gf_avg_wilson_loop_normalized_tr(gf, 1, 1)
+        assert abs(w - wl[traj]) <= 1e-10 * abs(wl[traj]), (traj, w, wl[traj])

@@ -316,3 +316,26 @@ def test_gpu_energy_density_dir_and_charge_5(q, oracle):
         assert np.abs(d - o.gf_energy_density_dir_field(ref, ts)).max() < 1e-13
         assert np.abs(d.sum(axis=1) - q.gf_energy_density_field(gf).to_numpy()[:, 0]).max() < 1e-13
         assert q.topology_charge_5(gf) == q.gf_topology(gf)
+
+
+def test_oracle_wilson_loop_1x1_is_the_timelike_plaquette(oracle):
+    """gf_avg_wilson_loop(gf, 1, 1) averages the plaquettes of the planes (i, 3)."""
+    o = oracle
+    gf = o.new_field(TS)
+    o.gf_set_rand(gf, TS, o.RngState("wl").split("gf-init"), 0.4, 2)
+    fp = o.gf_plaq_field(gf, TS)
+    assert abs(o.gf_avg_wilson_loop_normalized_tr(gf, TS, 1, 1) - fp[:, [2, 4, 5]].mean()) < 1e-14
+
+
+@pytest.mark.gpu
+def test_gpu_wilson_loops(q, oracle):
+    o = oracle
+    for ts in (TS, (3, 4, 5, 6)):
+        gf = q.GaugeField(q.Geometry(ts))
+        gf.set_rand(q.RngState("wl").split("gf-init"), 0.3, 2)
+        ref = o.new_field(ts)
+        o.gf_set_rand(ref, ts, o.RngState("wl").split("gf-init"), 0.3, 2)
+        for l, t in ((1, 1), (1, 2), (2, 1), (2, 3)):
+            a = q.gf_avg_wilson_loop_normalized_tr(gf, l, t)
+            b = o.gf_avg_wilson_loop_normalized_tr(ref, ts, l, t)
+            assert abs(a - b) < 1e-13, (ts, l, t, a, b)
