@@ -82,3 +82,22 @@ def test_field_creation_fails_loudly_without_device():
     with pytest.raises(q.QlatB200Error) as e:
         q.GaugeField(q.Geometry((4, 4, 4, 4)))
     assert e.value.code == 8
+
+
+def test_missing_library_fails_loudly():
+    """Without the CUDA library the package raises at its first call; nothing
+    falls back to another implementation."""
+    import subprocess
+    import sys
+    code = ("import qlat_b200._lib as L\n"
+            "L.LIB_PATH = '/nonexistent/libqlat_b200.so'\n"
+            "L._lib = None\n"
+            "import qlat_b200 as q\n"
+            "try:\n"
+            "    q.GaugeField(q.Geometry((4, 4, 4, 4)))\n"
+            "except RuntimeError as e:\n"
+            "    print('raised:', e)\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120,
+                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "raised:" in r.stdout and "is missing" in r.stdout
