@@ -531,11 +531,11 @@ int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int3
 int qgb_gf_action_sums_noalloc(const double* links_dev, const int32_t total_site[4], int32_t rect, double* out_dev,
                                void* stream);
 
-/* FP32 FMA rate of the current device in TFLOP/s (2 flop per FMA), from 16
+/* FMA rate of the current device in TFLOP/s (2 flop per FMA), from 16
  * independent FMA chains per thread over 16 blocks of 256 threads per SM:
- * scalar FFMA (packed = 0) or packed f32x2 FMA (packed = 1); best of reps
- * launches after one warm-up (no counterpart in the reference). */
-int qgb_fp32_fma_rate(int32_t packed, int32_t reps, double* tflops);
+ * kind 0 scalar FP32, 1 packed f32x2, 2 FP64; best of reps launches after one
+ * warm-up (no counterpart in the reference). */
+int qgb_fma_rate(int32_t kind, int32_t reps, double* tflops);
 
 /* Number of kernels this library has launched since it was loaded. */
 int qgb_launch_count(int64_t* out);

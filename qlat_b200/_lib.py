@@ -70,7 +70,7 @@ SIGNATURES = {
     "qgb_field_glb_min_max": [c_field, c_dbl_p, c_dbl_p],
     "qgb_field_glb_sum_tslice": [c_field, ctypes.c_int32, c_dbl_p],
     "qgb_field_abs": [c_field],
-    "qgb_fp32_fma_rate": [ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+    "qgb_fma_rate": [ctypes.c_int32, ctypes.c_int32, c_dbl_p],
     "qgb_gm_hamilton_node_sites": [c_field, ctypes.c_int64, ctypes.c_int64, c_dbl_p],
     "qgb_gf_action_sums_sites": [c_field, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, c_dbl_p],
     "qgb_gf_hamilton_node_sites": [c_field, ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int64,

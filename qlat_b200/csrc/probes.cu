@@ -1,6 +1,6 @@
 // probes.cu -- hardware-rate measurements used to put the force kernels'
-// counters in context (no counterpart in the reference): the FP32 FMA rate of
-// the device with scalar FFMA chains and with packed f32x2 chains.
+// counters in context (no counterpart in the reference): the FMA rate of the
+// device with scalar FP32 chains, packed f32x2 chains and FP64 chains.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -51,6 +51,21 @@ __global__ void __launch_bounds__(256) k_fma_packed(float* out, int iters, float
   out[(long)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+__global__ void __launch_bounds__(256) k_fma_double(double* out, int iters, double a, double b)
+{
+  double x[PROBE_CHAINS];
+#pragma unroll
+  for (int j = 0; j < PROBE_CHAINS; ++j) x[j] = threadIdx.x * 1e-3 + j;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < PROBE_CHAINS; ++j) x[j] = fma(x[j], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < PROBE_CHAINS; ++j) s += x[j];
+  out[(long)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 int pfail(int code, const std::string& m)
 {
   qgb::set_last_error(m);
@@ -61,25 +76,26 @@ int pfail(int code, const std::string& m)
 
 extern "C" {
 
-int qgb_fp32_fma_rate(int32_t packed, int32_t reps, double* tflops)
+int qgb_fma_rate(int32_t kind, int32_t reps, double* tflops)
 {
-  if (!tflops || reps < 1) return pfail(QGB_ERR_INVALID_ARG, "qgb_fp32_fma_rate: bad argument");
+  if (!tflops || reps < 1 || kind < 0 || kind > 2) return pfail(QGB_ERR_INVALID_ARG, "qgb_fma_rate: bad argument");
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
                                                  cudaSuccess)
-    return pfail(QGB_ERR_NO_DEVICE, "qgb_fp32_fma_rate: no CUDA device");
+    return pfail(QGB_ERR_NO_DEVICE, "qgb_fma_rate: no CUDA device");
   const int blocks = sms * 16, threads = 256, iters = 4096;
-  float* out = nullptr;
-  if (cudaMalloc(&out, sizeof(float) * (size_t)blocks * threads) != cudaSuccess)
-    return pfail(QGB_ERR_ALLOC, "qgb_fp32_fma_rate: cudaMalloc failed");
+  void* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double) * (size_t)blocks * threads) != cudaSuccess)
+    return pfail(QGB_ERR_ALLOC, "qgb_fma_rate: cudaMalloc failed");
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
   for (int r = 0; r <= reps; ++r) {  // the first launch warms up
     cudaEventRecord(e0);
-    if (packed) k_fma_packed<<<blocks, threads>>>(out, iters, 0.999f, 1e-3f);
-    else k_fma_scalar<<<blocks, threads>>>(out, iters, 0.999f, 1e-3f);
+    if (kind == 1) k_fma_packed<<<blocks, threads>>>((float*)out, iters, 0.999f, 1e-3f);
+    else if (kind == 2) k_fma_double<<<blocks, threads>>>((double*)out, iters, 0.999, 1e-3);
+    else k_fma_scalar<<<blocks, threads>>>((float*)out, iters, 0.999f, 1e-3f);
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -91,7 +107,7 @@ int qgb_fp32_fma_rate(int32_t packed, int32_t reps, double* tflops)
   cudaEventDestroy(e1);
   cudaFree(out);
   qgb::add_launches(reps + 1);
-  if (err != cudaSuccess) return pfail(QGB_ERR_CUDA, std::string("qgb_fp32_fma_rate: ") + cudaGetErrorString(err));
+  if (err != cudaSuccess) return pfail(QGB_ERR_CUDA, std::string("qgb_fma_rate: ") + cudaGetErrorString(err));
   const double fmas = (double)blocks * threads * iters * PROBE_CHAINS;
   *tflops = 2.0 * fmas / (best * 1e-3) / 1e12;
   return QGB_OK;

@@ -5,7 +5,7 @@
     python -m qlat_b200.kernel_bench force-profile --variants 0,7 [--lattice 24,24,24,48]
         one set_gm_force launch per variant and precision (Iwasaki), for ncu -k regex:k_force
     python -m qlat_b200.kernel_bench fma-peak [--reps 5]
-        FP32 FMA rate of the device: scalar FFMA chains and packed f32x2 chains
+        FMA rate of the device: scalar FP32, packed f32x2 and FP64 chains
     python -m qlat_b200.kernel_bench flow [--lattice 32,32,32,32] [--steps 80] [--every 4]
         gradient flow (RK3, eps = 0.05) with t^2 E(t) and the clover charge Q measured every
         `every` steps, FP64 and FP32 storage; prints timings and the FP32 errors
@@ -70,9 +70,9 @@ def fma_peak(args):
     from qlat_b200._lib import call
     torch.cuda.set_device(0)
     out = {}
-    for name, packed in (("scalar_ffma", 0), ("packed_ffma2", 1)):
+    for name, kind in (("scalar_ffma", 0), ("packed_ffma2", 1), ("fp64_dfma", 2)):
         t = ctypes.c_double()
-        call("qgb_fp32_fma_rate", packed, int(args.reps), ctypes.byref(t))
+        call("qgb_fma_rate", kind, int(args.reps), ctypes.byref(t))
         out[name + "_tflops"] = t.value
     print(json.dumps(out))
 
