@@ -44,6 +44,7 @@ extern "C" {
 #define QGB_ERR_MISMATCH 7
 #define QGB_ERR_NO_DEVICE 8
 #define QGB_ERR_IO 9 /* file missing, unreadable, short or not in the expected format */
+#define QGB_ERR_HOOK 10 /* a caller-supplied hook returned non-zero */
 
 #define QGB_F64 64
 #define QGB_F32 32
@@ -76,7 +77,15 @@ int qgb_synchronize(void);
  * 753-781); kind is QGB_KIND_COLOR_MATRIX or QGB_KIND_REAL. */
 int qgb_field_create(qgb_field** out, const int32_t total_site[4], int32_t multiplicity, int32_t kind,
                      int32_t precision);
+/* Releases the field; its device storage is kept in a pool keyed by size and
+ * reused by the next qgb_field_create of that size (the reference's
+ * run_hmc_pure_gauge, hmc.pyx:190-216, builds a link copy and a momentum field
+ * every trajectory). */
 int qgb_field_destroy(qgb_field* f);
+/* Frees the pooled storage of destroyed fields (qgb_field_create also does
+ * this by itself when cudaMalloc runs out of memory); writes the bytes freed
+ * when released is not NULL. */
+int qgb_field_pool_release(int64_t* released);
 int qgb_field_info(const qgb_field* f, int32_t total_site[4], int32_t* multiplicity, int32_t* kind,
                    int32_t* precision);
 /* Copy a host buffer in the reference memory image into the field (and back).
@@ -161,6 +170,23 @@ int qgb_run_hmc_evolve(qgb_field* gm, qgb_field* gf, double beta, double c1, int
 int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step,
                              double md_time, int32_t integrator, int32_t reunit_interval,
                              double* delta_h);
+
+/* Halo hook of a domain-decomposed trajectory: called with the link field
+ * before every force evaluation, after the kernels before it have been
+ * enqueued on the library stream; it must leave the field's halo sites fresh
+ * copies of the neighbouring domains' links and return 0 (any other value
+ * aborts the trajectory with QGB_ERR_HOOK). */
+typedef int (*qgb_halo_hook)(qgb_field* gf, void* user);
+/* The molecular dynamics of run_hmc_evolve_pure_gauge (hmc.pyx:169-188)
+ * without the Hamiltonians, in the fields' precision (gm, gf both FP64 or both
+ * FP32), on the reference's refresh-before-force schedule (hmc.cpp:466-490
+ * refreshes the expanded field before each force): hook(gf, user) runs before
+ * each force evaluation when hook is not NULL.  The kernel sequence is the one
+ * qgb_run_hmc_evolve (reunit_interval = 0: unitarise after every exponential)
+ * and qgb_run_hmc_evolve_mixed (reunit_interval > 0, on FP32 fields: FP64
+ * re-unitarisation every that many steps) run. */
+int qgb_run_md_hooked(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step, double md_time,
+                      int32_t integrator, int32_t reunit_interval, qgb_halo_hook hook, void* user);
 
 /* ---- hot path: gradient flow (wilson-flow.h:9-43, everything.pxd:514-521) --- */
 

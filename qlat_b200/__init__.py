@@ -131,3 +131,14 @@ def force_time_variant(gf, c1: float, variant: int, reps: int = 3) -> float:
 def synchronize():
     from ._lib import call
     call("qgb_synchronize")
+
+
+def release_field_pool() -> int:
+    """Free the device storage the library keeps from destroyed fields for
+    reuse (torch.cuda.empty_cache for this library's fields); returns the
+    bytes freed."""
+    import ctypes
+    from ._lib import call
+    n = ctypes.c_int64()
+    call("qgb_field_pool_release", ctypes.byref(n))
+    return int(n.value)

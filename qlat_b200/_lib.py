@@ -21,6 +21,8 @@ c_u64_p = ctypes.POINTER(ctypes.c_uint64)
 c_field = ctypes.c_void_p
 c_field_p = ctypes.POINTER(ctypes.c_void_p)
 i32x4 = ctypes.c_int32 * 4
+# qgb_halo_hook: int (*)(qgb_field* gf, void* user)
+HALO_HOOK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
 
 # name -> (argtypes); every entry point returns int status
 SIGNATURES = {
@@ -30,6 +32,7 @@ SIGNATURES = {
     "qgb_synchronize": [],
     "qgb_field_create": [c_field_p, i32x4, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "qgb_field_destroy": [c_field],
+    "qgb_field_pool_release": [c_i64_p],
     "qgb_nersc_write_host": [ctypes.c_char_p, c_dbl_p, i32x4, ctypes.c_double, ctypes.c_double, ctypes.c_char_p,
                              ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int64,
                              c_i64_p],
@@ -112,6 +115,8 @@ SIGNATURES = {
                            ctypes.c_int32, c_dbl_p],
     "qgb_run_hmc_evolve_mixed": [c_field, c_field, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                  ctypes.c_double, ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+    "qgb_run_md_hooked": [c_field, c_field, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_double,
+                          ctypes.c_int32, ctypes.c_int32, HALO_HOOK, ctypes.c_void_p],
     "qgb_set_wilson_flow_z": [c_field, c_field, ctypes.c_double],
     "qgb_gf_wilson_flow_step": [c_field, ctypes.c_double, ctypes.c_double],
     "qgb_gf_wilson_flow_step_euler": [c_field, ctypes.c_double, ctypes.c_double],

@@ -91,6 +91,10 @@ struct Ctx {
   cudaEvent_t up_ready[2] = {nullptr, nullptr};
   cudaEvent_t up_order[2] = {nullptr, nullptr};
   int up_next = 0;
+  // storage of destroyed fields by size, reused by the next field of that size
+  // (the reference's drivers build a momentum and a link copy every trajectory)
+  std::map<size_t, std::vector<void*>> field_pool;
+  size_t field_pool_bytes = 0;
 };
 
 Ctx g_ctx;
@@ -222,6 +226,14 @@ int get_scratch(size_t bytes, int tag, void** out)
   }
   *out = v[0];
   return QGB_OK;
+}
+
+void release_field_pool()
+{
+  for (auto& kv : g_ctx.field_pool)
+    for (void* p : kv.second) cudaFree(p);
+  g_ctx.field_pool.clear();
+  g_ctx.field_pool_bytes = 0;
 }
 
 int read_results(int slot, int n, double* out)
@@ -367,11 +379,20 @@ ForceArgs fargs(const void* U, void* out, double beta, double c1, double dt)
 // examples-py/hmc-pure-gauge-fgf.py:57-69 (gf_evolve dt/2, gm += dt F, gf_evolve dt/2).
 // unit_each: unitarize after every exponential; reunit_every > 0 re-unitarises
 // the links with FP64 arithmetic every that many steps.
+// hook (with hook_gf, the field whose buffer is gf) refreshes the halo of a
+// domain-decomposed field before each force evaluation that reads gf.
 template <typename R>
 int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, double c1, int n_step, double md_time,
-                  int integrator, int unit_each, int reunit_every)
+                  int integrator, int unit_each, int reunit_every, qgb_halo_hook hook = nullptr,
+                  qgb_field* hook_gf = nullptr, void* hook_user = nullptr)
 {
   const double dt = md_time / n_step;
+  auto refresh = [&]() -> int {
+    if (!hook) return QGB_OK;
+    const int rc = hook(hook_gf, hook_user);
+    if (rc) return fail(QGB_ERR_HOOK, "halo hook returned " + std::to_string(rc));
+    return QGB_OK;
+  };
   // gm += h F(U) followed by gf = exp(eps gm) gf, as one launch: the update
   // kernel's epilogue evolves this thread's own link of gf (U is tmp for the
   // force-gradient step, so gf is never read at other links; for leapfrog U is
@@ -393,6 +414,7 @@ int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, doub
     for (int i = 0; i < n_step; ++i) {
       const bool reunit = reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step;
       for (int half = 0; half < 2; ++half) {
+        QGB_RC(refresh());
         ForceArgs a = fargs(gf, tmp, beta, c1, fg_dt);
         a.unitarize = unit_each;
         QGB_RC(force<R>(g, qgb::FORCE_EVOLVE, a));
@@ -403,6 +425,7 @@ int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, doub
   } else if (integrator == QGB_INTEGRATOR_LEAPFROG) {
     for (int i = 0; i < n_step; ++i) {
       QGB_RC(evolve<R>(g, gf, gm, 0.5 * dt, unit_each));
+      QGB_RC(refresh());
       ForceArgs b = fargs(gf, gm, beta, c1, dt);
       QGB_RC(force<R>(g, qgb::FORCE_UPDATE, b));
       QGB_RC(evolve<R>(g, gf, gm, 0.5 * dt, unit_each));
@@ -631,7 +654,20 @@ int qgb_field_create(qgb_field** out, const int32_t total_site[4], int32_t multi
   f->bytes = (size_t)qgb::padded_sites(V) * multiplicity * (kind == QGB_KIND_COLOR_MATRIX ? 18 : 1) *
              (precision == QGB_F64 ? 8 : 4);
   f->d = nullptr;
-  cudaError_t e = cudaMalloc(&f->d, f->bytes);
+  cudaError_t e = cudaSuccess;
+  auto pooled = g_ctx.field_pool.find(f->bytes);
+  if (pooled != g_ctx.field_pool.end() && !pooled->second.empty()) {
+    f->d = pooled->second.back();
+    pooled->second.pop_back();
+    g_ctx.field_pool_bytes -= f->bytes;
+  } else {
+    e = cudaMalloc(&f->d, f->bytes);
+    if (e == cudaErrorMemoryAllocation && g_ctx.field_pool_bytes > 0) {
+      cudaGetLastError();
+      release_field_pool();
+      e = cudaMalloc(&f->d, f->bytes);
+    }
+  }
   if (e != cudaSuccess) {
     delete f;
     cudaGetLastError();
@@ -651,9 +687,24 @@ int qgb_field_destroy(qgb_field* f)
 {
   if (!f) return QGB_OK;
   std::lock_guard<std::recursive_mutex> lock(g_mu);
-  if (g_ctx.ready) cudaStreamSynchronize(g_ctx.stream);
-  cudaFree(f->d);
+  if (g_ctx.ready) {
+    // the storage goes back to the pool once no queued work can touch it
+    cudaStreamSynchronize(g_ctx.stream);
+    g_ctx.field_pool[f->bytes].push_back(f->d);
+    g_ctx.field_pool_bytes += f->bytes;
+  } else {
+    cudaFree(f->d);
+  }
   delete f;
+  return QGB_OK;
+}
+
+int qgb_field_pool_release(int64_t* released)
+{
+  std::lock_guard<std::recursive_mutex> lock(g_mu);
+  if (released) *released = (int64_t)g_ctx.field_pool_bytes;
+  if (g_ctx.ready) cudaStreamSynchronize(g_ctx.stream);
+  release_field_pool();
   return QGB_OK;
 }
 
@@ -1254,6 +1305,27 @@ int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c
   *delta_h = r[3] + gf_hamilton_from(r[4], r[5], beta, c1) - e0;
   if (isnan(*delta_h)) return fail(QGB_ERR_NAN, "qgb_run_hmc_evolve_mixed: delta_h is NaN");
   return QGB_OK;
+}
+
+int qgb_run_md_hooked(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step, double md_time,
+                      int32_t integrator, int32_t reunit_interval, qgb_halo_hook hook, void* user)
+{
+  QGB_CTX();
+  QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_run_md_hooked"));
+  QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_run_md_hooked"));
+  QGB_CHECK(gf->mult == 4 && gm->mult == 4 && same_geo(gf, gm) && gf->prec == gm->prec && gf != gm,
+            QGB_ERR_MISMATCH, "qgb_run_md_hooked: field mismatch");
+  QGB_CHECK(n_step >= 1 && reunit_interval >= 0, QGB_ERR_INVALID_ARG, "qgb_run_md_hooked: bad argument");
+  const Geo g = geo_of(gf);
+  void* tmp = nullptr;
+  // slot 14: no entry point the hook may call (field copies, packing) uses it
+  QGB_RC(get_scratch(gf->bytes, 14, &tmp));
+  const int unit_each = reunit_interval > 0 ? 0 : 1;
+  if (gf->prec == QGB_F64)
+    return md_trajectory<double>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, unit_each,
+                                 reunit_interval, hook, gf, user);
+  return md_trajectory<float>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, unit_each,
+                              reunit_interval, hook, gf, user);
 }
 
 // ---- gradient flow ---------------------------------------------------------

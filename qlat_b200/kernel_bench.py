@@ -14,12 +14,17 @@
     python -m qlat_b200.kernel_bench flow-adjoint [--lattice 16,16,16,16] [--steps 40] [--every 8]
         backward through the Wilson flow: timing, finite-difference check, flowed-field HMC
 
+    python -m qlat_b200.kernel_bench slabs [--lattice 24,24,24,64] [--precision mixed]
+        one chain as a one-rank time slab (4 halo slices each side, a halo refresh before every
+        force evaluation) against the plain single-GPU trajectory: traj/s and the exchange time
+
 Each command prints one JSON line.
 """
 
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import time
 
@@ -251,6 +256,73 @@ def flow_adjoint(args):
     print(json.dumps(out))
 
 
+def slabs(args):
+    """Iwasaki (beta 2.13, c1 -0.331) force-gradient trajectories of n_step steps,
+    always accepted, from one hot start: the plain single-GPU form and the same
+    chain held as a one-rank time slab, whose halo is its own periodic copy
+    refreshed through pack / unpack before every force evaluation.  The slab
+    form computes the extra halo slices and stops the stream at every
+    refresh, which is what a multi-rank run adds besides the network."""
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    ts = _lattice(args.lattice)
+    ga = q.GaugeAction(2.13, -0.331)
+    rs = q.RngState("b200-slabs-bench")
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(rs.split("gf-init"), 0.3, 1)
+    for prec in (q.F64, q.F32):
+        q.autotune_force(gf.copy(precision=prec), ga.c1())
+    sl = q.TimeSlabs(ts)
+    out = {"lattice": list(ts), "precision": args.precision, "n_step": args.n_step, "halo": sl.halo,
+           "local_time_extent": sl.nt + 2 * sl.halo}
+
+    def run(form):
+        if form == "plain":
+            g = gf.copy()
+            step = lambda t: q.run_hmc_pure_gauge(g, ga, t, rs, n_step=args.n_step, is_always_accept=True,
+                                                  precision=args.precision)
+        else:
+            g = sl.gauge_field()
+            sl.set_rand(g, rs.split("gf-init"), 0.3, 1)
+            step = lambda t: q.run_hmc_pure_gauge_slabs(sl, g, ga, t, rs, n_step=args.n_step,
+                                                        is_always_accept=True, precision=args.precision)
+        dhs, ms = [], []
+        for t in range(1, args.warmup + 1):
+            step(t)
+        torch.cuda.synchronize()
+        for t in range(args.warmup + 1, args.warmup + 1 + args.trajs):
+            t0 = time.perf_counter()
+            dhs.append(step(t)[1])
+            torch.cuda.synchronize()
+            ms.append(round((time.perf_counter() - t0) * 1e3, 2))
+        out[form + "_ms_per_traj"] = ms
+        return 1e3 * len(ms) / sum(ms), dhs
+
+    for form in args.order.split(","):
+        out[form + "_traj_per_s"], dh = run(form)
+        if form == "plain":
+            dh_plain = dh
+        else:
+            dh_slab = dh
+    out["slab_over_plain"] = out["slab_traj_per_s"] / out["plain_traj_per_s"]
+    out["max_delta_h_difference"] = max(abs(a - b) for a, b in zip(dh_plain, dh_slab))
+    g32 = sl.gauge_field().copy(precision=q.F32 if args.precision == "mixed" else q.F64)
+    for _ in range(3):
+        sl.exchange(g32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(20):
+        sl.exchange(g32)
+    torch.cuda.synchronize()
+    n = ctypes.c_int64()
+    q._lib.call("qgb_field_tslice_bytes", g32.handle, sl.halo, ctypes.byref(n))
+    out["exchange_ms"] = (time.perf_counter() - t0) / 20 * 1e3
+    out["exchange_bytes_each_way"] = 2 * n.value
+    out["exchanges_per_traj"] = 2 * args.n_step + 2
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -288,9 +360,16 @@ def main():
     e.add_argument("--hmc-warmup", type=int, default=10)
     f = sub.add_parser("fma-peak")
     f.add_argument("--reps", type=int, default=5)
+    g = sub.add_parser("slabs")
+    g.add_argument("--lattice", default="24,24,24,64")
+    g.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    g.add_argument("--n-step", type=int, default=8)
+    g.add_argument("--trajs", type=int, default=5)
+    g.add_argument("--warmup", type=int, default=2)
+    g.add_argument("--order", default="plain,slab")
     args = ap.parse_args()
     {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch,
-     "flow-adjoint": flow_adjoint, "fma-peak": fma_peak}[args.cmd](args)
+     "flow-adjoint": flow_adjoint, "fma-peak": fma_peak, "slabs": slabs}[args.cmd](args)
 
 
 if __name__ == "__main__":

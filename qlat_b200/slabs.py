@@ -14,6 +14,11 @@ sites are correct as long as the halo slices are fresh copies:
   the owned slices when the halo is 4 slices deep and was refreshed just before
   it: one exchange per update;
 - the link updates are site-local and need no exchange;
+- the molecular dynamics is the library's own fused kernel sequence
+  (qgb_run_md_hooked), which calls back into ``exchange`` before each force
+  evaluation: the FP64 form, and the mixed form on FP32 copies of the links
+  and momenta (FP32 halos, half the bytes), run the kernels the single-GPU
+  trajectories run;
 - the Hamiltonians sum over the owned sites only and are then summed over
   ranks in FP64;
 - momenta and hot starts use the per-site random streams of the global site
@@ -29,11 +34,10 @@ library's kernels.
 from __future__ import annotations
 
 import ctypes
-import math
 
-from ._lib import call
-from .field import GaugeAction, GaugeField, GaugeMomentum, Geometry, RngState
-from .hmc import gf_evolve, gm_evolve_fg_pure_gauge, metropolis_accept, unitarize
+from ._lib import HALO_HOOK, call
+from .field import F32, GaugeAction, GaugeField, GaugeMomentum, Geometry, RngState
+from .hmc import INTEGRATORS, metropolis_accept, unitarize
 
 
 class TimeSlabs:
@@ -124,6 +128,29 @@ class TimeSlabs:
             w.wait()
         return rbot, rtop
 
+    def run_md(self, gm: GaugeMomentum, gf: GaugeField, ga: GaugeAction, n_step: int, md_time: float = 1.0, *,
+               integrator: str = "force-gradient", reunit_interval: int = 0) -> None:
+        """The molecular dynamics of one trajectory on the slab fields (FP64 or
+        FP32), with a halo exchange before every force evaluation."""
+        errors = []
+
+        def hook(handle, user):
+            try:
+                self.exchange(gf)
+                return 0
+            except BaseException as e:  # raised again below, after the library call returns
+                errors.append(e)
+                return 1
+
+        cb = HALO_HOOK(hook)
+        try:
+            call("qgb_run_md_hooked", gm.handle, gf.handle, ga.beta(), ga.c1(), int(n_step), float(md_time),
+                 INTEGRATORS[integrator], int(reunit_interval), cb, None)
+        except Exception:
+            if errors:
+                raise errors[0]
+            raise
+
     def glb_sum(self, x: float) -> float:
         """glb_sum (mpi.h:273-308): FP64 sum over the ranks."""
         if self.world == 1:
@@ -177,38 +204,41 @@ class TimeSlabs:
 
 
 def run_hmc_evolve_slabs(slabs: TimeSlabs, gm: GaugeMomentum, gf: GaugeField, ga: GaugeAction, n_step: int,
-                         md_time: float = 1.0) -> float:
+                         md_time: float = 1.0, *, integrator: str = "force-gradient", precision: str = "fp64",
+                         reunit_interval: int = 4) -> float:
     """run_hmc_evolve_pure_gauge (hmc.pyx:169-188) on time slabs: the same
-    Omelyan force-gradient steps, a halo exchange before each momentum update
-    and before the closing Hamiltonian; returns the global delta_h."""
+    Omelyan force-gradient steps with a halo exchange before each momentum
+    update, FP64 Hamiltonians over the owned sites summed over ranks; returns
+    the global delta_h.  ``precision`` "mixed" runs the molecular dynamics on
+    FP32 copies with FP64 re-unitarisation every ``reunit_interval`` steps, as
+    run_hmc_evolve_pure_gauge(precision="mixed") does on one GPU."""
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
     slabs.exchange(gf)
     energy = slabs.gm_hamilton(gm) + slabs.gf_hamilton(gf, ga)
-    dt = md_time / n_step
-    lam = 0.5 * (1.0 - 1.0 / math.sqrt(3.0))
-    theta = (2.0 - math.sqrt(3.0)) / 48.0
-    ttheta = theta * dt * dt * dt
-    gf_evolve(gf, gm, lam * dt)
-    for i in range(n_step):
-        slabs.exchange(gf)
-        gm_evolve_fg_pure_gauge(gm, gf, ga, 4.0 * ttheta / dt, 0.5 * dt)
-        gf_evolve(gf, gm, (1.0 - 2.0 * lam) * dt)
-        slabs.exchange(gf)
-        gm_evolve_fg_pure_gauge(gm, gf, ga, 4.0 * ttheta / dt, 0.5 * dt)
-        gf_evolve(gf, gm, (2.0 if i < n_step - 1 else 1.0) * lam * dt)
+    if precision == "fp64":
+        slabs.run_md(gm, gf, ga, n_step, md_time, integrator=integrator)
+    else:
+        gf32, gm32 = gf.copy(F32), gm.copy(F32)
+        slabs.run_md(gm32, gf32, ga, n_step, md_time, integrator=integrator, reunit_interval=reunit_interval)
+        gf @= gf32
+        gm @= gm32
     unitarize(gf)
     slabs.exchange(gf)
     return slabs.gm_hamilton(gm) + slabs.gf_hamilton(gf, ga) - energy
 
 
 def run_hmc_pure_gauge_slabs(slabs: TimeSlabs, gf: GaugeField, ga: GaugeAction, traj: int, rs: RngState, *,
-                             n_step: int = 6, md_time: float = 1.0, is_always_accept: bool = False):
+                             n_step: int = 6, md_time: float = 1.0, is_always_accept: bool = False,
+                             integrator: str = "force-gradient", precision: str = "fp64", reunit_interval: int = 4):
     """run_hmc_pure_gauge (hmc.pyx:190-216) on time slabs; every rank takes the
     same Metropolis decision from the global delta_h.  Returns (flag, delta_h)."""
     rs = rs.split(f"{traj}")
     gf0 = gf.copy()
     gm = slabs.gauge_momentum()
     slabs.set_rand_momentum(gm, rs.split("set_rand_gauge_momentum"), 1.0)
-    delta_h = run_hmc_evolve_slabs(slabs, gm, gf0, ga, n_step, md_time)
+    delta_h = run_hmc_evolve_slabs(slabs, gm, gf0, ga, n_step, md_time, integrator=integrator,
+                                   precision=precision, reunit_interval=reunit_interval)
     flag, _ = metropolis_accept(delta_h, traj, rs.split("metropolis_accept"))
     if flag or is_always_accept:
         gf @= gf0

@@ -242,3 +242,21 @@ def test_upload_pipelined(q):
         gf.upload_host_pipelined(bufs[0].data_ptr(), bufs[1].data_ptr())
         gf.upload_host_pipelined(bufs[2].data_ptr(), None)
         assert np.abs(np.asarray(gf) - bufs[2].numpy()).max() <= tol * 10
+
+
+@pytest.mark.gpu
+def test_field_storage_pool(q):
+    """A destroyed field's storage is pooled and reused by the next field of
+    its size, which still starts at zero; release_field_pool frees it."""
+    geo = q.Geometry((4, 4, 4, 8))
+    nbytes = 4 * 4 * 4 * 8 * 4 * 18 * 8  # 512 sites (a multiple of 32), 4 links, 18 doubles
+    q.release_field_pool()
+    f = q.GaugeField(geo)
+    f.set_rand(q.RngState("pool"), 0.5, 1)
+    del f
+    g = q.GaugeField(geo)  # takes the pooled block
+    assert not np.asarray(g).any()
+    assert q.release_field_pool() == 0
+    del g
+    assert q.release_field_pool() == nbytes
+    assert q.release_field_pool() == 0

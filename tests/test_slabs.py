@@ -7,8 +7,10 @@ instead of waiting for ever.
 GPU: a one-rank slab (its halo is its own periodic copy) and two ranks run as
 two processes on one GPU, exchanging halos through host memory over gloo (no
 kernel waits on another rank), both against the single-GPU trajectory of the
-whole lattice: the same links on every owned site, the same delta_h and the
-same accept / reject decisions.
+whole lattice, in the FP64 and the mixed FP32/FP64 forms: the same links on
+every owned site, the same delta_h and the same accept / reject decisions.  A
+halo exchange that raises inside the library's trajectory ends the call with
+its exception.
 """
 
 import json
@@ -78,7 +80,7 @@ def test_halo_ring_on_gloo_ranks(tmp_path, world):
 # ---- GPU ------------------------------------------------------------------------------------
 
 
-def _global_run(q):
+def _global_run(q, precision="fp64"):
     """The single-GPU reference: hot start and N_TRAJ trajectories of the whole lattice."""
     ga = q.GaugeAction(BETA, C1)
     rs = q.RngState("slabs")
@@ -86,12 +88,13 @@ def _global_run(q):
     gf.set_rand(rs.split("gf-init"), 0.3, 1)
     rows = []
     for traj in range(1, N_TRAJ + 1):
-        flag, dh = q.run_hmc_pure_gauge(gf, ga, traj, rs.split("hmc"), n_step=N_STEP, is_always_accept=traj < 2)
+        flag, dh = q.run_hmc_pure_gauge(gf, ga, traj, rs.split("hmc"), n_step=N_STEP, is_always_accept=traj < 2,
+                                        precision=precision)
         rows.append([bool(flag), dh, q.gf_avg_plaq(gf)])
     return rows, np.asarray(gf)
 
 
-def _slab_run(q, slabs):
+def _slab_run(q, slabs, precision="fp64"):
     ga = q.GaugeAction(BETA, C1)
     rs = q.RngState("slabs")
     gf = slabs.gauge_field()
@@ -99,7 +102,7 @@ def _slab_run(q, slabs):
     rows = []
     for traj in range(1, N_TRAJ + 1):
         flag, dh = q.run_hmc_pure_gauge_slabs(slabs, gf, ga, traj, rs.split("hmc"), n_step=N_STEP,
-                                              is_always_accept=traj < 2)
+                                              is_always_accept=traj < 2, precision=precision)
         slabs.exchange(gf)
         rows.append([bool(flag), dh, slabs.plaq(gf)])
     return rows, slabs.owned_slices(np.asarray(gf))
@@ -115,14 +118,42 @@ def _compare(rows, ref_rows, links, ref_links, t0, nt):
 
 
 @pytest.mark.gpu
-def test_one_rank_slab_matches_global(q):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_rank_slab_matches_global(q, precision):
     slabs = q.TimeSlabs(TS)
-    rows, links = _slab_run(q, slabs)
-    ref_rows, ref_links = _global_run(q)
+    rows, links = _slab_run(q, slabs, precision)
+    ref_rows, ref_links = _global_run(q, precision)
     _compare(rows, ref_rows, links, ref_links, 0, TS[3])
 
 
-def _slab_main(rank, world, port, out_dir):
+@pytest.mark.gpu
+def test_halo_hook_error_aborts_trajectory(q):
+    """An exchange that fails inside the library's trajectory (the third halo
+    refresh raises) ends the call with that exception; the library stays
+    usable afterwards."""
+
+    class Failing(q.TimeSlabs):
+        calls = 0
+
+        def exchange(self, f):
+            Failing.calls += 1
+            if Failing.calls == 3:
+                raise ConnectionError("peer gone")
+            super().exchange(f)
+
+    slabs = Failing(TS)
+    ga = q.GaugeAction(BETA, C1)
+    gf = slabs.gauge_field()
+    slabs.set_rand(gf, q.RngState("hook"), 0.3, 1)  # exchange call 1
+    gm = slabs.gauge_momentum()
+    slabs.set_rand_momentum(gm, q.RngState("hook-gm"), 1.0)
+    with pytest.raises(ConnectionError):
+        slabs.run_md(gm, gf, ga, N_STEP)  # calls 2 and 3 are the hook's
+    assert Failing.calls == 3
+    assert np.isfinite(slabs.plaq(gf))
+
+
+def _slab_main(rank, world, port, out_dir, precision):
     import datetime
 
     import torch
@@ -134,7 +165,7 @@ def _slab_main(rank, world, port, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         slabs = q.TimeSlabs(TS)
-        rows, links = _slab_run(q, slabs)
+        rows, links = _slab_run(q, slabs, precision)
         np.save(os.path.join(out_dir, f"links{rank}.npy"), links)
         with open(os.path.join(out_dir, f"rows{rank}.json"), "w") as f:
             json.dump({"t0": slabs.t0, "nt": slabs.nt, "rows": rows}, f)
@@ -143,10 +174,12 @@ def _slab_main(rank, world, port, out_dir):
 
 
 @pytest.mark.gpu
-def test_two_rank_slabs_match_global(q, tmp_path):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_two_rank_slabs_match_global(q, tmp_path, precision):
     import torch.multiprocessing as mp
-    mp.start_processes(_slab_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True, start_method="spawn")
-    ref_rows, ref_links = _global_run(q)
+    mp.start_processes(_slab_main, args=(2, _free_port(), str(tmp_path), precision), nprocs=2, join=True,
+                       start_method="spawn")
+    ref_rows, ref_links = _global_run(q, precision)
     for r in range(2):
         g = json.load(open(tmp_path / f"rows{r}.json"))
         _compare(g["rows"], ref_rows, np.load(tmp_path / f"links{r}.npy"), ref_links, g["t0"], g["nt"])
