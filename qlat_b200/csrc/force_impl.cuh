@@ -114,26 +114,7 @@ __device__ __forceinline__ M3<R> staple_sum_rt(const CField<R>& U, const Geo& g,
 // - hop(x) and U_mu(x+e), each used twice per direction, loaded once.
 // Offsets are 32-bit: the launcher uses this form only when 36 V < 2^31.
 
-template <typename R>
-struct LinkLd {
-  const Cx<R>* __restrict__ p;
-  int nblk;  // 32-site blocks of the field
-  __device__ __forceinline__ M3<R> operator()(int link, int site) const
-  {
-    const Cx<R>* q = p + (((link * nblk + (site >> 5)) * 9) * 32 + (site & 31));
-    M3<R> r;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + 32 * k);
-    return r;
-  }
-};
-
-__device__ __forceinline__ int sel4(const int (&v)[4], int k)
-{
-  return k == 0 ? v[0] : k == 1 ? v[1] : k == 2 ? v[2] : v[3];
-}
-
-__device__ __forceinline__ int nb_delta(int xk, int a, int L, int stride) { return (wrap(xk + a, L) - xk) * stride; }
+// LinkLd, sel4 and nb_delta: gauge_common.cuh.
 
 // One signed direction e = SG nu.  dn1 = D_nu(SG), dn2 = D_nu(2 SG).
 // Stored links: hop(x + a mu + b e) is U_nu at D_nu(b) (SG > 0) or U_nu^+ at

@@ -152,4 +152,30 @@ __device__ __forceinline__ Geo chain_geo(const ChainInfo& c)
   return g;
 }
 
+// Link loads by 32-bit link and site indices (kernels that compute neighbour
+// sites as the thread's own site plus per-direction offsets; valid while
+// 36 * padded_sites(V) < 2^31):
+// site(x + a mu + b nu) = site(x) + D_mu(a) + D_nu(b) for mu != nu, with
+// D_k(a) = nb_delta(x_k, a, L_k, stride_k).
+template <typename R>
+struct LinkLd {
+  const Cx<R>* __restrict__ p;
+  int nblk;  // 32-site blocks of the field
+  __device__ __forceinline__ M3<R> operator()(int link, int site) const
+  {
+    const Cx<R>* q = p + (((link * nblk + (site >> 5)) * 9) * 32 + (site & 31));
+    M3<R> r;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + 32 * k);
+    return r;
+  }
+};
+
+__device__ __forceinline__ int sel4(const int (&v)[4], int k)
+{
+  return k == 0 ? v[0] : k == 1 ? v[1] : k == 2 ? v[2] : v[3];
+}
+
+__device__ __forceinline__ int nb_delta(int xk, int a, int L, int stride) { return (wrap(xk + a, L) - xk) * stride; }
+
 }  // namespace qgb

@@ -394,8 +394,52 @@ QGB_HD void rng_split_long(Rng& out, const Rng& rs0, int64_t sindex)
 // New cache block of rand_gen: SHA-256 of "[index]" (or "[type,index]")
 // appended to the state, with the already advanced index; caches three of the
 // four 64-bit words and returns the fourth.
+// The block of an untyped state, built in registers: "[" dec(index) "]"
+// (at most 22 bytes) and the 0x80 pad byte fill words 0-5 from the left,
+// words 14-15 hold the message length in bits.
+QGB_HD void refill_words_untyped(uint32_t w[16], uint64_t index, uint64_t numBytes)
+{
+  int nd = 1;
+  for (uint64_t t = index; t >= 10; t /= 10) ++nd;
+  uint64_t q0 = (uint64_t)'[' << 56, q1 = 0, q2 = 0;  // bytes 0-7, 8-15, 16-23, big-endian
+  auto put = [&](int p, uint64_t byte) {
+    const uint64_t v = byte << (56 - 8 * (p & 7));
+    if (p < 8) q0 |= v;
+    else if (p < 16) q1 |= v;
+    else q2 |= v;
+  };
+  uint64_t v = index;
+  for (int p = nd; p >= 1; --p) {
+    put(p, '0' + v % 10);
+    v /= 10;
+  }
+  put(nd + 1, ']');
+  put(nd + 2, 0x80);
+  const uint64_t bits = 8 * (numBytes + (uint64_t)(nd + 2));
+  w[0] = (uint32_t)(q0 >> 32);
+  w[1] = (uint32_t)q0;
+  w[2] = (uint32_t)(q1 >> 32);
+  w[3] = (uint32_t)q1;
+  w[4] = (uint32_t)(q2 >> 32);
+  w[5] = (uint32_t)q2;
+#pragma unroll
+  for (int i = 6; i < 14; ++i) w[i] = 0;
+  w[14] = (uint32_t)(bits >> 32);
+  w[15] = (uint32_t)bits;
+}
+
 QGB_HD uint64_t rng_refill(Rng& rs)
 {
+  uint32_t w[16], h[8];
+  if (rs.type == RNG_NO_TYPE) {
+    refill_words_untyped(w, rs.index, rs.numBytes);
+    sha256_compress(h, rs.hash, w);
+    rs.cache[0] = ((uint64_t)h[0] << 32) | h[1];
+    rs.cache[1] = ((uint64_t)h[2] << 32) | h[3];
+    rs.cache[2] = ((uint64_t)h[4] << 32) | h[5];
+    rs.cacheAvail = 3;
+    return ((uint64_t)h[6] << 32) | h[7];
+  }
   uint8_t blk[64];
   for (int i = 0; i < 64; ++i) blk[i] = 0;
   int n = 0;
@@ -409,7 +453,6 @@ QGB_HD uint64_t rng_refill(Rng& rs)
   blk[n] = 0x80;
   const uint64_t bits = 8 * (rs.numBytes + (uint64_t)n);
   for (int i = 0; i < 8; ++i) blk[63 - i] = (uint8_t)(bits >> (8 * i));
-  uint32_t w[16], h[8];
   bytes_to_words(w, blk);
   sha256_compress(h, rs.hash, w);
   rs.cache[0] = ((uint64_t)h[0] << 32) | h[1];
@@ -419,16 +462,30 @@ QGB_HD uint64_t rng_refill(Rng& rs)
   return ((uint64_t)h[6] << 32) | h[7];
 }
 
+// Takes cache[--cacheAvail] and clears it, with constant indices (a
+// run-time index would put the cache in local memory).
+QGB_HD uint64_t rng_cache_pop(Rng& rs)
+{
+  const int k = --rs.cacheAvail;
+  uint64_t r;
+  if (k == 2) {
+    r = rs.cache[2];
+    rs.cache[2] = 0;
+  } else if (k == 1) {
+    r = rs.cache[1];
+    rs.cache[1] = 0;
+  } else {
+    r = rs.cache[0];
+    rs.cache[0] = 0;
+  }
+  return r;
+}
+
 // rand_gen (rng-state.cpp:215-238)
 QGB_HD uint64_t rng_rand_gen(Rng& rs)
 {
   rs.index += 1;
-  if (rs.cacheAvail > 0) {
-    rs.cacheAvail -= 1;
-    const uint64_t r = rs.cache[rs.cacheAvail];
-    rs.cache[rs.cacheAvail] = 0;
-    return r;
-  }
+  if (rs.cacheAvail > 0) return rng_cache_pop(rs);
   return rng_refill(rs);
 }
 
@@ -541,10 +598,7 @@ __device__ __forceinline__ void rng_gaussians_converged(Rng& rs, double sigma, b
       }
       rs.index += 1;  // rand_gen
       if (rs.cacheAvail > 0) {
-        rs.cacheAvail -= 1;
-        const uint64_t u = rs.cache[rs.cacheAvail];
-        rs.cache[rs.cacheAvail] = 0;
-        consume(u);
+        consume(rng_cache_pop(rs));
       } else {
         need = true;
       }
