@@ -1282,23 +1282,31 @@ int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c
   QGB_RC(get_scratch(b32, 11, &gf32));
   QGB_RC(get_scratch(b32, 12, &gm32));
   QGB_RC(get_scratch(b32, 13, &tmp32));
-  QGB_RC(hamiltonian_slots(gm, gf, c1, 0));
-  const long n = n_store(gf);
+  // H0's two sums, each writing the FP32 copy of its field in the same pass
+  const int nb = qgb::reduce_blocks(g);
+  QGB_RC(ensure_partials((size_t)nb * 2));
   {
-    Prof p("convert", 2);
-    QGB_TRY_CUDA((qgb::launch_convert<double, float>(n, gf->d, gf32, g_ctx.stream)));
-    QGB_TRY_CUDA((qgb::launch_convert<double, float>(n, gm->d, gm32, g_ctx.stream)));
+    Prof p("reduce", 4);
+    QGB_TRY_CUDA((qgb::launch_gm_hamilton_convert<double, float>(g, gm->d, gm32, g_ctx.partials, g_ctx.stream)));
+    QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 0, g_ctx.stream));
+    QGB_TRY_CUDA(qgb::launch_action<double>(g, gf->d, c1 != 0.0, g_ctx.partials, g_ctx.stream, gf32));
+    QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, c1 != 0.0 ? 2 : 1, nb, g_ctx.results, 1, g_ctx.stream));
   }
   const int unit_each = reunit_interval > 0 ? 0 : 1;
   QGB_RC(md_trajectory<float>(g, gf32, gm32, tmp32, beta, c1, n_step, md_time, integrator, unit_each,
                               reunit_interval));
+  // back to FP64: the links unitarised in the same pass, the momenta with H1's
+  // kinetic sum
   {
-    Prof p("convert", 2);
-    QGB_TRY_CUDA((qgb::launch_convert<float, double>(n, gf32, gf->d, g_ctx.stream)));
-    QGB_TRY_CUDA((qgb::launch_convert<float, double>(n, gm32, gm->d, g_ctx.stream)));
+    Prof p("unitarize");
+    QGB_TRY_CUDA(qgb::launch_unitarize_to_f64(g, gf32, gf->d, g_ctx.stream));
   }
-  QGB_RC(qgb_unitarize(gf));
-  QGB_RC(hamiltonian_slots(gm, gf, c1, 3));
+  {
+    Prof p("reduce", 2);
+    QGB_TRY_CUDA((qgb::launch_gm_hamilton_convert<float, double>(g, gm32, gm->d, g_ctx.partials, g_ctx.stream)));
+    QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 3, g_ctx.stream));
+  }
+  QGB_RC(action_slot(gf, c1 != 0.0, 4));
   double r[6];
   QGB_RC(read_results(0, 6, r));
   const double e0 = r[0] + gf_hamilton_from(r[1], r[2], beta, c1);

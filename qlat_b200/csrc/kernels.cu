@@ -176,6 +176,69 @@ cudaError_t launch_gm_hamilton(const Geo& g, const void* P, double* partials, cu
   return cudaGetLastError();
 }
 
+// Threads cover the padded sites too (reduce_blocks(g) blocks of RED_BS span
+// padded_sites(V), RED_BS being a multiple of 32), so Q's padding is written
+// (with the zeros of P's).  The sum uses the FP64 one of the two matrices, so
+// it equals k_gm_hamilton<double> on the FP64 field bit for bit.
+template <typename RI, typename RO>
+__global__ void __launch_bounds__(RED_BS) k_gm_hamilton_convert(Geo g, const Cx<RI>* P, Cx<RO>* Q, double* partials)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (s < padded_sites(g.V)) {
+    const CField<RI> Pf{P, g.V};
+    const WField<RO> Qf{Q, g.V};
+    const bool sum = s < g.V && in_reduce(g, s);
+#pragma unroll 1
+    for (int mu = 0; mu < 4; ++mu) {
+      const M3<RI> p = Pf.ld(s, mu);
+      M3<RO> q;
+      M3<double> d;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        q.e[k] = cx<RO>((RO)p.e[k].re, (RO)p.e[k].im);
+        d.e[k] = sizeof(RI) == 8 ? cx<double>((double)p.e[k].re, (double)p.e[k].im)
+                                 : cx<double>((double)q.e[k].re, (double)q.e[k].im);
+      }
+      Qf.st(s, mu, q);
+      if (sum) v[0] += neg_half_tr_square(d);
+    }
+  }
+  block_reduce_store<1>(v, partials);
+}
+
+template <typename RI, typename RO>
+cudaError_t launch_gm_hamilton_convert(const Geo& g, const void* P, void* Q, double* partials, cudaStream_t st)
+{
+  k_gm_hamilton_convert<RI, RO><<<reduce_blocks(g), RED_BS, 0, st>>>(g, (const Cx<RI>*)P, (Cx<RO>*)Q, partials);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) k_unitarize_to_f64(long V, const Cx<float>* P, Cx<double>* Q)
+{
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= padded_sites(V)) return;
+  const CField<float> Pf{P, V};
+  const WField<double> Qf{Q, V};
+#pragma unroll 1
+  for (int mu = 0; mu < 4; ++mu) {
+    const M3<float> p = Pf.ld(s, mu);
+    M3<double> u;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) u.e[k] = cx<double>((double)p.e[k].re, (double)p.e[k].im);
+    if (s < V) unitarize_as<double, double>(u);
+    Qf.st(s, mu, u);
+  }
+}
+
+cudaError_t launch_unitarize_to_f64(const Geo& g, const void* P, void* Q, cudaStream_t st)
+{
+  const int bs = 256;
+  k_unitarize_to_f64<<<(unsigned)((padded_sites(g.V) + bs - 1) / bs), bs, 0, st>>>(g.V, (const Cx<float>*)P,
+                                                                                  (Cx<double>*)Q);
+  return cudaGetLastError();
+}
+
 // Sums over the 6 planes mu < nu at x of (Re tr plaq - 3) and, with RECT, of
 // (Re tr rect - 3) for both rectangle orientations (hmc.cpp:9-25,203-252):
 // plaq = A B^+ with A = U_mu(x) U_nu(x+mu), B = U_nu(x) U_mu(x+nu);
@@ -226,11 +289,26 @@ __global__ void __launch_bounds__(RED_BS) k_action(Geo g, const Cx<R>* Up, doubl
 // (24^3 x 64 on B200: FP64 0.56 ms with the double link recomputed against
 // 0.59 ms shared, FP32 0.31 ms shared against 0.34 ms; 0.79 / 0.53 ms for
 // k_action).
+// With copy != nullptr each thread also writes its site's links, converted to
+// FP32, into copy (padded sites included, with zeros).
 template <typename R, bool RECT>
-__global__ void __launch_bounds__(RED_BS, 2) k_action_loops(Geo g, const Cx<R>* Up, double* partials)
+__global__ void __launch_bounds__(RED_BS, 2) k_action_loops(Geo g, const Cx<R>* Up, double* partials,
+                                                            Cx<float>* copy)
 {
   constexpr bool SHARE = sizeof(R) == 4;
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (copy != nullptr && s < padded_sites(g.V)) {
+    const CField<R> Uf{Up, g.V};
+    const WField<float> Cf{copy, g.V};
+#pragma unroll 1
+    for (int mu = 0; mu < 4; ++mu) {
+      const M3<R> u = Uf.ld(s, mu);
+      M3<float> c;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) c.e[k] = cx<float>((float)u.e[k].re, (float)u.e[k].im);
+      Cf.st(s, mu, c);
+    }
+  }
   double v[2] = {0.0, 0.0};
   if (s < g.V && in_reduce(g, s)) {
     const LinkLd<R> L{Up, (int)site_blocks(g.V)};
@@ -279,15 +357,17 @@ __global__ void __launch_bounds__(RED_BS, 2) k_action_loops(Geo g, const Cx<R>* 
 }
 
 template <typename R>
-cudaError_t launch_action(const Geo& g, const void* U, int rect, double* partials, cudaStream_t st)
+cudaError_t launch_action(const Geo& g, const void* U, int rect, double* partials, cudaStream_t st, void* copy_f32)
 {
   const Cx<R>* u = (const Cx<R>*)U;
+  Cx<float>* c = (Cx<float>*)copy_f32;
   if (padded_sites(g.V) * 36 < 2147483647L) {
-    if (rect) k_action_loops<R, true><<<reduce_blocks(g), RED_BS, 0, st>>>(g, u, partials);
-    else k_action_loops<R, false><<<reduce_blocks(g), RED_BS, 0, st>>>(g, u, partials);
+    if (rect) k_action_loops<R, true><<<reduce_blocks(g), RED_BS, 0, st>>>(g, u, partials, c);
+    else k_action_loops<R, false><<<reduce_blocks(g), RED_BS, 0, st>>>(g, u, partials, c);
   } else {  // 32-bit link offsets would overflow
     if (rect) k_action<R, true><<<reduce_blocks(g), RED_BS, 0, st>>>(g, u, partials);
     else k_action<R, false><<<reduce_blocks(g), RED_BS, 0, st>>>(g, u, partials);
+    if (c != nullptr) return launch_convert<R, float>(padded_sites(g.V) * 4 * 18, U, c, st);
   }
   return cudaGetLastError();
 }
@@ -1009,7 +1089,7 @@ cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st)
 #define QGB_INST(R)                                                                                          \
   template cudaError_t launch_evolve<R>(const Geo&, void*, const void*, double, int, int, cudaStream_t);    \
   template cudaError_t launch_gm_hamilton<R>(const Geo&, const void*, double*, cudaStream_t);              \
-  template cudaError_t launch_action<R>(const Geo&, const void*, int, double*, cudaStream_t);              \
+  template cudaError_t launch_action<R>(const Geo&, const void*, int, double*, cudaStream_t, void*);       \
   template cudaError_t launch_clover<R>(const Geo&, const void*, void*, void*, double*, cudaStream_t);     \
   template cudaError_t launch_topology_5li<R>(const Geo&, const void*, void*, void*, double*, cudaStream_t); \
   template cudaError_t launch_qnorm<R>(long, const void*, double*, int, cudaStream_t);                    \
@@ -1025,6 +1105,8 @@ QGB_INST(float)
 template cudaError_t launch_unitarize<double, double>(const Geo&, int, void*, cudaStream_t);
 template cudaError_t launch_unitarize<float, float>(const Geo&, int, void*, cudaStream_t);
 template cudaError_t launch_unitarize<float, double>(const Geo&, int, void*, cudaStream_t);
+template cudaError_t launch_gm_hamilton_convert<double, float>(const Geo&, const void*, void*, double*, cudaStream_t);
+template cudaError_t launch_gm_hamilton_convert<float, double>(const Geo&, const void*, void*, double*, cudaStream_t);
 template cudaError_t launch_convert<double, float>(long, const void*, void*, cudaStream_t);
 template cudaError_t launch_convert<float, double>(long, const void*, void*, cudaStream_t);
 template cudaError_t launch_convert<double, double>(long, const void*, void*, cudaStream_t);

@@ -83,9 +83,17 @@ cudaError_t launch_unitarize(const Geo& g, int m, void* U, cudaStream_t st);
 int reduce_blocks(const Geo& g);
 template <typename R>
 cudaError_t launch_gm_hamilton(const Geo& g, const void* P, double* partials, cudaStream_t st);
+// The same sum (taken on the FP64 one of P and Q) and Q = P converted from RI
+// to RO on every stored site, in one pass.
+template <typename RI, typename RO>
+cudaError_t launch_gm_hamilton_convert(const Geo& g, const void* P, void* Q, double* partials, cudaStream_t st);
+// Q = unitarize(P) with FP64 arithmetic, P FP32 and Q FP64 (the conversion and
+// k_unitarize<double, double> in one pass).
+cudaError_t launch_unitarize_to_f64(const Geo& g, const void* P, void* Q, cudaStream_t st);
 // values: 0 = sum(ReTr plaq - 3), 1 = sum(ReTr rect - 3) (if rect)
 template <typename R>
-cudaError_t launch_action(const Geo& g, const void* U, int rect, double* partials, cudaStream_t st);
+cudaError_t launch_action(const Geo& g, const void* U, int rect, double* partials, cudaStream_t st,
+                          void* copy_f32 = nullptr);
 // values: 0 = energy density sum, 1 = clover topological charge sum; optional fields
 template <typename R>
 cudaError_t launch_clover(const Geo& g, const void* U, void* e_field, void* q_field, double* partials,
