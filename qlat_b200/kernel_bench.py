@@ -18,6 +18,11 @@
         one chain as a one-rank time slab (4 halo slices each side, a halo refresh before every
         force evaluation) against the plain single-GPU trajectory: traj/s and the exchange time
 
+    python -m qlat_b200.kernel_bench functions hmc|flow [--lattice ...] [--reps 20]
+        seconds per call of single API functions (hmc: 24^3x64 Iwasaki set_gm_force, gf_evolve,
+        the Hamiltonians, the momentum draw, unitarize, gf_avg_plaq; flow: 32^4 RK3 Wilson flow step,
+        energy density, clover and 5-loop charges), each call synchronised
+
 Each command prints one JSON line.
 """
 
@@ -323,6 +328,53 @@ def slabs(args):
     print(json.dumps(out))
 
 
+def functions(args):
+    """Per-call time of single API functions, as a user calls them (launch,
+    kernels and, for the scalar results, the read-back; a synchronisation
+    after every call), on the hot start set_rand(RngState(name).split("gf-init"),
+    sigma, 1)."""
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    hmc = args.set == "hmc"
+    ts = _lattice(args.lattice or ("24,24,24,64" if hmc else "32,32,32,32"))
+    rs = q.RngState("b200-c2-24x64-iwasaki" if hmc else "b200-c3-32x32-flow")
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(rs.split("gf-init"), 0.3 if hmc else 0.5, 1)
+    out = {"set": args.set, "lattice": list(ts), "reps": args.reps}
+
+    def per_call(fn):
+        for _ in range(2):
+            fn()
+        q.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            fn()
+            q.synchronize()
+        return (time.perf_counter() - t0) / args.reps
+
+    if hmc:
+        ga = q.GaugeAction(2.13, -0.331)
+        q.autotune_force(gf, ga.c1())
+        gm = q.GaugeMomentum(gf.geo)
+        gm.set_rand(rs.split("1").split("set_rand_gauge_momentum"), 1.0)
+        force = q.GaugeMomentum(gf.geo)
+        out["set_gm_force"] = per_call(lambda: q.set_gm_force(force, gf, ga))
+        out["gf_evolve"] = per_call(lambda: q.gf_evolve(gf, gm, 1e-3))
+        out["gm_hamilton_node"] = per_call(lambda: q.gm_hamilton_node(gm))
+        out["gf_hamilton_node"] = per_call(lambda: q.gf_hamilton_node(gf, ga))
+        out["set_rand_gauge_momentum"] = per_call(
+            lambda: gm.set_rand(rs.split("2").split("set_rand_gauge_momentum"), 1.0))
+        out["unitarize"] = per_call(lambda: q.unitarize(gf))
+        out["gf_avg_plaq"] = per_call(lambda: q.gf_avg_plaq(gf))
+    else:
+        out["gf_wilson_flow_step"] = per_call(lambda: q.gf_wilson_flow_step(gf, 0.05, c1=0.0))
+        out["gf_energy_density"] = per_call(lambda: q.gf_energy_density(gf))
+        out["clf_topology_sum"] = per_call(lambda: q.gf_topology_clf(gf))
+        out["topology_charge_5"] = per_call(lambda: q.topology_charge_5(gf))
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -367,9 +419,13 @@ def main():
     g.add_argument("--trajs", type=int, default=5)
     g.add_argument("--warmup", type=int, default=2)
     g.add_argument("--order", default="plain,slab")
+    h = sub.add_parser("functions")
+    h.add_argument("set", choices=["hmc", "flow"])
+    h.add_argument("--lattice", default=None)
+    h.add_argument("--reps", type=int, default=20)
     args = ap.parse_args()
     {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch,
-     "flow-adjoint": flow_adjoint, "fma-peak": fma_peak, "slabs": slabs}[args.cmd](args)
+     "flow-adjoint": flow_adjoint, "fma-peak": fma_peak, "slabs": slabs, "functions": functions}[args.cmd](args)
 
 
 if __name__ == "__main__":
