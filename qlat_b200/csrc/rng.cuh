@@ -160,15 +160,17 @@ QGB_HD double log_cr(double x, int* ambiguous)
   const DD s = dd_fast_two_sum(sh, QGB_DDIV(r, sum.hi));
   // z = s^2
   const DD z = dd_mul(s, s);
-  // q = z/3 + z^2/5 + z^3 (1/7 + z (1/9 + z (1/11 + z/13)))
-  const DD third = dd_fast_two_sum(QGB_DDIV(1.0, 3.0), QGB_DDIV(QGB_DFMA(-QGB_DDIV(1.0, 3.0), 3.0, 1.0), 3.0));
-  const DD fifth = dd_fast_two_sum(QGB_DDIV(1.0, 5.0), QGB_DDIV(QGB_DFMA(-QGB_DDIV(1.0, 5.0), 5.0, 1.0), 5.0));
+  // q = z/3 + z^2/5 + z^3 (1/7 + z (1/9 + z (1/11 + z/13))); the
+  // coefficients are generated constants (gen_log_table.py): 1/3 and 1/5 as
+  // (RN(1/k), RN((1 - k RN(1/k))/k)), the others RN(1/k)
+  const DD third = dd_fast_two_sum(QGB_INV3_HI, QGB_INV3_LO);
+  const DD fifth = dd_fast_two_sum(QGB_INV5_HI, QGB_INV5_LO);
   const DD q1 = dd_mul(z, third);
   const DD z2 = dd_mul(z, z);
   const DD q2 = dd_mul(z2, fifth);
-  double t = QGB_DADD(QGB_DDIV(1.0, 11.0), QGB_DMUL(z.hi, QGB_DDIV(1.0, 13.0)));
-  t = QGB_DADD(QGB_DDIV(1.0, 9.0), QGB_DMUL(z.hi, t));
-  t = QGB_DADD(QGB_DDIV(1.0, 7.0), QGB_DMUL(z.hi, t));
+  double t = QGB_DADD(QGB_INV11_HI, QGB_DMUL(z.hi, QGB_INV13_HI));
+  t = QGB_DADD(QGB_INV9_HI, QGB_DMUL(z.hi, t));
+  t = QGB_DADD(QGB_INV7_HI, QGB_DMUL(z.hi, t));
   t = QGB_DMUL(QGB_DMUL(z2.hi, z.hi), t);
   DD q = dd_add(q1, q2);
   q = dd_add(q, DD{t, 0.0});

@@ -167,3 +167,33 @@ def test_gf_utils_topology_log(q, goldens):
         q5 = q.gf_topology(gf)
         assert abs(q5 - g["topo_5li"][t]) < g["eps_topo"] * max(1.0, abs(q5)), (t, q5)
         assert abs(q.gf_topology_terms(gf).sum() - g["topo_5li_terms_sum"][t]) < g["eps_topo"] * max(1.0, abs(q5))
+
+
+@pytest.mark.parametrize("ts", [(6, 6, 6, 12), (3, 5, 7, 4)])
+def test_mixed_trajectory_equals_its_steps(q, ts):
+    """The mixed trajectory, whose H0 / H1 kernels also convert the fields,
+    equals the same steps run one by one (FP64 Hamiltonians, FP32 copies,
+    FP32 molecular dynamics with re-unitarisation every 4 steps, copies back,
+    unitarize, FP64 Hamiltonians) bit for bit: delta_h, links and momenta.
+    3 x 5 x 7 x 4 has a partly filled last block of 32 sites."""
+    import ctypes
+    from qlat_b200._lib import HALO_HOOK, call
+    ga = q.GaugeAction(2.13, -0.331)
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("mixed-steps").split("gf-init"), 0.3, 1)
+    gm = q.GaugeMomentum(gf.geo)
+    gm.set_rand(q.RngState("mixed-steps").split("mom"), 1.0)
+    g1, m1 = gf.copy(), gm.copy()
+    dh = q.run_hmc_evolve_pure_gauge(m1, g1, ga, None, 8, 1.0, precision="mixed", reunit_interval=4)
+    g2, m2 = gf.copy(), gm.copy()
+    h0 = q.gm_hamilton_node(m2) + q.gf_hamilton_node(g2, ga)
+    g32, m32 = g2.copy(precision=q.F32), m2.copy(precision=q.F32)
+    call("qgb_run_md_hooked", m32.handle, g32.handle, ga.beta(), ga.c1(), 8, 1.0, 0, 4,
+         ctypes.cast(None, HALO_HOOK), None)
+    g2 @= g32
+    m2 @= m32
+    q.unitarize(g2)
+    h1 = q.gm_hamilton_node(m2) + q.gf_hamilton_node(g2, ga)
+    assert dh == h1 - h0
+    assert np.array_equal(np.asarray(g1), np.asarray(g2))
+    assert np.array_equal(np.asarray(m1), np.asarray(m2))
