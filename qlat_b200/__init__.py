@@ -108,6 +108,13 @@ def force_set_variant(precision: int, rect: bool, variant: int):
     from ._lib import call
     call("qgb_force_set_variant", int(precision), int(bool(rect)), int(variant))
 
+def force_get_variant(precision: int, rect: bool) -> int:
+    import ctypes
+    from ._lib import call
+    v = ctypes.c_int32()
+    call("qgb_force_get_variant", int(precision), int(bool(rect)), ctypes.byref(v))
+    return int(v.value)
+
 
 def autotune_force(gf, c1: float, reps: int = 3):
     """Time every force-kernel variant on gf (its precision) and keep the

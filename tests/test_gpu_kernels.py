@@ -204,6 +204,7 @@ def test_every_force_variant(q, oracle, prec):
         Fr[c1] = oracle.new_field(ts)
         oracle.set_gm_force(Fr[c1], ref, ts, 2.0, c1)
     P = q.F64 if prec == "f64" else q.F32
+    saved = {rect: q.force_get_variant(P, rect) for rect in (False, True)}
     try:
         for v in range(len(q.force_variants())):
             for c1 in (0.0, -0.331):
@@ -212,8 +213,8 @@ def test_every_force_variant(q, oracle, prec):
                 q.set_gm_force(F, g, q.GaugeAction(2.0, c1))
                 assert nrel(np.asarray(F), Fr[c1]) < tol, (v, c1)
     finally:
-        q.force_set_variant(P, False, 0)
-        q.force_set_variant(P, True, 0)
+        for rect, v in saved.items():
+            q.force_set_variant(P, rect, v)
 
 
 @pytest.mark.gpu
