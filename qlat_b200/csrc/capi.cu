@@ -100,11 +100,12 @@ struct Ctx {
 Ctx g_ctx;
 int64_t g_launches = 0;  // kernels launched by this library
 // force-kernel launch variant per [precision: 0 = FP64, 1 = FP32][rect]; the
-// defaults are the fastest on B200 at 24^3 x 64 (FP64: 128 threads x 3 blocks
-// per SM for the plaquette force, 256 x 1 for Iwasaki; FP32: 128 x 4 with
-// two-row chains), so callers that never run the autotuner (the reference's
-// API has no such call) start from them
-int g_force_variant[2][2] = {{6, 5}, {10, 10}};
+// defaults are the fastest on B200 at 24^3 x 64 and 32^4 (FP64: 128 threads x
+// 3 blocks per SM for the plaquette force, 256 x 1 for Iwasaki; FP32, two-row
+// chains: 128 x 8 for the plaquette force, 128 x 4 for Iwasaki), so callers
+// that never run the autotuner (the reference's API has no such call) start
+// from them
+int g_force_variant[2][2] = {{6, 5}, {13, 10}};
 
 int ensure_ctx()
 {

@@ -357,8 +357,11 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
   X(7, 128, 1, 1, 3)          \
   X(8, 256, 1, 1, 3)          \
   X(9, 128, 3, 1, 3)          \
-  X(10, 128, 4, 1, 3)
-static const int N_FORCE_VARIANTS = 11;
+  X(10, 128, 4, 1, 3)         \
+  X(11, 128, 5, 1, 3)         \
+  X(12, 128, 6, 1, 3)         \
+  X(13, 128, 8, 1, 3)
+static const int N_FORCE_VARIANTS = 14;
 
 template <int BS>
 struct Tile {
