@@ -19,6 +19,7 @@ from source into oracle/_ref by oracle/ref/Makefile) on this host's cores.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -235,6 +236,10 @@ def our_arm(args):
     g32 = gf.copy(precision=q.F32)
     tuned["fp32"] = q.autotune_force(g32, C1, 3)
     del g32
+    # the FP32 FMA rate of this GPU (chains of scalar FFMA), the compute
+    # roofline of the force kernel (untimed)
+    fma_peak = ctypes.c_double()
+    q._lib.call("qgb_fma_rate", 0, 3, ctypes.byref(fma_peak))
 
     def trajectory(traj, precision):
         nonlocal gf, gf0
@@ -385,7 +390,10 @@ def our_arm(args):
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
                      "algorithmic_bytes_per_launch": bytes_fu, "mean_launch_ms": t_fu / n_fu if n_fu else None,
                      "fp32_tflops_achieved": tflops, "flops_per_site": flops_site,
-                     "note": "compute-bound on CUDA cores (FP32); HBM fraction is reported as the metric asks"},
+                     "note": "compute-bound on CUDA cores (FP32); HBM fraction is reported as the metric asks",
+                     "compute": {"achieved": tflops, "peak": fma_peak.value, "unit": "TFLOP/s",
+                                 "frac": (tflops / fma_peak.value) if tflops and fma_peak.value else None,
+                                 "peak_source": "FP32 FFMA chains measured in this run (qgb_fma_rate)"}},
         "kernel_ms_per_traj": {k: v[0] / args.steps for k, v in prof.items()},
         "force_variant": {k: {"variant": v[0], "ms": v[1], **q.force_variants()[v[0]]} for k, v in tuned.items()},
         "clocks": clk, "gpu_launches": launches,

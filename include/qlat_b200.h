@@ -171,8 +171,8 @@ int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c
                              double md_time, int32_t integrator, int32_t reunit_interval,
                              double* delta_h);
 
-/* Halo hook of a domain-decomposed trajectory: called with the link field
- * before every force evaluation, after the kernels before it have been
+/* Halo hook of a domain-decomposed trajectory: called with a link field
+ * before a force evaluation reads it, after the kernels before it have been
  * enqueued on the library stream; it must leave the field's halo sites fresh
  * copies of the neighbouring domains' links and return 0 (any other value
  * aborts the trajectory with QGB_ERR_HOOK). */
@@ -180,13 +180,18 @@ typedef int (*qgb_halo_hook)(qgb_field* gf, void* user);
 /* The molecular dynamics of run_hmc_evolve_pure_gauge (hmc.pyx:169-188)
  * without the Hamiltonians, in the fields' precision (gm, gf both FP64 or both
  * FP32), on the reference's refresh-before-force schedule (hmc.cpp:466-490
- * refreshes the expanded field before each force): hook(gf, user) runs before
- * each force evaluation when hook is not NULL.  The kernel sequence is the one
- * qgb_run_hmc_evolve (reunit_interval = 0: unitarise after every exponential)
- * and qgb_run_hmc_evolve_mixed (reunit_interval > 0, on FP32 fields: FP64
- * re-unitarisation every that many steps) run. */
+ * refreshes the expanded field before each force).  When hook is not NULL,
+ * hook(gf, user) runs before each force evaluation on gf, and with
+ * refresh_shifted != 0 also hook(shifted, user) before the force at the
+ * force-gradient shift U' = exp(eps F(U)) U (shifted: a library-owned field of
+ * gf's shape; a halo thinner than twice the force's reach needs it).  The
+ * kernel sequence is the one qgb_run_hmc_evolve (reunit_interval = 0:
+ * unitarise after every exponential) and qgb_run_hmc_evolve_mixed
+ * (reunit_interval > 0, on FP32 fields: FP64 re-unitarisation every that many
+ * steps) run. */
 int qgb_run_md_hooked(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step, double md_time,
-                      int32_t integrator, int32_t reunit_interval, qgb_halo_hook hook, void* user);
+                      int32_t integrator, int32_t reunit_interval, int32_t refresh_shifted, qgb_halo_hook hook,
+                      void* user);
 
 /* ---- hot path: gradient flow (wilson-flow.h:9-43, everything.pxd:514-521) --- */
 

@@ -385,19 +385,27 @@ ForceArgs fargs(const void* U, void* out, double beta, double c1, double dt)
 // unit_each: unitarize after every exponential; reunit_every > 0 re-unitarises
 // the links with FP64 arithmetic every that many steps.
 // hook (with hook_gf, the field whose buffer is gf) refreshes the halo of a
-// domain-decomposed field before each force evaluation that reads gf.
+// domain-decomposed field before each force evaluation that reads gf, and
+// with hook_shifted also that of the force-gradient shift tmp before the force
+// that reads it.
 template <typename R>
 int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, double c1, int n_step, double md_time,
                   int integrator, int unit_each, int reunit_every, qgb_halo_hook hook = nullptr,
-                  qgb_field* hook_gf = nullptr, void* hook_user = nullptr)
+                  qgb_field* hook_gf = nullptr, void* hook_user = nullptr, bool hook_shifted = false)
 {
   const double dt = md_time / n_step;
-  auto refresh = [&]() -> int {
+  qgb_field_s shifted;  // tmp, described as a field of gf's shape for the hook
+  if (hook_gf) {
+    shifted = *hook_gf;
+    shifted.d = tmp;
+  }
+  auto refresh_field = [&](qgb_field* f) -> int {
     if (!hook) return QGB_OK;
-    const int rc = hook(hook_gf, hook_user);
+    const int rc = hook(f, hook_user);
     if (rc) return fail(QGB_ERR_HOOK, "halo hook returned " + std::to_string(rc));
     return QGB_OK;
   };
+  auto refresh = [&]() -> int { return refresh_field(hook_gf); };
   // gm += h F(U) followed by gf = exp(eps gm) gf, as one launch: the update
   // kernel's epilogue evolves this thread's own link of gf (U is tmp for the
   // force-gradient step, so gf is never read at other links; for leapfrog U is
@@ -423,6 +431,7 @@ int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, doub
         ForceArgs a = fargs(gf, tmp, beta, c1, fg_dt);
         a.unitarize = unit_each;
         QGB_RC(force<R>(g, qgb::FORCE_EVOLVE, a));
+        if (hook_shifted) QGB_RC(refresh_field(&shifted));
         const double eps = half == 0 ? (1.0 - 2.0 * lam) * dt : (i < n_step - 1 ? 2.0 * lam : lam) * dt;
         QGB_RC(update_evolve(tmp, 0.5 * dt, eps, half == 1 && reunit));
       }
@@ -1321,7 +1330,8 @@ int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c
 }
 
 int qgb_run_md_hooked(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step, double md_time,
-                      int32_t integrator, int32_t reunit_interval, qgb_halo_hook hook, void* user)
+                      int32_t integrator, int32_t reunit_interval, int32_t refresh_shifted, qgb_halo_hook hook,
+                      void* user)
 {
   QGB_CTX();
   QGB_RC(check_field(gm, QGB_KIND_COLOR_MATRIX, "qgb_run_md_hooked"));
@@ -1336,9 +1346,9 @@ int qgb_run_md_hooked(qgb_field* gm, qgb_field* gf, double beta, double c1, int3
   const int unit_each = reunit_interval > 0 ? 0 : 1;
   if (gf->prec == QGB_F64)
     return md_trajectory<double>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, unit_each,
-                                 reunit_interval, hook, gf, user);
+                                 reunit_interval, hook, gf, user, refresh_shifted != 0);
   return md_trajectory<float>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, unit_each,
-                              reunit_interval, hook, gf, user);
+                              reunit_interval, hook, gf, user, refresh_shifted != 0);
 }
 
 // ---- gradient flow ---------------------------------------------------------

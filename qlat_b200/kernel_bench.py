@@ -14,9 +14,10 @@
     python -m qlat_b200.kernel_bench flow-adjoint [--lattice 16,16,16,16] [--steps 40] [--every 8]
         backward through the Wilson flow: timing, finite-difference check, flowed-field HMC
 
-    python -m qlat_b200.kernel_bench slabs [--lattice 24,24,24,64] [--precision mixed]
-        one chain as a one-rank time slab (4 halo slices each side, a halo refresh before every
-        force evaluation) against the plain single-GPU trajectory: traj/s and the exchange time
+    python -m qlat_b200.kernel_bench slabs [--lattice 24,24,24,64] [--precision mixed] [--halo 4]
+        one chain as a one-rank time slab (4 halo slices each side and a refresh before every
+        force-gradient update, or 2 and a refresh before every force) against the plain single-GPU
+        trajectory: traj/s and the exchange time
 
     python -m qlat_b200.kernel_bench functions hmc|flow [--lattice ...] [--reps 20]
         seconds per call of single API functions (hmc: 24^3x64 Iwasaki set_gm_force, gf_evolve,
@@ -278,7 +279,7 @@ def slabs(args):
     gf.set_rand(rs.split("gf-init"), 0.3, 1)
     for prec in (q.F64, q.F32):
         q.autotune_force(gf.copy(precision=prec), ga.c1())
-    sl = q.TimeSlabs(ts)
+    sl = q.TimeSlabs(ts, halo=args.halo)
     out = {"lattice": list(ts), "precision": args.precision, "n_step": args.n_step, "halo": sl.halo,
            "local_time_extent": sl.nt + 2 * sl.halo}
 
@@ -324,7 +325,7 @@ def slabs(args):
     q._lib.call("qgb_field_tslice_bytes", g32.handle, sl.halo, ctypes.byref(n))
     out["exchange_ms"] = (time.perf_counter() - t0) / 20 * 1e3
     out["exchange_bytes_each_way"] = 2 * n.value
-    out["exchanges_per_traj"] = 2 * args.n_step + 2
+    out["exchanges_per_traj"] = 2 * args.n_step * (2 if args.halo < 4 else 1) + 2
     print(json.dumps(out))
 
 
@@ -419,6 +420,7 @@ def main():
     g.add_argument("--trajs", type=int, default=5)
     g.add_argument("--warmup", type=int, default=2)
     g.add_argument("--order", default="plain,slab")
+    g.add_argument("--halo", type=int, default=4)
     h = sub.add_parser("functions")
     h.add_argument("set", choices=["hmc", "flow"])
     h.add_argument("--lattice", default=None)

@@ -9,10 +9,14 @@ its two neighbours on either side, as one ordinary GPU field of time extent
 T / R + 2 halo.  The library's kernels run unchanged on that field; the owned
 sites are correct as long as the halo slices are fresh copies:
 
-- the Iwasaki force reaches two slices, so a force-gradient momentum update
-  (the force at U, the shifted U' = exp(eps F) U, the force at U') is right on
-  the owned slices when the halo is 4 slices deep and was refreshed just before
-  it: one exchange per update;
+- the Iwasaki force reaches two slices (the Wilson force one), so a
+  force-gradient momentum update (the force at U, the shifted
+  U' = exp(eps F) U, the force at U') is right on the owned slices when the
+  halo is twice the reach deep (4 slices) and was refreshed just before it:
+  one exchange per update.  With a halo of just the reach (2 slices, the
+  reference's own expansion for the rectangle action) the shifted field is
+  exchanged too, before the force at U': two exchanges per update of half the
+  slices each, and half the redundant halo work;
 - the link updates are site-local and need no exchange;
 - the molecular dynamics is the library's own fused kernel sequence
   (qgb_run_md_hooked), which calls back into ``exchange`` before each force
@@ -86,16 +90,19 @@ class TimeSlabs:
     def exchange(self, f) -> None:
         """Refresh the halo slices of f from the neighbouring ranks (the ring
         of time slabs is periodic)."""
+        self._exchange_handle(f.handle)
+
+    def _exchange_handle(self, handle) -> None:
         import torch
         from . import synchronize
         h, nt = self.halo, self.nt
         n = ctypes.c_int64()
-        call("qgb_field_tslice_bytes", f.handle, h, ctypes.byref(n))
+        call("qgb_field_tslice_bytes", handle, h, ctypes.byref(n))
         nbytes = n.value
         up_dev = self._buffer("send_up", nbytes, "cuda")
         dn_dev = self._buffer("send_dn", nbytes, "cuda")
-        call("qgb_field_pack_tslices", f.handle, nt, h, ctypes.c_void_p(up_dev.data_ptr()))  # top owned slices
-        call("qgb_field_pack_tslices", f.handle, h, h, ctypes.c_void_p(dn_dev.data_ptr()))   # bottom owned slices
+        call("qgb_field_pack_tslices", handle, nt, h, ctypes.c_void_p(up_dev.data_ptr()))  # top owned slices
+        call("qgb_field_pack_tslices", handle, h, h, ctypes.c_void_p(dn_dev.data_ptr()))   # bottom owned slices
         synchronize()
         if self.world == 1:
             rbot, rtop = up_dev, dn_dev
@@ -106,8 +113,8 @@ class TimeSlabs:
                 rbot = rbot.to("cuda")
                 rtop = rtop.to("cuda")
             torch.cuda.current_stream().synchronize()
-        call("qgb_field_unpack_tslices", f.handle, 0, h, ctypes.c_void_p(rbot.data_ptr()))
-        call("qgb_field_unpack_tslices", f.handle, nt + h, h, ctypes.c_void_p(rtop.data_ptr()))
+        call("qgb_field_unpack_tslices", handle, 0, h, ctypes.c_void_p(rbot.data_ptr()))
+        call("qgb_field_unpack_tslices", handle, nt + h, h, ctypes.c_void_p(rtop.data_ptr()))
         synchronize()
 
     def _swap(self, send_up, send_dn):
@@ -131,12 +138,17 @@ class TimeSlabs:
     def run_md(self, gm: GaugeMomentum, gf: GaugeField, ga: GaugeAction, n_step: int, md_time: float = 1.0, *,
                integrator: str = "force-gradient", reunit_interval: int = 0) -> None:
         """The molecular dynamics of one trajectory on the slab fields (FP64 or
-        FP32), with a halo exchange before every force evaluation."""
+        FP32), with a halo exchange before every force evaluation that needs
+        one."""
+        reach = 2 if ga.c1() != 0.0 else 1
+        if self.halo < reach:
+            raise ValueError(f"TimeSlabs: a halo of {self.halo} slices is thinner than the force's reach {reach}")
+        shifted = 1 if self.halo < 2 * reach else 0
         errors = []
 
         def hook(handle, user):
             try:
-                self.exchange(gf)
+                self._exchange_handle(handle)
                 return 0
             except BaseException as e:  # raised again below, after the library call returns
                 errors.append(e)
@@ -145,7 +157,7 @@ class TimeSlabs:
         cb = HALO_HOOK(hook)
         try:
             call("qgb_run_md_hooked", gm.handle, gf.handle, ga.beta(), ga.c1(), int(n_step), float(md_time),
-                 INTEGRATORS[integrator], int(reunit_interval), cb, None)
+                 INTEGRATORS[integrator], int(reunit_interval), shifted, cb, None)
         except Exception:
             if errors:
                 raise errors[0]

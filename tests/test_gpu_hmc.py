@@ -188,7 +188,7 @@ def test_mixed_trajectory_equals_its_steps(q, ts):
     g2, m2 = gf.copy(), gm.copy()
     h0 = q.gm_hamilton_node(m2) + q.gf_hamilton_node(g2, ga)
     g32, m32 = g2.copy(precision=q.F32), m2.copy(precision=q.F32)
-    call("qgb_run_md_hooked", m32.handle, g32.handle, ga.beta(), ga.c1(), 8, 1.0, 0, 4,
+    call("qgb_run_md_hooked", m32.handle, g32.handle, ga.beta(), ga.c1(), 8, 1.0, 0, 4, 0,
          ctypes.cast(None, HALO_HOOK), None)
     g2 @= g32
     m2 @= m32

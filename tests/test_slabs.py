@@ -7,8 +7,10 @@ instead of waiting for ever.
 GPU: a one-rank slab (its halo is its own periodic copy) and two ranks run as
 two processes on one GPU, exchanging halos through host memory over gloo (no
 kernel waits on another rank), both against the single-GPU trajectory of the
-whole lattice, in the FP64 and the mixed FP32/FP64 forms: the same links on
-every owned site, the same delta_h and the same accept / reject decisions.  A
+whole lattice, in the FP64 and the mixed FP32/FP64 forms and with halos of 4
+slices (one exchange per force-gradient update) and 2 slices (the shifted
+field exchanged too): the same links on every owned site, the same delta_h
+and the same accept / reject decisions.  A
 halo exchange that raises inside the library's trajectory ends the call with
 its exception.
 """
@@ -31,6 +33,17 @@ def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
+
+
+def test_halo_thinner_than_reach_is_refused():
+    """A 1-slice halo cannot carry the rectangle force (reach 2); the check
+    runs before any GPU work."""
+    sys.path.insert(0, ROOT)
+    from qlat_b200.field import GaugeAction
+    from qlat_b200.slabs import TimeSlabs
+    s = TimeSlabs((4, 4, 4, 8), halo=1)
+    with pytest.raises(ValueError):
+        s.run_md(None, None, GaugeAction(2.13, -0.331), 4)
 
 
 def test_slab_geometry():
@@ -118,9 +131,9 @@ def _compare(rows, ref_rows, links, ref_links, t0, nt):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_one_rank_slab_matches_global(q, precision):
-    slabs = q.TimeSlabs(TS)
+@pytest.mark.parametrize("precision,halo", [("fp64", 4), ("mixed", 4), ("fp64", 2), ("mixed", 2)])
+def test_one_rank_slab_matches_global(q, precision, halo):
+    slabs = q.TimeSlabs(TS, halo=halo)
     rows, links = _slab_run(q, slabs, precision)
     ref_rows, ref_links = _global_run(q, precision)
     _compare(rows, ref_rows, links, ref_links, 0, TS[3])
@@ -135,11 +148,11 @@ def test_halo_hook_error_aborts_trajectory(q):
     class Failing(q.TimeSlabs):
         calls = 0
 
-        def exchange(self, f):
+        def _exchange_handle(self, handle):
             Failing.calls += 1
             if Failing.calls == 3:
                 raise ConnectionError("peer gone")
-            super().exchange(f)
+            super()._exchange_handle(handle)
 
     slabs = Failing(TS)
     ga = q.GaugeAction(BETA, C1)
@@ -153,7 +166,7 @@ def test_halo_hook_error_aborts_trajectory(q):
     assert np.isfinite(slabs.plaq(gf))
 
 
-def _slab_main(rank, world, port, out_dir, precision):
+def _slab_main(rank, world, port, out_dir, precision, halo):
     import datetime
 
     import torch
@@ -164,7 +177,7 @@ def _slab_main(rank, world, port, out_dir, precision):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
-        slabs = q.TimeSlabs(TS)
+        slabs = q.TimeSlabs(TS, halo=halo)
         rows, links = _slab_run(q, slabs, precision)
         np.save(os.path.join(out_dir, f"links{rank}.npy"), links)
         with open(os.path.join(out_dir, f"rows{rank}.json"), "w") as f:
@@ -174,10 +187,10 @@ def _slab_main(rank, world, port, out_dir, precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_two_rank_slabs_match_global(q, tmp_path, precision):
+@pytest.mark.parametrize("precision,halo", [("fp64", 4), ("mixed", 4), ("mixed", 2)])
+def test_two_rank_slabs_match_global(q, tmp_path, precision, halo):
     import torch.multiprocessing as mp
-    mp.start_processes(_slab_main, args=(2, _free_port(), str(tmp_path), precision), nprocs=2, join=True,
+    mp.start_processes(_slab_main, args=(2, _free_port(), str(tmp_path), precision, halo), nprocs=2, join=True,
                        start_method="spawn")
     ref_rows, ref_links = _global_run(q, precision)
     for r in range(2):
