@@ -24,6 +24,10 @@
         the Hamiltonians, the momentum draw, unitarize, gf_avg_plaq; flow: 32^4 RK3 Wilson flow step,
         energy density, clover and 5-loop charges), each call synchronised
 
+    python -m qlat_b200.kernel_bench c1 [--trajs 10]
+        8^4 Wilson (beta 5.5) leapfrog, 6 steps per unit trajectory, hot start at scale 1: the small
+        configuration, through run_hmc_pure_gauge, per-trajectory time
+
 Each command prints one JSON line.
 """
 
@@ -376,6 +380,35 @@ def functions(args):
     print(json.dumps(out))
 
 
+def c1(args):
+    """The 8^4 Wilson leapfrog chain (10 trajectories, the first always
+    accepted) through the qlat-compatible run_hmc_pure_gauge, in FP64 and in
+    the mixed form: milliseconds per trajectory and the plaquettes."""
+    import torch
+    import qlat_b200 as q
+    torch.cuda.set_device(0)
+    ts = (8, 8, 8, 8)
+    ga = q.GaugeAction(5.5, 0.0)
+    out = {"lattice": list(ts), "beta": 5.5, "integrator": "leapfrog", "n_step": 6, "trajs": args.trajs}
+    for prec in ("fp64", "mixed"):
+        rs = q.RngState("b200-c1-8x4-wilson")
+        gf = q.GaugeField(q.Geometry(ts))
+        gf.set_rand(rs.split("gf-init"), 1.0, 1)
+        for t in range(1, 4):  # warm-up chain, discarded
+            q.run_hmc_pure_gauge(gf.copy(), ga, t, rs.split("warm"), n_step=6, integrator="leapfrog",
+                                 precision=prec)
+        q.synchronize()
+        t0 = time.perf_counter()
+        plaq = []
+        for t in range(1, args.trajs + 1):
+            q.run_hmc_pure_gauge(gf, ga, t, rs.split("hmc"), n_step=6, integrator="leapfrog", precision=prec,
+                                 is_always_accept=t == 1)
+            plaq.append(q.gf_avg_plaq(gf))
+        q.synchronize()
+        out[prec] = {"ms_per_traj": (time.perf_counter() - t0) / args.trajs * 1e3, "plaq": plaq}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -421,13 +454,16 @@ def main():
     g.add_argument("--warmup", type=int, default=2)
     g.add_argument("--order", default="plain,slab")
     g.add_argument("--halo", type=int, default=4)
+    c1p = sub.add_parser("c1")
+    c1p.add_argument("--trajs", type=int, default=10)
     h = sub.add_parser("functions")
     h.add_argument("set", choices=["hmc", "flow"])
     h.add_argument("--lattice", default=None)
     h.add_argument("--reps", type=int, default=20)
     args = ap.parse_args()
     {"force-variants": force_variants, "force-profile": force_profile, "flow": flow, "batch": batch,
-     "flow-adjoint": flow_adjoint, "fma-peak": fma_peak, "slabs": slabs, "functions": functions}[args.cmd](args)
+     "flow-adjoint": flow_adjoint, "fma-peak": fma_peak, "slabs": slabs, "functions": functions,
+     "c1": c1}[args.cmd](args)
 
 
 if __name__ == "__main__":
