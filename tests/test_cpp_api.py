@@ -2,7 +2,9 @@
 drivers (examples-cpp/hmc/main.cpp, examples-cpp/flowed-hmc/main.cpp)
 rewritten on it (tests/cpp/hmc_main.cpp, tests/cpp/flowed_hmc_main.cpp)
 compile against the library (CPU) and, on the GPU, print the reference's CHECK
-lines (examples-cpp/hmc/log, examples-cpp/flowed-hmc/log) to 12 digits."""
+lines (examples-cpp/hmc/log, examples-cpp/flowed-hmc/log) to 12 digits.  A
+time-slab caller written on the bare C ABI (tests/cpp/slab_hook_main.cpp: a C
+halo hook, owned-site sums) reproduces the plain trajectory on the GPU."""
 
 import os
 import re
@@ -14,17 +16,22 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_DIR = os.path.join(ROOT, "qlat_b200")
 
 
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+# drivers that allocate their own device buffers (the halo hook's) use the CUDA runtime too
+CUDART = {"slab_hook_main": ["-I", os.path.join(CUDA, "include"), "-L", os.path.join(CUDA, "lib64"), "-lcudart"]}
+
+
 def build_driver(out_dir, name="hmc_main"):
     exe = os.path.join(out_dir, name)
     cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
            os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-L", LIB_DIR, "-lqlat_b200",
-           f"-Wl,-rpath,{LIB_DIR}", "-o", exe]
+           f"-Wl,-rpath,{LIB_DIR}", *CUDART.get(name, []), "-o", exe]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-3000:]
     return exe
 
 
-@pytest.mark.parametrize("name", ["hmc_main", "flowed_hmc_main", "api_surface"])
+@pytest.mark.parametrize("name", ["hmc_main", "flowed_hmc_main", "api_surface", "slab_hook_main"])
 def test_cpp_driver_compiles_and_links(tmp_path, name):
     if not os.path.exists(os.path.join(LIB_DIR, "libqlat_b200.so")):
         pytest.skip("library not built")
@@ -119,3 +126,11 @@ def test_cpp_api_surface_matches_python(q, tmp_path):
     for k, v in want.items():
         assert abs(got[k] - v) <= 1e-12 * max(abs(v), 1.0), (k, got[k], v)
     assert got["flow_round_trip"] < 1e-24 * gf.qnorm()
+
+
+@pytest.mark.gpu
+def test_cpp_slab_hook_driver(tmp_path):
+    exe = build_driver(str(tmp_path), "slab_hook_main")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "CHECK: slab hook ok" in r.stdout
