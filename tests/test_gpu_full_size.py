@@ -1,5 +1,6 @@
 """Checks at the benchmark's own size, 24^3 x 64 (884,736 sites, site indices
-up to six digits in the per-site random streams).
+up to six digits in the per-site random streams), and at the gradient-flow
+configuration's 32^4.
 
 - The hot start and the momenta are bit-exact against the oracle (run with a
   correctly rounded log) on every site.
@@ -9,6 +10,8 @@ up to six digits in the per-site random streams).
   bound of hmc.pyx:211), and delta_h changes sign.
 - The mixed trajectory from the same state matches the FP64 one: plaquette
   within 1e-6, delta_h within 5% (plus 0.05) of the FP64 value.
+- 32^4: one RK3 flow step matches the oracle (links 1e-13, energy density
+  1e-12, clover charge 1e-9; with FP32 links 1e-6 and 1e-4).
 """
 
 import numpy as np
@@ -71,3 +74,32 @@ def test_trajectory_properties_at_full_size(q, fields):
     dh32 = q.run_hmc_evolve_pure_gauge(m32, g32, ga, None, 8, 1.0, precision="mixed", reunit_interval=4)
     assert abs(q.gf_avg_plaq(g32) - q.gf_avg_plaq(g64)) < 1e-6
     assert abs(dh32 - dh) <= 0.05 * abs(dh) + 0.05
+
+
+def test_flow_at_full_size(q, oracle):
+    """The gradient-flow configuration's lattice, 32^4: after one RK3 step
+    (eps = 0.05, Wilson flow) from the seeded hot start, the links, the
+    energy density and the clover charge agree with the oracle, in FP64 and
+    (to FP32 accuracy) with FP32 links."""
+    ts = (32, 32, 32, 32)
+    rs = "b200-c3-32x32-flow"
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState(rs).split("gf-init"), 0.5, 1)
+    g32 = gf.copy(precision=q.F32)
+    ogf = oracle.new_field(ts)
+    oracle.set_log_mode(1)
+    try:
+        oracle.gf_set_rand(ogf, ts, oracle.RngState(rs).split("gf-init"), 0.5, 1)
+    finally:
+        oracle.set_log_mode(0)
+    q.gf_wilson_flow_step(gf, 0.05, c1=0.0)
+    q.gf_wilson_flow_step(g32, 0.05, c1=0.0)
+    oracle.gf_wilson_flow_step(ogf, ts, 0.05, 0.0)
+    got = np.asarray(gf)
+    assert float(np.linalg.norm((got - ogf).ravel()) / np.linalg.norm(ogf.ravel())) < 1e-13
+    e, oe = q.gf_energy_density(gf), oracle.gf_energy_density(ogf, ts)
+    assert abs(e - oe) <= 1e-12 * abs(oe)
+    qc, oq = q.gf_topology_clf(gf), oracle.gf_topology_clf(ogf, ts)
+    assert abs(qc - oq) <= 1e-9
+    assert abs(q.gf_energy_density(g32) - oe) <= 1e-6 * abs(oe)
+    assert abs(q.gf_topology_clf(g32) - oq) <= 1e-4
