@@ -261,11 +261,14 @@ __device__ __forceinline__ void staple_dir_fast(M3<R>& S, const LinkLd<R>& L, in
   }
 }
 
+// s: the site's index in the field U (the lattice's sites start at g.off);
+// nblk: the field's 32-site blocks (default: those of the lattice alone).
 template <typename R, bool RECT, bool TWO>
-__device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, int s, int mu, R cp, R cr)
+__device__ __forceinline__ M3<R> staple_sum_fast(const Cx<R>* U, const Geo& g, int s, int mu, R cp, R cr,
+                                                 int nblk = -1)
 {
-  const LinkLd<R> L{U, (int)site_blocks(g.V)};
-  const Coord x = coord_of(g, s);
+  const LinkLd<R> L{U, nblk >= 0 ? nblk : (int)site_blocks(g.V)};
+  const Coord x = coord_of(g, s - g.off);
   const int st[4] = {1, g.d[0], g.d[0] * g.d[1], g.d[0] * g.d[1] * g.d[2]};
   const int xm = sel4(x.c, mu), Lm = sel4(g.d, mu), sm = sel4(st, mu);
   const int dmm1 = nb_delta(xm, -1, Lm, sm), dmp1 = nb_delta(xm, 1, Lm, sm), dmp2 = nb_delta(xm, 2, Lm, sm);
@@ -485,10 +488,20 @@ inline int force_variant_info(int variant, int* bs, int* minb, int* split, int* 
 // the concatenated field (Vtot sites, block = 4 * site block + mu).  Each thread finds its
 // chain by binary search over the chain offsets and uses that chain's lattice,
 // beta and c1.  RECT is set when any chain has c1 != 0 (Wilson chains then add
-// rectangle terms with weight 0).
-template <typename R, int MODE, bool RECT>
-__global__ void __launch_bounds__(128) k_force_batch(long Vtot, int nchain, const long* __restrict__ offs,
-                                                     const ChainInfo* __restrict__ chains, ForceArgs a)
+// rectangle terms with weight 0).  FAST: the staple sum of the single-lattice
+// kernel's fastest form (per-direction neighbour offsets within the chain's
+// lattice, two-row chains in FP32; 32-bit link offsets, so the launcher uses
+// it while 36 padded sites < 2^31), with that form's register budget.
+template <typename R, bool RECT>
+constexpr int batch_min_blocks()
+{
+  return sizeof(R) == 4 ? (RECT ? 4 : 8) : (RECT ? 1 : 3);
+}
+
+template <typename R, int MODE, bool RECT, bool FAST>
+__global__ void __launch_bounds__(128, FAST ? batch_min_blocks<R, RECT>() : 1)
+    k_force_batch(long Vtot, int nchain, const long* __restrict__ offs, const ChainInfo* __restrict__ chains,
+                  ForceArgs a)
 {
   const long sg = (long)(blockIdx.x >> 2) * 128 + threadIdx.x;  // block = 4 * (site block) + mu
   if (sg >= Vtot) return;
@@ -497,9 +510,14 @@ __global__ void __launch_bounds__(128) k_force_batch(long Vtot, int nchain, cons
   const Geo g = chain_geo(ci);
   const int mu = blockIdx.x & 3;
   const CField<R> U{(const Cx<R>*)a.U, Vtot};
-  const Coord x = coord_of(g, sg - ci.off);
   const R cp = R(1.0 - 8.0 * ci.c1), cr = R(ci.c1);
-  const M3<R> S = staple_sum_rt<R, RECT>(U, g, x, mu, cp, cr, 0, 6);
+  M3<R> S;
+  if constexpr (FAST) {
+    S = staple_sum_fast<R, RECT, sizeof(R) == 4>((const Cx<R>*)a.U, g, (int)sg, mu, cp, cr, (int)site_blocks(Vtot));
+  } else {
+    const Coord x = coord_of(g, sg - ci.off);
+    S = staple_sum_rt<R, RECT>(U, g, x, mu, cp, cr, 0, 6);
+  }
   force_epilogue<R, MODE>(a, U, Vtot, sg, mu, S, ci.beta);
 }
 
@@ -508,9 +526,15 @@ cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const Ch
                                ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
   dim3 grid((unsigned)(4 * ((Vtot + 127) / 128)), 1);
-#define QGB_LAUNCH(M)                                                                      \
-  if (rect) k_force_batch<R, M, true><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a); \
-  else k_force_batch<R, M, false><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);
+  const bool fast = padded_sites(Vtot) * 36 < 2147483647L;
+#define QGB_LAUNCH(M)                                                                                  \
+  if (fast) {                                                                                          \
+    if (rect) k_force_batch<R, M, true, true><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);   \
+    else k_force_batch<R, M, false, true><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);       \
+  } else {                                                                                             \
+    if (rect) k_force_batch<R, M, true, false><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);  \
+    else k_force_batch<R, M, false, false><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);      \
+  }
   switch (mode) {
     case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
     case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;
