@@ -256,6 +256,18 @@ inline double run_hmc_evolve(GaugeMomentum& gm, GaugeField& gf, const GaugeActio
   check(qgb_run_hmc_evolve(gm.handle(), gf.handle(), ga.beta, ga.c1, n_step, md_time, integrator, &dh));
   return dh;
 }
+/* The same trajectory in the mixed form: FP32 molecular dynamics on copies of
+ * the FP64 fields, FP64 re-unitarisation every reunit_interval steps, FP64
+ * Hamiltonians; returns delta_h. */
+inline double run_hmc_evolve_mixed(GaugeMomentum& gm, GaugeField& gf, const GaugeAction& ga, int n_step,
+                                   double md_time = 1.0, int integrator = QGB_INTEGRATOR_FORCE_GRADIENT,
+                                   int reunit_interval = 4)
+{
+  double dh;
+  check(qgb_run_hmc_evolve_mixed(gm.handle(), gf.handle(), ga.beta, ga.c1, n_step, md_time, integrator,
+                                 reunit_interval, &dh));
+  return dh;
+}
 inline void gf_wilson_flow_step(GaugeField& gf, double epsilon, double c1 = 0.0)
 {
   check(qgb_gf_wilson_flow_step(gf.handle(), epsilon, c1));

@@ -76,5 +76,13 @@ int main()
   gfi -= gf;
   std::printf("flow_steps %d\nflow_round_trip %.17g\nflowed_action %.17g\n", (int)fi.v.size(), qnorm(gfi),
               gf_hamilton_flowed_node(gf, GaugeAction(2.31, -0.331), fi));
+  // the mixed trajectory
+  GaugeField g3;
+  g3 = gf;
+  GaugeMomentum m3;
+  m3.init(geo);
+  set_rand_gauge_momentum(m3, 1.0, rs.split("mom"));
+  std::printf("delta_h_mixed %.17g\n", run_hmc_evolve_mixed(m3, g3, GaugeAction(2.13, -0.331), 6));
+  std::printf("plaq_mixed %.17g\n", gf_avg_plaq(g3));
   return 0;
 }

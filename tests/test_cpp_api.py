@@ -123,6 +123,12 @@ def test_cpp_api_surface_matches_python(q, tmp_path):
     want["flow_steps"] = len(fi.v)
     act, ld = q.gf_hamilton_flowed(gf, q.GaugeAction(2.31, -0.331), fi)
     want["flowed_action"] = act - ld
+    g3 = gf.copy()
+    m3 = q.GaugeMomentum(geo)
+    m3.set_rand(rs.split("mom"), 1.0)
+    want["delta_h_mixed"] = q.run_hmc_evolve_pure_gauge(m3, g3, q.GaugeAction(2.13, -0.331), None, 6,
+                                                        precision="mixed", reunit_interval=4)
+    want["plaq_mixed"] = g3.plaq()
     for k, v in want.items():
         assert abs(got[k] - v) <= 1e-12 * max(abs(v), 1.0), (k, got[k], v)
     assert got["flow_round_trip"] < 1e-24 * gf.qnorm()
