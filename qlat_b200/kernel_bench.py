@@ -2,8 +2,9 @@
 
     python -m qlat_b200.kernel_bench force-variants [--lattice 24,24,24,64]
         time every force-kernel launch variant (FP64 / FP32, Wilson / Iwasaki)
-    python -m qlat_b200.kernel_bench force-profile --variants 0,7 [--lattice 24,24,24,48]
-        one set_gm_force launch per variant and precision (Iwasaki), for ncu -k regex:k_force
+    python -m qlat_b200.kernel_bench force-profile --variants 0,7 [--lattice 24,24,24,48] [--c1 -0.331]
+        one set_gm_force launch per variant and precision (FP32 then FP64, or --precision fp32), for
+        ncu -k regex:k_force
     python -m qlat_b200.kernel_bench fma-peak [--reps 5]
         FMA rate of the device: scalar FP32, packed f32x2 and FP64 chains
     python -m qlat_b200.kernel_bench flow [--lattice 32,32,32,32] [--steps 80] [--every 4]
@@ -68,14 +69,16 @@ def force_profile(args):
     gf = q.GaugeField(q.Geometry(ts))
     gf.set_rand(q.RngState("kernel-bench").split("gf-init"), 0.3, 1)
     g32 = gf.copy(precision=q.F32)
-    ga = q.GaugeAction(2.13, -0.331)
-    for prec, g in ((q.F32, g32), (q.F64, gf)):
+    ga = q.GaugeAction(2.13, args.c1)
+    precs = ((q.F32, g32), (q.F64, gf)) if args.precision == "both" else ((q.F32, g32),)
+    for prec, g in precs:
         F = q.GaugeMomentum(gf.geo, precision=prec)
         for v in variants:
-            q.force_set_variant(prec, True, v)
+            q.force_set_variant(prec, args.c1 != 0.0, v)
             q.set_gm_force(F, g, ga)
     q.synchronize()
-    print(json.dumps({"lattice": list(ts), "variants": variants, "launches": 2 * len(variants)}))
+    print(json.dumps({"lattice": list(ts), "variants": variants, "c1": args.c1,
+                      "launches": len(precs) * len(variants)}))
 
 
 def fma_peak(args):
@@ -418,6 +421,8 @@ def main():
     b = sub.add_parser("force-profile")
     b.add_argument("--lattice", default="24,24,24,48")
     b.add_argument("--variants", default="0")
+    b.add_argument("--c1", type=float, default=-0.331)
+    b.add_argument("--precision", default="both", choices=["both", "fp32"])
     c = sub.add_parser("flow")
     c.add_argument("--lattice", default="32,32,32,32")
     c.add_argument("--steps", type=int, default=80)
