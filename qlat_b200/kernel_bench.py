@@ -409,6 +409,22 @@ def c1(args):
             plaq.append(q.gf_avg_plaq(gf))
         q.synchronize()
         out[prec] = {"ms_per_traj": (time.perf_counter() - t0) / args.trajs * 1e3, "plaq": plaq}
+        # the same chain as a batch of one (every phase one launch, the trajectory's
+        # molecular dynamics one CUDA graph), with run_hmc_pure_gauge's RNG splits
+        b = q.ChainBatch([ts], [5.5])
+        b.set_rand([rs.split("gf-init")], 1.0, 1)
+        for t in range(1, 4):
+            b.run_hmc(t, [rs.split("warm")], 6, precision=prec)
+        b.set_rand([rs.split("gf-init")], 1.0, 1)  # back to the hot start
+        q.synchronize()
+        t0 = time.perf_counter()
+        bplaq = []
+        for t in range(1, args.trajs + 1):
+            b.run_hmc(t, [rs.split("hmc")], 6, precision=prec, is_always_accept=t == 1)
+            bplaq.append(float(b.plaq()[0]))
+        q.synchronize()
+        out[prec + "_batch_of_one"] = {"ms_per_traj": (time.perf_counter() - t0) / args.trajs * 1e3,
+                                       "max_plaq_difference": max(abs(x - y) for x, y in zip(plaq, bplaq))}
     print(json.dumps(out))
 
 
