@@ -3,7 +3,8 @@
 CPU: the library's host-side format code against files that the reference
 library itself writes and reads (oracle/_ref/ref_nersc, built from the
 reference's sources): byte-identical data, identical header, both checksums,
-both directions.  GPU: GaugeField.save / GaugeField.load through the C ABI.
+both directions.  GPU: GaugeField.save / GaugeField.load through the C ABI,
+and a chain resumed from a checkpoint file.
 """
 
 import ctypes
@@ -168,3 +169,39 @@ def test_gpu_loads_reference_file(q, oracle, tmp_path):
     gf = q.GaugeField()
     gf.load(str(ref_path))
     assert np.abs(np.asarray(gf) - links).max() < 1e-14
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_chain_resumes_from_checkpoint(q, tmp_path, precision):
+    """The checkpoint / resume pattern of examples-py/hmc-pure-gauge.py:67-79:
+    a chain saved after 3 of 6 trajectories, read back into a fresh field and
+    continued with the same counter-based RNG splits, makes the same
+    accept / reject decisions as the uninterrupted chain, with plaquettes
+    within 1e-10 and delta_h within 1e-8 (the file keeps two rows of each
+    link; the third is rebuilt on reading, as qcd.h:244-246 does)."""
+    ga = q.GaugeAction(2.13, -0.331)
+    rs = q.RngState("resume")
+
+    def chain(gf, trajs):
+        rows = []
+        for t in trajs:
+            flag, dh = q.run_hmc_pure_gauge(gf, ga, t, rs.split("hmc"), n_step=6, is_always_accept=t <= 2,
+                                            precision=precision)
+            rows.append((bool(flag), dh, gf.plaq()))
+        return rows
+
+    gf = q.GaugeField(q.Geometry(TS))
+    gf.set_rand(rs.split("gf-init"), 0.1, 2)
+    g_ref = gf.copy()
+    full = chain(g_ref, range(1, 7))
+    first = chain(gf, range(1, 4))
+    p = tmp_path / f"ckpoint_lat.{precision}.3"
+    gf.save(str(p), beta=2.13, sequence_num=3)
+    g2 = q.GaugeField()
+    g2.load(str(p))
+    rest = chain(g2, range(4, 7))
+    for (f, dh, pl), (rf, rdh, rpl) in zip(first + rest, full):
+        assert f == rf
+        assert abs(dh - rdh) < 1e-8
+        assert abs(pl - rpl) < 1e-10
