@@ -712,34 +712,53 @@ cudaError_t launch_rand_momentum(const Geo& g, void* P, const uint32_t* rs24, do
   return cudaGetLastError();
 }
 
+// The four links of one site of a hot start (below): per link n_step factors,
+// each unitarize(exp_taylor20(X)) with X made from 8 Gaussians, multiplied in
+// order.  The Gaussians come from rng_gaussians_converged, 8 per factor, so a
+// warp's SHA-256 refills run together; the values are those of 8 successive
+// g_rand_gen calls.  Called by all 32 lanes of a warp.
+template <typename R>
+__device__ __forceinline__ void hot_start_links(Rng& rs, bool active, double s_sigma, double inv_sqrt3, int n_step,
+                                                const WField<R>& Uf, long s, int* amb)
+{
+  __shared__ double sb[8 * 128];  // the 8 Gaussians of a factor (run-time draw index)
+  const int nk = n_step > 1 ? n_step : 1;  // the reference always draws at least one factor
+  for (int mu = 0; mu < 4; ++mu) {
+    M3<double> v;
+    for (int k = 0; k < nk; ++k) {
+      rng_gaussians_converged<8>(rs, s_sigma, active, amb,
+                                 [&](int i, double x) { sb[i * 128 + threadIdx.x] = x; });
+      double b[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) b[i] = active ? sb[i * 128 + threadIdx.x] : 0.0;
+      M3<double> e = x_exp_taylor20(x_make_anti_hermitian(b, inv_sqrt3));
+      x_unitarize(e);
+      v = (k == 0) ? e : xm_mul(v, e);
+    }
+    if (active) {
+      M3<R> vr;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) vr.e[k] = cx<R>((R)v.e[k].re, (R)v.e[k].im);
+      Uf.st(s, mu, vr);
+    }
+  }
+}
+
 // set_g_rand_color_matrix_field: per link n_step products of
 // unitarize(exp_taylor20(X)) with X from make_g_rand_anti_hermitian_matrix.
 template <typename R>
 __global__ void __launch_bounds__(128) k_hot_start(Geo g, RngArg ra, double s_sigma, double inv_sqrt3, int n_step,
                                                    Cx<R>* U, int* ambiguous)
 {
+  // every lane of the warp stays to the end (warp-wide refills); lanes past
+  // the last site draw nothing and store nothing
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= g.V) return;
+  const bool active = s < g.V;
   Rng base, rs;
   rng_import(base, ra.v);
-  rng_split_long(rs, base, (int64_t)(s + g.rng_off));
+  if (active) rng_split_long(rs, base, (int64_t)(s + g.rng_off));
   int amb = 0;
-  const WField<R> Uf{U, g.V};
-  for (int mu = 0; mu < 4; ++mu) {
-    M3<double> v;
-    const int nk = n_step > 1 ? n_step : 1;  // the reference always draws at least one factor
-    for (int k = 0; k < nk; ++k) {
-      double b[8];
-      for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
-      M3<double> e = x_exp_taylor20(x_make_anti_hermitian(b, inv_sqrt3));
-      x_unitarize(e);
-      v = (k == 0) ? e : xm_mul(v, e);
-    }
-    M3<R> vr;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) vr.e[k] = cx<R>((R)v.e[k].re, (R)v.e[k].im);
-    Uf.st(s, mu, vr);
-  }
+  hot_start_links<R>(rs, active, s_sigma, inv_sqrt3, n_step, WField<R>{U, g.V}, s, &amb);
   if (amb) atomicAdd(ambiguous, 1);
 }
 
@@ -792,28 +811,16 @@ __global__ void __launch_bounds__(128) k_hot_start_batch(long Vtot, int nchain, 
                                                          double inv_sqrt3, int n_step, Cx<R>* U, int* ambiguous)
 {
   const long sg = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (sg >= Vtot) return;
-  const int c = chain_of(offs, nchain, sg);
-  Rng base, rs;
-  rng_import(base, rs24 + 24 * c);
-  rng_split_long(rs, base, (int64_t)(sg - offs[c]));
-  int amb = 0;
-  const WField<R> Uf{U, Vtot};
-  for (int mu = 0; mu < 4; ++mu) {
-    M3<double> v;
-    const int nk = n_step > 1 ? n_step : 1;
-    for (int k = 0; k < nk; ++k) {
-      double b[8];
-      for (int i = 0; i < 8; ++i) b[i] = rng_g_rand_gen<true>(rs, 0.0, s_sigma, &amb);
-      M3<double> e = x_exp_taylor20(x_make_anti_hermitian(b, inv_sqrt3));
-      x_unitarize(e);
-      v = (k == 0) ? e : xm_mul(v, e);
-    }
-    M3<R> vr;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) vr.e[k] = cx<R>((R)v.e[k].re, (R)v.e[k].im);
-    Uf.st(sg, mu, vr);
+  const bool active = sg < Vtot;
+  Rng rs;
+  if (active) {
+    const int c = chain_of(offs, nchain, sg);
+    Rng base;
+    rng_import(base, rs24 + 24 * c);
+    rng_split_long(rs, base, (int64_t)(sg - offs[c]));
   }
+  int amb = 0;
+  hot_start_links<R>(rs, active, s_sigma, inv_sqrt3, n_step, WField<R>{U, Vtot}, sg, &amb);
   if (amb) atomicAdd(ambiguous, 1);
 }
 
