@@ -534,31 +534,36 @@ int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int3
 /* ---- allocation-free action sums (no counterpart in the reference) ------ */
 
 /* For callers that cannot allocate GPU memory: a host whose device memory
- * belongs to its own pool (a framework's caching allocator, a fixed-budget
- * solver), or code recording into a CUDA graph, where a cudaMalloc during
- * stream capture fails and breaks the capture.  Every other entry point may
- * allocate (the library context, reduction scratch, staging); this one calls
- * no cudaMalloc, cudaFree or allocating library routine.
+ * belongs to its own pool (a framework's caching allocator, a solver with a
+ * fixed memory budget set at start-up), or one that cannot afford the
+ * device-wide synchronisation that cudaMalloc / cudaFree may cause while its
+ * other streams are busy.  Every other entry point may allocate (the library
+ * context, reduction scratch, staging); this one calls no cudaMalloc, cudaFree
+ * or allocating library routine.
  *
  * Computes the gauge-action sums of gf_sum_re_tr_plaq_node_no_comm and
  * gf_sum_re_tr_rect_node_no_comm (hmc.cpp:203-252): out_dev[0] = sum over
  * plaquettes of (Re tr P - 3), out_dev[1] = sum over rectangles of
  * (Re tr R - 3) when rect != 0, else 0.  links_dev is a caller-owned device
  * buffer holding the FP64 gauge field in the reference memory image
- * ([site][mu][3][3] complex128, x fastest); out_dev is caller-owned device
- * memory for two doubles.  Work is queued on `stream` (a cudaStream_t; NULL
- * for the legacy default stream) and nothing is synchronised.
+ * ([site][mu][3][3] complex128, x fastest), 16-byte aligned; out_dev is
+ * caller-owned device memory for two doubles, 8-byte aligned.  Work is queued
+ * on `stream` (a cudaStream_t; NULL for the legacy default stream) and nothing
+ * is synchronised.
  *
- * Limit: at most 2^24 = 16,777,216 sites (e.g. 64^4); larger lattices are
- * rejected with QGB_ERR_INVALID_ARG.  The scratch is a fixed 1 MiB device
- * array inside the library, which every GPU that loads the library holds
- * until the process exits.  The first call on each device looks up that
- * array's device address (cudaGetSymbolAddress) with the device current;
- * make that first call before any stream capture.  All calls share the one
- * array and it keeps the last call's partial sums (each call overwrites every
- * entry it reads, so nothing needs to start at zero): calls that overlap on
- * the GPU -- two streams, or two host threads -- race and must be serialised
- * by the caller. */
+ * Limit: at most 2^24 = 16,777,216 sites (e.g. 64^4), each extent in
+ * [1, 2^20].  Larger lattices and misaligned pointers are rejected with
+ * QGB_ERR_INVALID_ARG (bad extents with QGB_ERR_BAD_GEOMETRY) before anything
+ * is launched; so is a call made while an earlier, unrelated CUDA error is
+ * pending (QGB_ERR_CUDA; that error is left for its owner).  The scratch is a
+ * fixed 1 MiB device array inside the library, which every GPU that loads the
+ * library holds until the process exits.  The first call on each device looks
+ * up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture.  All calls share
+ * the one array and it keeps the last call's partial sums (each call
+ * overwrites every entry it reads, so nothing needs to start at zero): calls
+ * that overlap on the GPU -- two streams, or two host threads -- race and must
+ * be serialised by the caller. */
 int qgb_gf_action_sums_noalloc(const double* links_dev, const int32_t total_site[4], int32_t rect, double* out_dev,
                                void* stream);
 

@@ -220,6 +220,11 @@ int qgb_batch_create(qgb_batch** out, int32_t n_chains, const int32_t* total_sit
       }
       ci.d[i] = total_sites[4 * c + i];
       V *= ci.d[i];
+      // checked after every factor, so the product cannot wrap before it is refused
+      if (V > (1L << 34) || offs[c] + V > (1L << 34)) {
+        delete b;
+        return bfail(QGB_ERR_BAD_GEOMETRY, "qgb_batch_create: batch too large");
+      }
     }
     ci.V = V;
     ci.off = offs[c];

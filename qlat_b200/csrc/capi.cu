@@ -653,12 +653,15 @@ int qgb_field_create(qgb_field** out, const int32_t total_site[4], int32_t multi
   QGB_CHECK(precision == QGB_F64 || precision == QGB_F32, QGB_ERR_INVALID_ARG,
             "qgb_field_create: precision must be 64 or 32");
   long V = 1;
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 4; ++i)
     QGB_CHECK(total_site[i] >= 1 && total_site[i] <= (1 << 20), QGB_ERR_BAD_GEOMETRY,
               "qgb_field_create: each lattice extent must be in [1, 2^20]");
+  // checked after every factor: at most 2^34 sites times an extent of at most
+  // 2^20 stays below 2^54, so the product cannot wrap before it is refused
+  for (int i = 0; i < 4; ++i) {
     V *= total_site[i];
+    QGB_CHECK(V <= (1L << 34), QGB_ERR_BAD_GEOMETRY, "qgb_field_create: lattice too large");
   }
-  QGB_CHECK(V <= (1L << 34), QGB_ERR_BAD_GEOMETRY, "qgb_field_create: lattice too large");
   qgb_field_s* f = new qgb_field_s;
   for (int i = 0; i < 4; ++i) f->dims[i] = total_site[i];
   f->V = V;

@@ -1,14 +1,15 @@
 // noalloc.cu -- gauge-action sums for callers that cannot allocate GPU memory.
 //
 // Some callers of this library cannot call cudaMalloc: a host that has handed
-// the device memory to its own pool (a framework's caching allocator, a
-// fixed-budget solver), or code that records work into a CUDA graph, where a
-// cudaMalloc during stream capture fails and invalidates the capture.  The
-// regular entry points allocate lazily (the library context, reduction
-// scratch, staging), so this file provides one entry point that allocates
-// nothing: the sums of (Re tr P - 3) over all plaquettes and rectangles
-// (gf_sum_re_tr_plaq_node_no_comm / gf_sum_re_tr_rect_node_no_comm), read
-// straight from a caller-owned device buffer in the reference memory image.
+// the device memory to its own pool (a framework's caching allocator, a solver
+// with a fixed memory budget set at start-up), or one that cannot afford the
+// device-wide synchronisation an allocation or free may cause while its other
+// streams are busy.  The regular entry points allocate lazily (the library
+// context, reduction scratch, staging), so this file provides one entry point
+// that allocates nothing: the sums of (Re tr P - 3) over all plaquettes and
+// rectangles (gf_sum_re_tr_plaq_node_no_comm / gf_sum_re_tr_rect_node_no_comm),
+// read straight from a caller-owned device buffer in the reference memory
+// image.
 //
 // Its only scratch is the per-block partial-sum array below, a file-scope
 // device array that every GPU loading the library holds until the process
@@ -130,6 +131,7 @@ __global__ void __launch_bounds__(1024) k_finalize_noalloc(const double* partial
 namespace qgb
 {
 void set_last_error(const std::string& msg);  // capi.cu: the message qgb_last_error() returns
+void add_launches(int64_t n);                 // capi.cu: the count qgb_launch_count() returns
 }
 
 namespace
@@ -152,20 +154,32 @@ int qgb_gf_action_sums_noalloc(const double* links_dev, const int32_t total_site
 {
   if (!links_dev || !total_site || !out_dev)
     return noalloc_fail(QGB_ERR_INVALID_ARG, "qgb_gf_action_sums_noalloc: null argument");
+  // the kernels read links as 16-byte complex128 pairs and write doubles
+  if ((reinterpret_cast<uintptr_t>(links_dev) & 15) != 0 || (reinterpret_cast<uintptr_t>(out_dev) & 7) != 0)
+    return noalloc_fail(QGB_ERR_INVALID_ARG,
+                        "qgb_gf_action_sums_noalloc: links_dev must be 16-byte and out_dev 8-byte aligned");
   qgb::Geo g;
   g.V = 1;
+  g.off = 0;
   for (int i = 0; i < 4; ++i) {
     if (total_site[i] < 1 || total_site[i] > (1 << 20))
       return noalloc_fail(QGB_ERR_BAD_GEOMETRY, "qgb_gf_action_sums_noalloc: each lattice extent must be in [1, 2^20]");
     g.d[i] = total_site[i];
+  }
+  // The site count is checked against the scratch limit after every factor:
+  // a running product of at most 2^24 sites times an extent of at most 2^20
+  // stays below 2^44, so no product can wrap before it is refused.
+  const long max_sites = qgb::NOALLOC_MAX_BLOCKS * qgb::NOALLOC_BS;
+  for (int i = 0; i < 4; ++i) {
     g.V *= total_site[i];
+    if (g.V > max_sites)
+      return noalloc_fail(QGB_ERR_INVALID_ARG,
+                          "qgb_gf_action_sums_noalloc: lattice " + std::to_string(total_site[0]) + "x" +
+                              std::to_string(total_site[1]) + "x" + std::to_string(total_site[2]) + "x" +
+                              std::to_string(total_site[3]) + " has more sites than the fixed scratch supports (at most " +
+                              std::to_string(max_sites) + " sites)");
   }
   const long blocks = (g.V + qgb::NOALLOC_BS - 1) / qgb::NOALLOC_BS;
-  if (blocks > qgb::NOALLOC_MAX_BLOCKS)
-    return noalloc_fail(QGB_ERR_INVALID_ARG,
-                        "qgb_gf_action_sums_noalloc: lattice has " + std::to_string(g.V) +
-                            " sites; the fixed scratch supports at most " +
-                            std::to_string(qgb::NOALLOC_MAX_BLOCKS * qgb::NOALLOC_BS) + " sites");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return noalloc_fail(QGB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
@@ -184,12 +198,20 @@ int qgb_gf_action_sums_noalloc(const double* links_dev, const int32_t total_site
     }
     partials = g_noalloc_ptr[dev];
   }
+  // An error left pending by earlier, unrelated work is reported as such and
+  // left in place for its owner, so that an error after the launches below is
+  // theirs.
+  e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return noalloc_fail(QGB_ERR_CUDA, std::string("qgb_gf_action_sums_noalloc: an earlier CUDA call left an error "
+                                                  "pending, nothing launched: ") + cudaGetErrorString(e));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   qgb::k_action_aos_noalloc<<<(unsigned)blocks, qgb::NOALLOC_BS, 0, st>>>(
       g, reinterpret_cast<const qgb::Cx<double>*>(links_dev), rect ? 1 : 0, partials);
   qgb::k_finalize_noalloc<<<1, 1024, 0, st>>>(partials, (int)blocks, rect ? 1 : 0, out_dev);
   e = cudaGetLastError();
   if (e != cudaSuccess) return noalloc_fail(QGB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  qgb::add_launches(2);
   return QGB_OK;
 }
 
