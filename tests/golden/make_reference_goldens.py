@@ -2,8 +2,8 @@
 """Extract the golden values that pin the pure-gauge path from the
 reference's own test logs into reference_goldens.json.
 
-Run in a checkout that has the reference source tree (default
-/root/reference, or pass its path).  Sources:
+Run in a checkout that has the reference source tree, passing its path as
+the first argument or in QLAT_REFERENCE_ROOT (there is no default).  Sources:
   examples-cpp/hmc/log                        C++ force-gradient HMC, plaq per trajectory
   examples-cpp/flowed-hmc/log                 C++ flowed HMC (masked invertible flows), plaq per trajectory
   examples-py/hmc-pure-gauge.log.json         Python HMC, plaq and delta_h per trajectory
@@ -24,7 +24,9 @@ import sys
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QLAT_REFERENCE_ROOT")
+    if not ref:
+        sys.exit("usage: make_reference_goldens.py <reference source tree> (or set QLAT_REFERENCE_ROOT)")
     out = {}
     # C++ HMC log
     lines = open(os.path.join(ref, "examples-cpp/hmc/log")).read().splitlines()
