@@ -100,6 +100,18 @@ int qgb_field_download(const qgb_field* f, double* host);
  * host_next when the copy engine reaches it: keep that buffer unchanged until
  * the next call.  Overlap needs pinned host memory. */
 int qgb_field_upload_pipelined(qgb_field* f, const double* host_now, const double* host_next);
+/* Queue a copy of f, in the reference memory image, into `host` behind the
+ * work queued so far, without waiting: the field is converted into one of two
+ * library staging slots on the library stream and copied to the host on a
+ * library download stream, so the copy overlaps the work queued after it
+ * (pinned host memory).  `host` holds the data once qgb_synchronize (or
+ * qgb_field_download_join followed by a synchronisation of the library
+ * stream) has returned; keep it unread and unchanged until then.  A third
+ * download waits for the first's copy to leave its slot. */
+int qgb_field_download_async(const qgb_field* f, double* host);
+/* Orders the library stream after every queued download (qgb_synchronize does
+ * this itself). */
+int qgb_field_download_join(void);
 /* Same, from / into a device buffer in the reference memory image. */
 int qgb_field_upload_device(qgb_field* f, const double* dev);
 int qgb_field_download_device(const qgb_field* f, double* dev);
@@ -566,12 +578,6 @@ int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int3
  * be serialised by the caller. */
 int qgb_gf_action_sums_noalloc(const double* links_dev, const int32_t total_site[4], int32_t rect, double* out_dev,
                                void* stream);
-
-/* FMA rate of the current device in TFLOP/s (2 flop per FMA), from 16
- * independent FMA chains per thread over 16 blocks of 256 threads per SM:
- * kind 0 scalar FP32, 1 packed f32x2, 2 FP64; best of reps launches after one
- * warm-up (no counterpart in the reference). */
-int qgb_fma_rate(int32_t kind, int32_t reps, double* tflops);
 
 /* Number of kernels this library has launched since it was loaded. */
 int qgb_launch_count(int64_t* out);

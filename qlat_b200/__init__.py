@@ -140,6 +140,12 @@ def synchronize():
     call("qgb_synchronize")
 
 
+def download_join():
+    """Order the library stream after every queued GaugeField.download_host_async."""
+    from ._lib import call
+    call("qgb_field_download_join")
+
+
 def release_field_pool() -> int:
     """Free the device storage the library keeps from destroyed fields for
     reuse (torch.cuda.empty_cache for this library's fields); returns the

@@ -73,7 +73,6 @@ SIGNATURES = {
     "qgb_field_glb_min_max": [c_field, c_dbl_p, c_dbl_p],
     "qgb_field_glb_sum_tslice": [c_field, ctypes.c_int32, c_dbl_p],
     "qgb_field_abs": [c_field],
-    "qgb_fma_rate": [ctypes.c_int32, ctypes.c_int32, c_dbl_p],
     "qgb_gm_hamilton_node_sites": [c_field, ctypes.c_int64, ctypes.c_int64, c_dbl_p],
     "qgb_gf_action_sums_sites": [c_field, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, c_dbl_p],
     "qgb_gf_hamilton_node_sites": [c_field, ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int64,
@@ -88,6 +87,8 @@ SIGNATURES = {
     "qgb_field_download": [c_field, c_dbl_p],
     "qgb_field_upload_device": [c_field, ctypes.c_void_p],
     "qgb_field_upload_pipelined": [c_field, ctypes.c_void_p, ctypes.c_void_p],
+    "qgb_field_download_async": [c_field, ctypes.c_void_p],
+    "qgb_field_download_join": [],
     "qgb_field_download_device": [c_field, ctypes.c_void_p],
     "qgb_field_copy": [c_field, c_field],
     "qgb_field_set_zero": [c_field],
@@ -165,6 +166,12 @@ SIGNATURES = {
 _lib = None
 
 
+# exported for the benchmark, not declared in include/qlat_b200.h
+INTERNAL = {
+    "qgb_fma_rate": [ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+}
+
+
 def load() -> ctypes.CDLL:
     """Load the shared library (building nothing).  Raises RuntimeError if absent."""
     global _lib
@@ -174,7 +181,7 @@ def load() -> ctypes.CDLL:
         raise RuntimeError(
             f"{LIB_PATH} is missing: build it with `python -m qlat_b200.build` (nvcc, sm_100a)")
     lib = ctypes.CDLL(LIB_PATH)
-    for name, args in SIGNATURES.items():
+    for name, args in {**SIGNATURES, **INTERNAL}.items():
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = ctypes.c_int

@@ -83,6 +83,16 @@ struct Ctx {
   // device staging slots; slot i holds the copy of up_host[i] once up_ready[i]
   // has fired, and up_order[i] orders its next copy after the work queued on
   // the library stream (the conversion that last read the slot included)
+  // asynchronous downloads (qgb_field_download_async): a stream of their own,
+  // so they run on the other copy engine beside the uploads; slot i is free
+  // again once dn_done[i] has fired
+  cudaStream_t dn_stream = nullptr;
+  void* dn_buf[2] = {nullptr, nullptr};
+  size_t dn_cap[2] = {0, 0};
+  cudaEvent_t dn_ready[2] = {nullptr, nullptr};
+  cudaEvent_t dn_done[2] = {nullptr, nullptr};
+  bool dn_used[2] = {false, false};
+  int dn_next = 0;
   cudaStream_t copy_stream = nullptr;
   void* up_buf[2] = {nullptr, nullptr};
   size_t up_cap[2] = {0, 0};
@@ -115,8 +125,10 @@ int ensure_ctx()
   QGB_TRY_CUDA(cudaGetDevice(&g_ctx.device));
   QGB_TRY_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
   g_ctx.own_stream = true;
-  QGB_TRY_CUDA(cudaMalloc(&g_ctx.results, Ctx::NSLOT * sizeof(double)));
-  QGB_TRY_CUDA(cudaMallocHost(&g_ctx.results_host, Ctx::NSLOT * sizeof(double)));
+  // NSLOT result slots, then the flag that a force kernel's wait gave up (site map 6)
+  QGB_TRY_CUDA(cudaMalloc(&g_ctx.results, (Ctx::NSLOT + 1) * sizeof(double)));
+  QGB_TRY_CUDA(cudaMallocHost(&g_ctx.results_host, (Ctx::NSLOT + 1) * sizeof(double)));
+  QGB_TRY_CUDA(cudaMemset(g_ctx.results, 0, (Ctx::NSLOT + 1) * sizeof(double)));
   QGB_TRY_CUDA(cudaMalloc(&g_ctx.ambiguous, sizeof(int)));
   QGB_TRY_CUDA(cudaMemset(g_ctx.ambiguous, 0, sizeof(int)));
   qgb::init_constants();
@@ -241,11 +253,26 @@ void release_field_pool()
   g_ctx.field_pool_bytes = 0;
 }
 
+// The wait-gave-up flag of the force kernels: reported (and cleared) as
+// QGB_ERR_TIMEOUT once the stream has reached it.
+int check_wave_flag()
+{
+  if (g_ctx.results_host[Ctx::NSLOT] == 0.0) return QGB_OK;
+  g_ctx.results_host[Ctx::NSLOT] = 0.0;
+  QGB_TRY_CUDA(cudaMemsetAsync(g_ctx.results + Ctx::NSLOT, 0, sizeof(double), g_ctx.stream));
+  return fail(QGB_ERR_TIMEOUT, "force kernel: a wait for the corner products of neighbouring time slices gave up; "
+                               "its results are invalid");
+}
+
 int read_results(int slot, int n, double* out)
 {
   QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.results_host + slot, g_ctx.results + slot, n * sizeof(double),
                                cudaMemcpyDeviceToHost, g_ctx.stream));
+  QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.results_host + Ctx::NSLOT, g_ctx.results + Ctx::NSLOT, sizeof(double),
+                               cudaMemcpyDeviceToHost, g_ctx.stream));
   QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  const int rc = check_wave_flag();
+  if (rc != QGB_OK) return rc;
   for (int i = 0; i < n; ++i) out[i] = g_ctx.results_host[slot + i];
   return QGB_OK;
 }
@@ -346,11 +373,49 @@ double gf_hamilton_from(double sp, double sr, double beta, double c1)
 
 // ---- elementary launches with profiling -----------------------------------
 
+// The corner field of force site map 5 (FP32 only): a scratch of 16 color
+// matrices per site, filled from a.U by the corner pass.  When `variant`
+// uses it, sets a.corners and queues the pass (profiled as "corners" when
+// `prof`); returns the number of kernels queued.
 template <typename R>
-int force(const Geo& g, qgb::ForceMode mode, const ForceArgs& a)
+int prepare_corners(const Geo& g, int variant, ForceArgs& a, bool prof, int* kernels)
+{
+  int bs, minb, split, map;
+  *kernels = 0;
+  if (sizeof(R) != 4 || !qgb::force_variant_info_c(variant, &bs, &minb, &split, &map) || (map != 5 && map != 6))
+    return QGB_OK;
+  if (g.off != 0 || qgb::padded_sites(g.V) * 144 >= 2147483647L) return QGB_OK;  // the launcher runs map 3
+  void* c = nullptr;
+  QGB_RC(get_scratch((size_t)qgb::padded_sites(g.V) * qgb::N_CORNER_FIELDS * 18 * sizeof(R), 40, &c));
+  a.corners = c;
+  // site map 6 (the same conditions as its launcher): the corner items run
+  // inside the force launch (k_force_wave): its work ticket and per-slice
+  // counters, and the flag that a wait gave up; otherwise map 5's pass
+  if (map == 6 && g.d[3] >= 6 && ((long)g.d[0] * g.d[1] * g.d[2]) % 32 == 0) {
+    void* w = nullptr;
+    QGB_RC(get_scratch((size_t)(g.d[3] + 1) * sizeof(int), 41, &w));
+    a.wave = static_cast<int*>(w);
+    a.wave_err = g_ctx.results + Ctx::NSLOT;
+    return QGB_OK;
+  }
+  if (prof) {
+    Prof p("corners");
+    QGB_TRY_CUDA(qgb::launch_corners<R>(g, a.U, c, g_ctx.stream));
+  } else {
+    QGB_TRY_CUDA(qgb::launch_corners<R>(g, a.U, c, g_ctx.stream));
+  }
+  *kernels = 1;
+  return QGB_OK;
+}
+
+template <typename R>
+int force(const Geo& g, qgb::ForceMode mode, const ForceArgs& a0)
 {
   static const char* names[] = {"force", "force_update", "force_evolve", "flow_stage", "force_update_evolve"};
-  const int v = g_force_variant[sizeof(R) == 8 ? 0 : 1][a.c1 != 0.0 ? 1 : 0];
+  const int v = g_force_variant[sizeof(R) == 8 ? 0 : 1][a0.c1 != 0.0 ? 1 : 0];
+  ForceArgs a = a0;
+  int nk = 0;
+  QGB_RC(prepare_corners<R>(g, v, a, true, &nk));
   Prof p(names[mode]);
   QGB_TRY_CUDA(qgb::launch_force<R>(g, mode, a, v, g_ctx.stream));
   return QGB_OK;
@@ -635,10 +700,22 @@ int qgb_set_stream(void* stream)
   return QGB_OK;
 }
 
+int qgb_field_download_join(void)
+{
+  QGB_CTX();
+  for (int k = 0; k < 2; ++k)
+    if (g_ctx.dn_used[k]) QGB_TRY_CUDA(cudaStreamWaitEvent(g_ctx.stream, g_ctx.dn_done[k], 0));
+  return QGB_OK;
+}
+
 int qgb_synchronize(void)
 {
   QGB_CTX();
+  QGB_RC(qgb_field_download_join());
+  QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.results_host + Ctx::NSLOT, g_ctx.results + Ctx::NSLOT, sizeof(double),
+                               cudaMemcpyDeviceToHost, g_ctx.stream));
   QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  QGB_RC(check_wave_flag());
   return QGB_OK;
 }
 
@@ -832,6 +909,40 @@ int qgb_field_download(const qgb_field* f, double* host)
   QGB_RC(download_to_device_aos(f, g_ctx.staging));
   QGB_TRY_CUDA(cudaMemcpyAsync(host, g_ctx.staging, bytes, cudaMemcpyDeviceToHost, g_ctx.stream));
   QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return QGB_OK;
+}
+
+int qgb_field_download_async(const qgb_field* f, double* host)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, "qgb_field_download_async"));
+  QGB_CHECK(host, QGB_ERR_INVALID_ARG, "qgb_field_download_async: null host buffer");
+  const size_t bytes = (size_t)n_reals(f) * sizeof(double);
+  if (!g_ctx.dn_stream) {
+    QGB_TRY_CUDA(cudaStreamCreateWithFlags(&g_ctx.dn_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+      QGB_TRY_CUDA(cudaEventCreateWithFlags(&g_ctx.dn_ready[k], cudaEventDisableTiming));
+      QGB_TRY_CUDA(cudaEventCreateWithFlags(&g_ctx.dn_done[k], cudaEventDisableTiming));
+    }
+  }
+  const int i = g_ctx.dn_next;
+  // the slot's previous host copy must have left it before the conversion refills it
+  if (g_ctx.dn_used[i]) QGB_TRY_CUDA(cudaStreamWaitEvent(g_ctx.stream, g_ctx.dn_done[i], 0));
+  if (g_ctx.dn_cap[i] < bytes) {
+    QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+    if (g_ctx.dn_buf[i]) QGB_TRY_CUDA(cudaFree(g_ctx.dn_buf[i]));
+    g_ctx.dn_buf[i] = nullptr;
+    g_ctx.dn_cap[i] = 0;
+    QGB_TRY_CUDA(cudaMalloc(&g_ctx.dn_buf[i], bytes));
+    g_ctx.dn_cap[i] = bytes;
+  }
+  QGB_RC(download_to_device_aos(f, (double*)g_ctx.dn_buf[i]));
+  QGB_TRY_CUDA(cudaEventRecord(g_ctx.dn_ready[i], g_ctx.stream));
+  QGB_TRY_CUDA(cudaStreamWaitEvent(g_ctx.dn_stream, g_ctx.dn_ready[i], 0));
+  QGB_TRY_CUDA(cudaMemcpyAsync(host, g_ctx.dn_buf[i], bytes, cudaMemcpyDeviceToHost, g_ctx.dn_stream));
+  QGB_TRY_CUDA(cudaEventRecord(g_ctx.dn_done[i], g_ctx.dn_stream));
+  g_ctx.dn_used[i] = true;
+  g_ctx.dn_next = 1 - i;
   return QGB_OK;
 }
 
@@ -1659,7 +1770,12 @@ int qgb_autotune_force(const qgb_field* gf, double c1, int32_t reps, int32_t* be
   const int nv = qgb::force_variant_count();
   for (int v = 0; v < nv; ++v) {
     ForceArgs a = fargs(gf->d, P, 3.0, c1, 1e-3);
-    auto launch = [&]() {
+    int nk = 0;
+    // each timed launch is the corner pass (site map 5) + the force kernel
+    auto launch = [&]() -> cudaError_t {
+      const int rc = gf->prec == QGB_F64 ? prepare_corners<double>(g, v, a, false, &nk)
+                                         : prepare_corners<float>(g, v, a, false, &nk);
+      if (rc != QGB_OK) return cudaErrorUnknown;
       return gf->prec == QGB_F64 ? qgb::launch_force<double>(g, qgb::FORCE_UPDATE, a, v, g_ctx.stream)
                                  : qgb::launch_force<float>(g, qgb::FORCE_UPDATE, a, v, g_ctx.stream);
     };
@@ -1671,7 +1787,7 @@ int qgb_autotune_force(const qgb_field* gf, double c1, int32_t reps, int32_t* be
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     ms /= reps;
-    g_launches += reps + 1;
+    g_launches += (reps + 1) * (1 + nk);
     if (ms < best_t) {
       best_t = ms;
       best_v = v;
@@ -1698,7 +1814,11 @@ int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int3
   QGB_TRY_CUDA(cudaMemsetAsync(P, 0, gf->bytes, g_ctx.stream));
   cudaEvent_t e0 = get_event(), e1 = get_event();
   ForceArgs a = fargs(gf->d, P, 3.0, c1, 1e-3);
-  auto launch = [&]() {
+  int nk = 0;
+  auto launch = [&]() -> cudaError_t {
+    const int rc = gf->prec == QGB_F64 ? prepare_corners<double>(g, variant, a, false, &nk)
+                                       : prepare_corners<float>(g, variant, a, false, &nk);
+    if (rc != QGB_OK) return cudaErrorUnknown;
     return gf->prec == QGB_F64 ? qgb::launch_force<double>(g, qgb::FORCE_UPDATE, a, variant, g_ctx.stream)
                                : qgb::launch_force<float>(g, qgb::FORCE_UPDATE, a, variant, g_ctx.stream);
   };
@@ -1711,7 +1831,7 @@ int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int3
   cudaEventElapsedTime(&ms, e0, e1);
   g_ctx.event_pool.push_back(e0);
   g_ctx.event_pool.push_back(e1);
-  g_launches += reps + 1;
+  g_launches += (reps + 1) * (1 + nk);
   *ms_per_launch = ms / reps;
   return QGB_OK;
 }

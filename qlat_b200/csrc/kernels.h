@@ -54,7 +54,17 @@ struct ForceArgs {
   void* ev;         // UPDATE_EVOLVE: W, evolved in place (never read at other links, so W != U)
   double ev_eps;    // UPDATE_EVOLVE: exponential step of W
   int ev_unit;      // UPDATE_EVOLVE: 0 none, 1 unitarize in R, 2 unitarize with FP64 arithmetic
+  void* corners;    // site maps 5, 6: scratch for the 16 two-link products per site (corner_id), or null
+  int* wave;        // site map 6: 1 + T ints (work ticket, per-slice corner counts), zeroed by the launcher
+  double* wave_err; // site map 6: set to 1 when a wait for corner work gives up
 };
+
+// Site map 5 of the force kernel keeps, per site, the 4 double links
+// D_a(x) = U_a(x) U_a(x+a) (component a) and the 12 corners
+// P_ab(x) = U_a(x) U_b(x+a), a != b (component corner_id(a, b)), as a
+// 16-component color-matrix field in the blocked layout.
+__host__ __device__ __forceinline__ int corner_id(int a, int b) { return 4 + 3 * a + (b < a ? b : b - 1); }
+static const int N_CORNER_FIELDS = 16;
 
 void init_constants();  // SHA-256 and log tables into constant memory (per device)
 
@@ -62,6 +72,8 @@ void init_constants();  // SHA-256 and log tables into constant memory (per devi
 template <typename R>
 cudaError_t launch_force(const Geo& g, ForceMode mode, const ForceArgs& a, int variant, cudaStream_t st);
 int force_variant_count();
+template <typename R>
+cudaError_t launch_corners(const Geo& g, const void* U, void* C, cudaStream_t st);
 // All chains of a batch in one launch (offs: nchain + 1 ascending offsets on the device).
 template <typename R>
 cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,

@@ -1,6 +1,14 @@
 // probes.cu -- hardware-rate measurements used to put the force kernels'
 // counters in context (no counterpart in the reference): the FMA rate of the
 // device with scalar FP32 chains, packed f32x2 chains and FP64 chains.
+// Internal: exported for the benchmark's compute roofline, not part of the
+// public header.
+//
+//   int qgb_fma_rate(int32_t kind, int32_t reps, double* tflops)
+//   FMA rate of the current device in TFLOP/s (2 flop per FMA), from 16
+//   independent FMA chains per thread over 16 blocks of 256 threads per SM:
+//   kind 0 scalar FP32, 1 packed f32x2, 2 FP64; best of reps launches after
+//   one warm-up.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -75,6 +83,8 @@ int pfail(int code, const std::string& m)
 }  // namespace
 
 extern "C" {
+
+int qgb_fma_rate(int32_t kind, int32_t reps, double* tflops);
 
 int qgb_fma_rate(int32_t kind, int32_t reps, double* tflops)
 {

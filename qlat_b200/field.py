@@ -276,6 +276,12 @@ class Field:
         call("qgb_field_upload_pipelined", self.handle, ctypes.c_void_p(ptr_now),
              None if ptr_next is None else ctypes.c_void_p(ptr_next))
 
+    def download_host_async(self, ptr: int) -> None:
+        """Queue a copy of the field, in the reference memory image, into host
+        memory at ``ptr`` (pinned) without waiting; the data is there after
+        ``qlat_b200.synchronize()`` (``qgb_field_download_async``)."""
+        call("qgb_field_download_async", self.handle, ctypes.c_void_p(ptr))
+
     def upload_device(self, ptr: int) -> None:
         """Copy from a device buffer (e.g. a torch CUDA tensor's data_ptr) in
         the reference memory image."""

@@ -193,9 +193,12 @@ def test_errors_are_reported(q):
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_every_force_variant(q, oracle, prec):
-    """All launch shapes of the autotuner compute the same force."""
-    ts = (3, 4, 5, 6)
+@pytest.mark.parametrize("ts", [(3, 4, 5, 6), (4, 4, 4, 8), (8, 4, 2, 6)])
+def test_every_force_variant(q, oracle, prec, ts):
+    """All launch shapes of the autotuner compute the same force.  3 x 4 x 5 x 6
+    has time slices of 60 sites (the corner-wave shapes fall back to a
+    separate corner pass); 4 x 4 x 4 x 8 and 8 x 4 x 2 x 6 run them as one
+    persistent launch (slices of 64 sites, 8 and 6 slices)."""
     gf, ref = hot_start(q, oracle, ts)
     g = gf if prec == "f64" else gf.copy(precision=q.F32)
     tol = 1e-13 if prec == "f64" else 2e-6
@@ -215,6 +218,39 @@ def test_every_force_variant(q, oracle, prec):
     finally:
         for rect, v in saved.items():
             q.force_set_variant(P, rect, v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("c1", [-0.331, 0.0])
+def test_force_shapes_agree_in_every_mode(q, c1):
+    """The FP32 force shapes used by the mixed trajectory -- two-row chains
+    (variant 10), the corner field with a separate pass (14) and the corner
+    wave in one launch (19) -- give the same mixed trajectory (force +
+    exponential, force + momentum update + link update) and the same FP32
+    flow stage, to FP32 rounding; the wave's waits never give up (no
+    QGB_ERR_TIMEOUT from the read-backs)."""
+    ts = (4, 4, 4, 8)
+    ga = q.GaugeAction(2.13, c1)
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("shapes").split("gf-init"), 0.3, 1)
+    gm = q.GaugeMomentum(gf.geo)
+    gm.set_rand(q.RngState("shapes").split("mom"), 1.0)
+    saved = q.force_get_variant(q.F32, c1 != 0.0)
+    res = {}
+    try:
+        for v in (10, 14, 19):
+            q.force_set_variant(q.F32, c1 != 0.0, v)
+            g, m = gf.copy(), gm.copy()
+            dh = q.run_hmc_evolve_pure_gauge(m, g, ga, None, 4, 1.0, precision="mixed", reunit_interval=4)
+            w = gf.copy(precision=q.F32)
+            q.gf_wilson_flow_step(w, 0.05, c1=c1)
+            res[v] = (dh, np.asarray(g), np.asarray(w))
+    finally:
+        q.force_set_variant(q.F32, c1 != 0.0, saved)
+    for v in (14, 19):
+        assert abs(res[v][0] - res[10][0]) < 1e-4 * max(1.0, abs(res[10][0])), (v, res[v][0], res[10][0])
+        assert nrel(res[v][1], res[10][1]) < 1e-6, v
+        assert nrel(res[v][2], res[10][2]) < 1e-6, v
 
 
 @pytest.mark.gpu
@@ -243,6 +279,30 @@ def test_upload_pipelined(q):
         gf.upload_host_pipelined(bufs[0].data_ptr(), bufs[1].data_ptr())
         gf.upload_host_pipelined(bufs[2].data_ptr(), None)
         assert np.abs(np.asarray(gf) - bufs[2].numpy()).max() <= tol * 10
+
+
+@pytest.mark.gpu
+def test_download_async(q):
+    """qgb_field_download_async: three queued downloads in a row (the third
+    reuses the first's staging slot), FP64 and FP32 fields, into pinned host
+    buffers, equal the synchronous download once qgb_synchronize returns, also
+    when the field changes after a download was queued."""
+    import torch
+    geo = q.Geometry((4, 4, 4, 8))
+    V = geo.total_volume
+    fields = []
+    for k, prec in enumerate((q.F64, q.F32, q.F64)):
+        f = q.GaugeField(geo, precision=prec)
+        f.set_rand(q.RngState(f"dl-{k}"), 0.5, 1)
+        fields.append(f)
+    expect = [np.asarray(f).copy() for f in fields]
+    hosts = [torch.zeros((V, 4, 3, 3), dtype=torch.complex128, pin_memory=True) for _ in fields]
+    for f, h in zip(fields, hosts):
+        f.download_host_async(h.data_ptr())
+    fields[0].set_rand(q.RngState("dl-changed"), 0.5, 1)  # queued after the first download
+    q.synchronize()
+    for e, h in zip(expect, hosts):
+        assert np.array_equal(h.numpy(), e)
 
 
 @pytest.mark.gpu
