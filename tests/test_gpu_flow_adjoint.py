@@ -55,6 +55,30 @@ def test_flow_vjp_matches_finite_differences(q, every):
     assert worst < 1e-7, worst
 
 
+def test_flow_vjp_at_the_differentiation_workload(q):
+    """The differentiation workload itself: 16^4, hot start at scale 0.4,
+    40 RK3 steps of 0.05 to t = 2, checkpoints every 8, loss = Wilson gauge
+    action (beta 5.8) of the flowed field; the adjoint against 4-point central
+    finite differences (h = 1e-4, FP64) along 4 random su(3) directions."""
+    ts = (16, 16, 16, 16)
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("b200-c4-adjoint").split("gf-init"), 0.4, 1)
+    eps, steps, beta = 0.05, 40, 5.8
+    loss, grad = q.gf_flow_action_grad(gf, eps, steps, beta, checkpoint_every=8)
+    assert abs(loss - q.gf_flow_action(gf, eps, steps, beta)) < 1e-10 * abs(loss)
+    for k in range(4):
+        X = q.GaugeMomentum(gf.geo)
+        X.set_rand(q.RngState(f"c4-direction-{k}"), 1.0)
+
+        def L(h):
+            u = gf.copy()
+            q.gf_evolve(u, X, h)
+            return q.gf_flow_action(u, eps, steps, beta)
+
+        fd = fd4(L, 1e-4)
+        assert abs(fd - ip(grad, X)) < 1e-7 * abs(fd), (k, fd, ip(grad, X))
+
+
 def test_flow_vjp_against_reference_forward(q, oracle):
     """Finite differences of the oracle's flow (the reference algorithm) agree with the GPU adjoint."""
     ts = (3, 4, 4, 5)
