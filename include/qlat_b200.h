@@ -229,9 +229,11 @@ int qgb_gf_wilson_flow(qgb_field* gf, double flow_time, int32_t steps, double c1
  * gradient of the gauge action is -2 x set_gm_force.
  *
  * Vector-Jacobian product of `steps` RK3 flow steps of size epsilon
- * (gf_wilson_flow_step, wilson-flow.cpp:29-50; Wilson flow, c1 = 0): given the
- * cotangent at the flowed field, writes the cotangent at gf.  Forward states
- * are checkpointed every `checkpoint_every` steps and recomputed. */
+ * (gf_wilson_flow_step, wilson-flow.cpp:29-50, with the flow force of
+ * GaugeAction(3, c1), set_wilson_flow_z at wilson-flow.cpp:12-17: Wilson,
+ * Iwasaki, DBW2 or any c1): given the cotangent at the flowed field, writes
+ * the cotangent at gf.  Forward states are checkpointed every
+ * `checkpoint_every` steps and recomputed. */
 int qgb_gf_wilson_flow_vjp(const qgb_field* gf, double epsilon, int32_t steps, double c1, int32_t checkpoint_every,
                            const qgb_field* cotangent, qgb_field* grad);
 /* L = gf_hamilton_node(V_t, GaugeAction(beta, c1_loss)) of the flowed field

@@ -74,29 +74,74 @@ __device__ __forceinline__ M3<R> commutator(const M3<R>& a, const M3<R>& b)
   return r;
 }
 
-// lambda_out = lambda_local + a (DF[Y] + [F, Y]) at every link, F the Wilson
-// force at beta (hmc.cpp:64-75 with c1 = 0), DF[Y] its derivative along Y.
+// The links of the staple paths at signed direction e = s nu as dual
+// matrices (positions x + a mu + b e, as SignedDir in force_impl.cuh): hop is
+// the link from there along +e, back the one along -e, umu U_mu there.
 template <typename R>
+struct DualDir {
+  const CField<R>& U;
+  const CField<R>& Y;
+  const Geo& g;
+  const Coord& x;
+  int mu, nu, s;
+  __device__ __forceinline__ Dual<R> umu(int a, int b, bool dagger = false) const
+  {
+    return dlink(U, Y, site_rt(g, x, mu, a, nu, b * s), mu, dagger);
+  }
+  __device__ __forceinline__ Dual<R> hop(int a, int b) const
+  {
+    return dlink(U, Y, site_rt(g, x, mu, a, nu, b * s + (s < 0 ? -1 : 0)), nu, s < 0);
+  }
+  __device__ __forceinline__ Dual<R> back(int a, int b) const
+  {
+    return dlink(U, Y, site_rt(g, x, mu, a, nu, b * s + (s < 0 ? 0 : -1)), nu, s > 0);
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ void dual_acc(M3<R>& S, M3<R>& dS, R w, const Dual<R>& P)
+{
+  axpy(S, w, P.v);
+  axpy(dS, w, P.d);
+}
+
+// lambda_out = lambda_local + a (DF[Y] + [F, Y]) at every link, F the force
+// of GaugeAction(beta, c1) (hmc.cpp:48-75: staples (1 - 8 c1) plaq + c1 rect,
+// the paths of hmc.cpp:27-46), DF[Y] its derivative along Y, every path
+// walked as a product of dual matrices.
+template <typename R, bool RECT>
 __global__ void __launch_bounds__(128) k_force_vjp(Geo g, const Cx<R>* Up, const Cx<R>* Yp, const Cx<R>* lam_local,
-                                                   Cx<R>* lam_out, double beta, double a)
+                                                   Cx<R>* lam_out, double beta, double c1, double a)
 {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= g.V) return;
   const int mu = blockIdx.y;
   const CField<R> U{Up, g.V}, Y{Yp, g.V};
   const Coord x = coord_of(g, s);
+  const R cp = R(1.0 - 8.0 * c1), cr = R(c1);
   M3<R> S = m3_zero<R>(), dS = m3_zero<R>();
 #pragma unroll 1
   for (int k = 0; k < 6; ++k) {
-    const int nu = (mu + 1 + (k >> 1)) & 3;
-    const int sg = (k & 1) ? -1 : 1;
-    // B = hop(x) U_mu(x+e); staple = B back(x+e+mu)
-    const Dual<R> hop = dlink(U, Y, site_rt(g, x, mu, 0, nu, sg < 0 ? -1 : 0), nu, sg < 0);
-    const Dual<R> lmu = dlink(U, Y, site_rt(g, x, mu, 0, nu, sg), mu, false);
-    const Dual<R> B = dmul(hop, lmu);
-    const Dual<R> back = dlink(U, Y, site_rt(g, x, mu, 1, nu, sg < 0 ? -1 : 0), nu, sg > 0);
-    S = add_mul(S, B.v, back.v);
-    dS = add_mul(add_mul(dS, B.d, back.v), B.v, back.d);
+    const DualDir<R> d{U, Y, g, x, mu, (mu + 1 + (k >> 1)) & 3, (k & 1) ? -1 : 1};
+    // plaq (nu, mu, -nu) = hop(x) U_mu(x+e) back(x+e+mu)
+    dual_acc(S, dS, cp, dmul(dmul(d.hop(0, 0), d.umu(0, 1)), d.back(1, 1)));
+    if (RECT) {
+      // rect1 (nu, nu, mu, -nu, -nu)
+      Dual<R> C = dmul(d.hop(0, 0), d.hop(0, 1));
+      C = dmul(C, d.umu(0, 2));
+      C = dmul(C, d.back(1, 2));
+      dual_acc(S, dS, cr, dmul(C, d.back(1, 1)));
+      // rect2 (nu, mu, mu, -nu, -mu)
+      C = dmul(d.hop(0, 0), d.umu(0, 1));
+      C = dmul(C, d.umu(1, 1));
+      C = dmul(C, d.back(2, 1));
+      dual_acc(S, dS, cr, dmul(C, d.umu(1, 0, true)));
+      // rect3 (-mu, nu, mu, mu, -nu)
+      C = dmul(d.umu(-1, 0, true), d.hop(-1, 0));
+      C = dmul(C, d.umu(-1, 1));
+      C = dmul(C, d.umu(0, 1));
+      dual_acc(S, dS, cr, dmul(C, d.back(1, 1)));
+    }
   }
   const M3<R> u = U.ld(s, mu);
   const M3<R> y = Y.ld(s, mu);
@@ -203,11 +248,15 @@ __global__ void k_matrix_to_basis(long V, int m, const Cx<R>* fc, R* basis)
 
 template <typename R>
 cudaError_t launch_force_vjp(const Geo& g, const void* U, const void* Y, const void* lam_local, void* lam_out,
-                             double beta, double a, cudaStream_t st)
+                             double beta, double c1, double a, cudaStream_t st)
 {
   dim3 grid((unsigned)((g.V + 127) / 128), 4);
-  k_force_vjp<R><<<grid, 128, 0, st>>>(g, (const Cx<R>*)U, (const Cx<R>*)Y, (const Cx<R>*)lam_local, (Cx<R>*)lam_out,
-                                       beta, a);
+  if (c1 != 0.0)
+    k_force_vjp<R, true><<<grid, 128, 0, st>>>(g, (const Cx<R>*)U, (const Cx<R>*)Y, (const Cx<R>*)lam_local,
+                                               (Cx<R>*)lam_out, beta, c1, a);
+  else
+    k_force_vjp<R, false><<<grid, 128, 0, st>>>(g, (const Cx<R>*)U, (const Cx<R>*)Y, (const Cx<R>*)lam_local,
+                                                (Cx<R>*)lam_out, beta, 0.0, a);
   return cudaGetLastError();
 }
 
@@ -245,7 +294,7 @@ cudaError_t launch_matrix_to_basis(long V, int m, const void* fc, void* basis, c
 
 #define QGB_ADJ_INST(R)                                                                                          \
   template cudaError_t launch_force_vjp<R>(const Geo&, const void*, const void*, const void*, void*, double, double, \
-                                           cudaStream_t);                                                       \
+                                           double, cudaStream_t);                                               \
   template cudaError_t launch_flow_adj_local<R>(long, const void*, const void*, const void*, double, double, void*, \
                                                 void*, cudaStream_t);                                           \
   template cudaError_t launch_dexp_adjoint<R>(long, int, const void*, const void*, void*, cudaStream_t);        \

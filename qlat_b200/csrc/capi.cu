@@ -125,10 +125,8 @@ int ensure_ctx()
   QGB_TRY_CUDA(cudaGetDevice(&g_ctx.device));
   QGB_TRY_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
   g_ctx.own_stream = true;
-  // NSLOT result slots, then the flag that a force kernel's wait gave up (site map 6)
-  QGB_TRY_CUDA(cudaMalloc(&g_ctx.results, (Ctx::NSLOT + 1) * sizeof(double)));
-  QGB_TRY_CUDA(cudaMallocHost(&g_ctx.results_host, (Ctx::NSLOT + 1) * sizeof(double)));
-  QGB_TRY_CUDA(cudaMemset(g_ctx.results, 0, (Ctx::NSLOT + 1) * sizeof(double)));
+  QGB_TRY_CUDA(cudaMalloc(&g_ctx.results, Ctx::NSLOT * sizeof(double)));
+  QGB_TRY_CUDA(cudaMallocHost(&g_ctx.results_host, Ctx::NSLOT * sizeof(double)));
   QGB_TRY_CUDA(cudaMalloc(&g_ctx.ambiguous, sizeof(int)));
   QGB_TRY_CUDA(cudaMemset(g_ctx.ambiguous, 0, sizeof(int)));
   qgb::init_constants();
@@ -253,26 +251,11 @@ void release_field_pool()
   g_ctx.field_pool_bytes = 0;
 }
 
-// The wait-gave-up flag of the force kernels: reported (and cleared) as
-// QGB_ERR_TIMEOUT once the stream has reached it.
-int check_wave_flag()
-{
-  if (g_ctx.results_host[Ctx::NSLOT] == 0.0) return QGB_OK;
-  g_ctx.results_host[Ctx::NSLOT] = 0.0;
-  QGB_TRY_CUDA(cudaMemsetAsync(g_ctx.results + Ctx::NSLOT, 0, sizeof(double), g_ctx.stream));
-  return fail(QGB_ERR_TIMEOUT, "force kernel: a wait for the corner products of neighbouring time slices gave up; "
-                               "its results are invalid");
-}
-
 int read_results(int slot, int n, double* out)
 {
   QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.results_host + slot, g_ctx.results + slot, n * sizeof(double),
                                cudaMemcpyDeviceToHost, g_ctx.stream));
-  QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.results_host + Ctx::NSLOT, g_ctx.results + Ctx::NSLOT, sizeof(double),
-                               cudaMemcpyDeviceToHost, g_ctx.stream));
   QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
-  const int rc = check_wave_flag();
-  if (rc != QGB_OK) return rc;
   for (int i = 0; i < n; ++i) out[i] = g_ctx.results_host[slot + i];
   return QGB_OK;
 }
@@ -382,22 +365,11 @@ int prepare_corners(const Geo& g, int variant, ForceArgs& a, bool prof, int* ker
 {
   int bs, minb, split, map;
   *kernels = 0;
-  if (sizeof(R) != 4 || !qgb::force_variant_info_c(variant, &bs, &minb, &split, &map) || (map != 5 && map != 6))
-    return QGB_OK;
+  if (sizeof(R) != 4 || !qgb::force_variant_info_c(variant, &bs, &minb, &split, &map) || map != 5) return QGB_OK;
   if (g.off != 0 || qgb::padded_sites(g.V) * 144 >= 2147483647L) return QGB_OK;  // the launcher runs map 3
   void* c = nullptr;
   QGB_RC(get_scratch((size_t)qgb::padded_sites(g.V) * qgb::N_CORNER_FIELDS * 18 * sizeof(R), 40, &c));
   a.corners = c;
-  // site map 6 (the same conditions as its launcher): the corner items run
-  // inside the force launch (k_force_wave): its work ticket and per-slice
-  // counters, and the flag that a wait gave up; otherwise map 5's pass
-  if (map == 6 && g.d[3] >= 6 && ((long)g.d[0] * g.d[1] * g.d[2]) % 32 == 0) {
-    void* w = nullptr;
-    QGB_RC(get_scratch((size_t)(g.d[3] + 1) * sizeof(int), 41, &w));
-    a.wave = static_cast<int*>(w);
-    a.wave_err = g_ctx.results + Ctx::NSLOT;
-    return QGB_OK;
-  }
   if (prof) {
     Prof p("corners");
     QGB_TRY_CUDA(qgb::launch_corners<R>(g, a.U, c, g_ctx.stream));
@@ -567,7 +539,8 @@ static int flow_step(qgb_field* gf, double eps, double c1, bool rk3)
 // `every` steps, each segment recomputed forward, each step's three stages
 // recomputed with their Z fields, then pulled back stage by stage.
 template <typename R>
-static int flow_vjp_impl(const qgb_field* gf, double eps, int steps, int every, const void* lam_in, void* grad)
+static int flow_vjp_impl(const qgb_field* gf, double eps, double c1, int steps, int every, const void* lam_in,
+                         void* grad)
 {
   const Geo g = geo_of(gf);
   const size_t bytes = gf->bytes;
@@ -587,7 +560,7 @@ static int flow_vjp_impl(const qgb_field* gf, double eps, int steps, int every, 
   QGB_RC(get_scratch(bytes, 49, &mua));
   QGB_RC(get_scratch(bytes, 50, &mub));
   auto stage = [&](const void* in, void* out, double a, double b, const void* zp, void* zo) -> int {
-    ForceArgs fa = fargs(in, out, 3.0, 0.0, eps);
+    ForceArgs fa = fargs(in, out, 3.0, c1, eps);
     fa.a = a;
     fa.b = b;
     fa.zp = zp;
@@ -622,13 +595,13 @@ static int flow_vjp_impl(const qgb_field* gf, double eps, int steps, int every, 
         Prof p("flow_adjoint", 6);
         // stage 3: W3 = exp(eps Z2) W2, Z2 = 3/4 F(W2) - Z1
         QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z2, nullptr, 0.0, eps, mua, laml, g_ctx.stream));
-        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W2, mua, laml, lam, 3.0, 0.75, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W2, mua, laml, lam, 3.0, c1, 0.75, g_ctx.stream));
         // stage 2: W2 = exp(eps Z1) W1, Z1 = 8/9 F(W1) - 17/9 Z0; carry -mu2 into Z1
         QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z1, mua, -1.0, eps, mub, laml, g_ctx.stream));
-        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W1, mub, laml, lam, 3.0, 8.0 / 9.0, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W1, mub, laml, lam, 3.0, c1, 8.0 / 9.0, g_ctx.stream));
         // stage 1: W1 = exp(eps Z0) W0, Z0 = 1/4 F(W0); carry -17/9 mu1 into Z0
         QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z0, mub, -17.0 / 9.0, eps, mua, laml, g_ctx.stream));
-        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, wst[j], mua, laml, lam, 3.0, 0.25, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, wst[j], mua, laml, lam, 3.0, c1, 0.25, g_ctx.stream));
       }
     }
   }
@@ -712,10 +685,7 @@ int qgb_synchronize(void)
 {
   QGB_CTX();
   QGB_RC(qgb_field_download_join());
-  QGB_TRY_CUDA(cudaMemcpyAsync(g_ctx.results_host + Ctx::NSLOT, g_ctx.results + Ctx::NSLOT, sizeof(double),
-                               cudaMemcpyDeviceToHost, g_ctx.stream));
   QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
-  QGB_RC(check_wave_flag());
   return QGB_OK;
 }
 
@@ -1601,15 +1571,14 @@ int qgb_gf_wilson_flow_vjp(const qgb_field* gf, double epsilon, int32_t steps, d
   QGB_CTX();
   QGB_RC(check_vjp_args(gf, cotangent, "qgb_gf_wilson_flow_vjp"));
   QGB_RC(check_vjp_args(gf, grad, "qgb_gf_wilson_flow_vjp"));
-  QGB_CHECK(c1 == 0.0, QGB_ERR_INVALID_ARG, "qgb_gf_wilson_flow_vjp: only the Wilson flow (c1 = 0) has an adjoint");
   QGB_CHECK(steps >= 0 && checkpoint_every >= 1, QGB_ERR_INVALID_ARG, "qgb_gf_wilson_flow_vjp: bad steps");
   if (steps == 0) {
     QGB_TRY_CUDA(cudaMemcpyAsync(grad->d, cotangent->d, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
     return QGB_OK;
   }
   const int every = checkpoint_every < steps ? checkpoint_every : steps;
-  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, steps, every, cotangent->d, grad->d);
-  return flow_vjp_impl<float>(gf, epsilon, steps, every, cotangent->d, grad->d);
+  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, c1, steps, every, cotangent->d, grad->d);
+  return flow_vjp_impl<float>(gf, epsilon, c1, steps, every, cotangent->d, grad->d);
 }
 
 int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, double c1, int32_t checkpoint_every,
@@ -1617,7 +1586,6 @@ int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, 
 {
   QGB_CTX();
   QGB_RC(check_vjp_args(gf, grad, "qgb_gf_flow_action_grad"));
-  QGB_CHECK(c1 == 0.0, QGB_ERR_INVALID_ARG, "qgb_gf_flow_action_grad: only the Wilson flow (c1 = 0) has an adjoint");
   QGB_CHECK(steps >= 0 && checkpoint_every >= 1, QGB_ERR_INVALID_ARG, "qgb_gf_flow_action_grad: bad steps");
   const Geo g = geo_of(gf);
   void *V = nullptr, *lamN = nullptr;
@@ -1627,7 +1595,7 @@ int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, 
   QGB_TRY_CUDA(cudaMemcpyAsync(V, gf->d, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
   qgb_field_s fv = *gf;
   fv.d = V;
-  for (int i = 0; i < steps; ++i) QGB_RC(flow_step(&fv, epsilon, 0.0, true));
+  for (int i = 0; i < steps; ++i) QGB_RC(flow_step(&fv, epsilon, c1, true));
   V = fv.d;  // flow_step hands the result buffer to the handle
   // loss and its gradient at V_t: dL = -2 <F(V_t), X> in the su(3) pairing
   QGB_RC(action_slot(&fv, c1_loss != 0.0, 0));
@@ -1648,8 +1616,8 @@ int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, 
     return QGB_OK;
   }
   const int every = checkpoint_every < steps ? checkpoint_every : steps;
-  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, steps, every, lamN, grad->d);
-  return flow_vjp_impl<float>(gf, epsilon, steps, every, lamN, grad->d);
+  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, c1, steps, every, lamN, grad->d);
+  return flow_vjp_impl<float>(gf, epsilon, c1, steps, every, lamN, grad->d);
 }
 
 int qgb_set_anti_hermitian_matrix_from_basis(qgb_field* fc, const qgb_field* basis)

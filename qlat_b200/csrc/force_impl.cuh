@@ -281,8 +281,8 @@ __device__ __forceinline__ void staple_dir_fast(M3<R>& S, const LinkLd<R>& L, in
 // force: 1 instead of 2); the 16 products per site of the pass are shared by
 // the links that read them.  The paths are those of hmc.cpp:27-62, only
 // grouped differently.
-template <typename R, bool RECT, int SG, typename CL>
-__device__ __forceinline__ void staple_dir_corner(M3<R>& S, const LinkLd<R>& L, const CL& Cn, int s, int mu,
+template <typename R, bool RECT, int SG>
+__device__ __forceinline__ void staple_dir_corner(M3<R>& S, const LinkLd<R>& L, const LinkLd<R>& Cn, int s, int mu,
                                                   int nu, int dmm1, int dmp1, int dn1, int dn2, R cp, R cr)
 {
   const int pnm = corner_id(nu, mu), pmn = corner_id(mu, nu);
@@ -334,16 +334,13 @@ __device__ __forceinline__ void staple_dir_corner(M3<R>& S, const LinkLd<R>& L, 
   }
 }
 
-// The staple sum of site s (g.off == 0) from the links U and the corner field
-// (CL: the corner loader, LinkLd or, when the corners are written by the same
-// kernel, LinkLdWeak).
-template <typename R, bool RECT, typename CL = LinkLd<R>>
+// The staple sum of site s (g.off == 0) from the links U and the corner field.
+template <typename R, bool RECT>
 __device__ __forceinline__ M3<R> staple_sum_corner(const Cx<R>* U, const Cx<R>* corners, const Geo& g, int s, int mu,
                                                    R cp, R cr)
 {
   const int nblk = (int)site_blocks(g.V);
-  const LinkLd<R> L{U, nblk};
-  const CL Cn{corners, nblk};
+  const LinkLd<R> L{U, nblk}, Cn{corners, nblk};
   const Coord x = coord_of(g, s);
   const int st[4] = {1, g.d[0], g.d[0] * g.d[1], g.d[0] * g.d[1] * g.d[2]};
   const int xm = sel4(x.c, mu), Lm = sel4(g.d, mu), sm = sel4(st, mu);
@@ -362,12 +359,15 @@ __device__ __forceinline__ M3<R> staple_sum_corner(const Cx<R>* U, const Cx<R>* 
   return S;
 }
 
-// The corner products of site s along a: D_a(x) and P_ab(x) for the three
-// b != a.  Two-row products completed to SU(3), as the chains of site map 3.
+// The pass that fills the corner field: one thread per (site, a), block =
+// 4 * (site block) + a, storing D_a(x) and P_ab(x) for the three b != a.
+// Two-row products completed to SU(3), as the chains of site map 3.
 template <typename R>
-__device__ __forceinline__ void corners_of(const Geo& g, const Cx<R>* __restrict__ U, Cx<R>* __restrict__ C, int s,
-                                           int a)
+__global__ void __launch_bounds__(128) k_corners(Geo g, const Cx<R>* __restrict__ U, Cx<R>* __restrict__ C)
 {
+  const int s = (int)((blockIdx.x >> 2) * 128 + threadIdx.x);
+  if (s >= g.V) return;
+  const int a = blockIdx.x & 3;
   const int nblk = (int)site_blocks(g.V);
   const LinkLd<R> L{U, nblk};
   const Coord x = coord_of(g, s);
@@ -383,15 +383,6 @@ __device__ __forceinline__ void corners_of(const Geo& g, const Cx<R>* __restrict
   }
 }
 
-// The pass that fills the corner field: one thread per (site, a), block =
-// 4 * (site block) + a.
-template <typename R>
-__global__ void __launch_bounds__(128) k_corners(Geo g, const Cx<R>* __restrict__ U, Cx<R>* __restrict__ C)
-{
-  const int s = (int)((blockIdx.x >> 2) * 128 + threadIdx.x);
-  if (s >= g.V) return;
-  corners_of<R>(g, U, C, s, blockIdx.x & 3);
-}
 
 // s: the site's index in the field U (the lattice's sites start at g.off);
 // nblk: the field's 32-site blocks (default: those of the lattice alone).
@@ -468,107 +459,6 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
   }
 }
 
-// ------------------------------------------------------------------------
-// site map 6: the corner pass and the force as one persistent launch
-//
-// The work is cut into items of 128 sites of one time slice and one
-// direction: corner items (the corner products of corners_of) and force items
-// (the staple sum from the corners and the epilogue).  The force at time
-// slice t reads corners of slices t-2 .. t+1, so the items are handed out in
-// this order of groups (one group = all items of one slice):
-//   C(T-2) C(T-1) C(0) C(1), then for t = 0 .. T-1: [C(t+2) while t+2 <= T-3] F(t)
-// Every block takes the next item from a ticket counter; a force item first
-// waits until the four corner groups it reads are complete.  Those groups
-// come earlier in the order, so they are held by blocks that are already
-// running, and corner items never wait: every wait ends.  Each wait still
-// gives up after about a second (wave_err = 1; the host reports
-// QGB_ERR_TIMEOUT), as a guard.  The corner traffic then overlaps the force
-// arithmetic instead of running as a separate memory-bound pass.  Needs
-// T >= 6 and X Y Z a multiple of 32 (no 32-site memory block straddles two
-// slices), g.off == 0; otherwise the launcher runs site map 5.
-
-__device__ __forceinline__ int ld_acquire_gpu(const int* p)
-{
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// group G of the hand-out order -> (force?, slice)
-__device__ __forceinline__ void wave_group(int G, int T, bool& force, int& t)
-{
-  if (G < 4) {
-    force = false;
-    t = G < 2 ? T - 2 + G : G - 2;
-    return;
-  }
-  G -= 4;
-  if (G < 2 * (T - 4)) {
-    force = (G & 1) != 0;
-    t = force ? G >> 1 : (G >> 1) + 2;
-    return;
-  }
-  force = true;
-  t = T - 4 + (G - 2 * (T - 4));
-}
-
-static const long WAVE_SPIN_LIMIT = 1L << 23;  // x ~128 ns sleeps: about a second
-
-template <typename R, int MODE, bool RECT, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_force_wave(Geo g, ForceArgs a, int S, int T)
-{
-  __shared__ int s_item, s_ok;
-  const int nb = (S + 127) >> 7;
-  const int per_group = 4 * nb;
-  const int total = 2 * T * per_group;
-  int* const ticket = a.wave;
-  int* const done = a.wave + 1;
-  const R cp = R(1.0 - 8.0 * a.c1), cr = R(a.c1);
-  for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
-    __syncthreads();
-    const int item = s_item;
-    if (item >= total) return;
-    const int G = item / per_group, within = item - G * per_group;
-    bool force;
-    int t;
-    wave_group(G, T, force, t);
-    const int local = (within >> 2) * 128 + threadIdx.x, dir = within & 3;
-    const int site = t * S + local;
-    if (!force) {
-      if (local < S) corners_of<R>(g, (const Cx<R>*)a.U, (Cx<R>*)a.corners, site, dir);
-      __threadfence();  // each thread's corner stores, before the count that releases them
-      __syncthreads();
-      if (threadIdx.x == 0) atomicAdd(done + t, 1);
-    } else {
-      if (threadIdx.x == 0) {
-        int ok = 1;
-        for (int d = -2; d <= 1 && ok; ++d) {
-          const int* c = done + (t + d + T) % T;
-          long it = 0;
-          while (ld_acquire_gpu(c) < per_group) {
-            if (++it > WAVE_SPIN_LIMIT) {
-              ok = 0;
-              break;
-            }
-            __nanosleep(128);
-          }
-        }
-        if (!ok) *a.wave_err = 1.0;
-        s_ok = ok;
-      }
-      __syncthreads();
-      if (s_ok && local < S) {
-        __threadfence();
-        const M3<R> Sm = staple_sum_corner<R, RECT, LinkLdWeak<R>>((const Cx<R>*)a.U, (const Cx<R>*)a.corners, g,
-                                                                 site, dir, cp, cr);
-        force_epilogue<R, MODE>(a, CField<R>{(const Cx<R>*)a.U, g.V}, g.V, site, dir, Sm, a.beta);
-      }
-    }
-    __syncthreads();  // s_item and s_ok are rewritten by the next round
-  }
-}
-
 // Launch variants for the autotuner: threads per block, minimum resident
 // blocks per SM (caps registers), threads per link (SPLIT = 2 gives each link
 // to a lane pair, each doing 3 of the 6 signed directions, combined by a
@@ -583,10 +473,7 @@ __global__ void __launch_bounds__(128, MINB) k_force_wave(Geo g, ForceArgs a, in
 // SPLIT = 1, otherwise MAP 0); MAP 3 is MAP 2 with the two-row SU(3) chains
 // (FP32; FP64 runs MAP 2); MAP 5 is MAP 3 with the staples formed from the
 // corner field of k_corners (FP32; needs ForceArgs::corners and 144 padded
-// sites < 2^31, otherwise MAP 3; FP64 runs MAP 2); MAP 6 is MAP 5 with the
-// corner pass inside the force launch (k_force_wave; 128 threads per block;
-// also needs ForceArgs::wave, T >= 6 and X Y Z a multiple of 32, otherwise
-// MAP 5).
+// sites < 2^31, otherwise MAP 3; FP64 runs MAP 2).
 #define QGB_FORCE_VARIANTS(X) \
   X(0, 128, 1, 1, 0)          \
   X(1, 256, 1, 1, 0)          \
@@ -604,13 +491,8 @@ __global__ void __launch_bounds__(128, MINB) k_force_wave(Geo g, ForceArgs a, in
   X(13, 128, 8, 1, 3)         \
   X(14, 128, 4, 1, 5)         \
   X(15, 128, 3, 1, 5)         \
-  X(16, 256, 2, 1, 5)         \
-  X(17, 128, 5, 1, 5)         \
-  X(18, 128, 8, 1, 5)         \
-  X(19, 128, 4, 1, 6)         \
-  X(20, 128, 3, 1, 6)         \
-  X(21, 128, 5, 1, 6)
-static const int N_FORCE_VARIANTS = 22;
+  X(16, 256, 2, 1, 5)
+static const int N_FORCE_VARIANTS = 17;
 
 template <int BS>
 struct Tile {
@@ -685,45 +567,8 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
 template <typename R, int BS, int MINB, int SPLIT, int MAP>
 cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
-  if constexpr ((MAP == 3 || MAP == 5 || MAP == 6) && sizeof(R) == 8) {
+  if constexpr ((MAP == 3 || MAP == 5) && sizeof(R) == 8) {
     return launch_force_v<R, BS, MINB, SPLIT, 2>(g, mode, a, st);
-  } else if constexpr (MAP == 6) {
-    const int S = g.d[0] * g.d[1] * g.d[2], T = g.d[3];
-    if (!(a.wave && a.wave_err && a.corners && g.off == 0 && T >= 6 && S % 32 == 0 &&
-          padded_sites(g.V) * 144 < 2147483647L))
-      return launch_force_v<R, BS, MINB, SPLIT, 5>(g, mode, a, st);
-    // as many blocks as are resident at once: each takes items until none are left
-    static int per_sm[5][2] = {{0}};
-    static int sms = 0;
-    const bool rect = a.c1 != 0.0;
-    if (!sms) {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
-    cudaError_t e = cudaMemsetAsync(a.wave, 0, (size_t)(T + 1) * sizeof(int), st);
-    if (e != cudaSuccess) return e;
-#define QGB_WAVE(M)                                                                                          \
-  {                                                                                                         \
-    int& n = per_sm[M][rect ? 1 : 0];                                                                       \
-    if (!n) {                                                                                               \
-      if (rect) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_force_wave<R, M, true, MINB>, 128, 0); \
-      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_force_wave<R, M, false, MINB>, 128, 0);    \
-      if (n < 1) n = 1;                                                                                     \
-    }                                                                                                       \
-    const dim3 grid((unsigned)(n * sms));                                                                   \
-    if (rect) k_force_wave<R, M, true, MINB><<<grid, 128, 0, st>>>(g, a, S, T);                             \
-    else k_force_wave<R, M, false, MINB><<<grid, 128, 0, st>>>(g, a, S, T);                                 \
-  }
-    switch (mode) {
-      case FORCE_SET: QGB_WAVE(FORCE_SET) break;
-      case FORCE_UPDATE: QGB_WAVE(FORCE_UPDATE) break;
-      case FORCE_EVOLVE: QGB_WAVE(FORCE_EVOLVE) break;
-      case FORCE_FLOW: QGB_WAVE(FORCE_FLOW) break;
-      case FORCE_UPDATE_EVOLVE: QGB_WAVE(FORCE_UPDATE_EVOLVE) break;
-    }
-#undef QGB_WAVE
-    return cudaGetLastError();
   } else {
   // site map 5 reads the corner field that launch_corners filled from a.U
   if (MAP == 5 && !(a.corners && g.off == 0 && padded_sites(g.V) * 144 < 2147483647L))

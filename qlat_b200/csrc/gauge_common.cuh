@@ -39,19 +39,6 @@ __device__ __forceinline__ Cx<float> ldg_cx(const Cx<float>* p)
   return cx<float>(v.x, v.y);
 }
 
-// ld.global.ca: coherent loads (not the read-only path) for data written by
-// other blocks of the running kernel
-__device__ __forceinline__ Cx<double> ldca_cx(const Cx<double>* p)
-{
-  const double2 v = __ldca(reinterpret_cast<const double2*>(p));
-  return cx<double>(v.x, v.y);
-}
-__device__ __forceinline__ Cx<float> ldca_cx(const Cx<float>* p)
-{
-  const float2 v = __ldca(reinterpret_cast<const float2*>(p));
-  return cx<float>(v.x, v.y);
-}
-
 // offset (in Cx<R> for K = 9, in reals for K = 1) of entry k of component m of site s
 template <int K>
 __host__ __device__ __forceinline__ long lay_index(long V, int m, int k, long s)
@@ -180,23 +167,6 @@ struct LinkLd {
     M3<R> r;
 #pragma unroll
     for (int k = 0; k < 9; ++k) r.e[k] = ldg_cx(q + 32 * k);
-    return r;
-  }
-};
-
-// The same loads through the coherent path (ld.global, no read-only cache),
-// for data that other blocks of the running kernel write before this block
-// reads it (after an acquire of their completion count).
-template <typename R>
-struct LinkLdWeak {
-  const Cx<R>* p;
-  int nblk;
-  __device__ __forceinline__ M3<R> operator()(int link, int site) const
-  {
-    const Cx<R>* q = p + (((link * nblk + (site >> 5)) * 9) * 32 + (site & 31));
-    M3<R> r;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) r.e[k] = ldca_cx(q + 32 * k);
     return r;
   }
 };

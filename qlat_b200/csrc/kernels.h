@@ -54,9 +54,7 @@ struct ForceArgs {
   void* ev;         // UPDATE_EVOLVE: W, evolved in place (never read at other links, so W != U)
   double ev_eps;    // UPDATE_EVOLVE: exponential step of W
   int ev_unit;      // UPDATE_EVOLVE: 0 none, 1 unitarize in R, 2 unitarize with FP64 arithmetic
-  void* corners;    // site maps 5, 6: scratch for the 16 two-link products per site (corner_id), or null
-  int* wave;        // site map 6: 1 + T ints (work ticket, per-slice corner counts), zeroed by the launcher
-  double* wave_err; // site map 6: set to 1 when a wait for corner work gives up
+  void* corners;    // site map 5: scratch for the 16 two-link products per site (corner_id), or null
 };
 
 // Site map 5 of the force kernel keeps, per site, the 4 double links
@@ -125,7 +123,7 @@ cudaError_t launch_combine(double* results, int out, int a, int b, int c, cudaSt
 // Flow adjoint (adjoint.cu).
 template <typename R>
 cudaError_t launch_force_vjp(const Geo& g, const void* U, const void* Y, const void* lam_local, void* lam_out,
-                             double beta, double a, cudaStream_t st);
+                             double beta, double c1, double a, cudaStream_t st);
 template <typename R>
 cudaError_t launch_flow_adj_local(long V, const void* lam, const void* Z, const void* mu_carry, double carry, double eps,
                                   void* mu_out, void* lam_local, cudaStream_t st);

@@ -79,6 +79,54 @@ def test_flow_vjp_at_the_differentiation_workload(q):
         assert abs(fd - ip(grad, X)) < 1e-7 * abs(fd), (k, fd, ip(grad, X))
 
 
+@pytest.mark.parametrize("c1,eps", [(-0.331, 0.03), (-1.4008, 0.01)])
+def test_rectangle_flow_vjp_matches_finite_differences(q, c1, eps):
+    """Iwasaki and DBW2 flows (flow force GaugeAction(3, c1)), loss with the
+    same rectangle coefficient: the adjoint against finite differences.  The
+    DBW2 flow of this rough start is unstable at eps = 0.03 (the action grows
+    a hundredfold in 5 steps; there the order-20 exponential and the exact one
+    whose derivative the adjoint takes part at 2e-7), so it runs at 0.01."""
+    gf = setup(q)
+    steps, beta = 5, 2.0
+    loss, grad = q.gf_flow_action_grad(gf, eps, steps, beta, c1=c1, c1_loss=c1, checkpoint_every=2)
+    assert abs(loss - q.gf_flow_action(gf, eps, steps, beta, c1=c1, c1_loss=c1)) < 1e-10 * abs(loss)
+    for k in range(8):
+        X = q.GaugeMomentum(gf.geo)
+        X.set_rand(q.RngState(f"rect-direction-{k}"), 1.0)
+
+        def L(h):
+            u = gf.copy()
+            q.gf_evolve(u, X, h)
+            return q.gf_flow_action(u, eps, steps, beta, c1=c1, c1_loss=c1)
+
+        fd = fd4(L, 1e-4)
+        assert abs(fd - ip(grad, X)) < 1e-7 * abs(fd), (k, fd, ip(grad, X))
+
+
+def test_rectangle_flow_vjp_against_reference_forward(q, oracle):
+    """Finite differences of the oracle's Iwasaki flow (c1 = -0.331, the
+    reference algorithm) agree with the GPU adjoint."""
+    ts = (3, 4, 4, 5)
+    gf = setup(q, ts)
+    eps, steps, beta, c1 = 0.05, 3, 2.5, -0.331
+    _, grad = q.gf_flow_action_grad(gf, eps, steps, beta, c1=c1, checkpoint_every=2)
+    U = np.ascontiguousarray(np.asarray(gf))
+    for k in range(3):
+        X = q.GaugeMomentum(gf.geo)
+        X.set_rand(q.RngState(f"ref-rect-direction-{k}"), 1.0)
+        Xn = np.ascontiguousarray(np.asarray(X))
+
+        def L(h):
+            u = U.copy()
+            oracle.gf_evolve(u, Xn, ts, h)
+            for _ in range(steps):
+                oracle.gf_wilson_flow_step(u, ts, eps, c1)
+            return oracle.gf_hamilton_node(u, ts, beta, 0.0)
+
+        fd = fd4(L, 1e-4)
+        assert abs(fd - ip(grad, X)) < 1e-7 * abs(fd), (k, fd, ip(grad, X))
+
+
 def test_flow_vjp_against_reference_forward(q, oracle):
     """Finite differences of the oracle's flow (the reference algorithm) agree with the GPU adjoint."""
     ts = (3, 4, 4, 5)

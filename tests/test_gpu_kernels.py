@@ -195,10 +195,9 @@ def test_errors_are_reported(q):
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("ts", [(3, 4, 5, 6), (4, 4, 4, 8), (8, 4, 2, 6)])
 def test_every_force_variant(q, oracle, prec, ts):
-    """All launch shapes of the autotuner compute the same force.  3 x 4 x 5 x 6
-    has time slices of 60 sites (the corner-wave shapes fall back to a
-    separate corner pass); 4 x 4 x 4 x 8 and 8 x 4 x 2 x 6 run them as one
-    persistent launch (slices of 64 sites, 8 and 6 slices)."""
+    """All launch shapes of the autotuner compute the same force, on lattices
+    whose site count is a multiple of 32 and not (3 x 4 x 5 x 6: a partly
+    filled last block of 32 sites)."""
     gf, ref = hot_start(q, oracle, ts)
     g = gf if prec == "f64" else gf.copy(precision=q.F32)
     tol = 1e-13 if prec == "f64" else 2e-6
@@ -224,12 +223,10 @@ def test_every_force_variant(q, oracle, prec, ts):
 @pytest.mark.parametrize("c1", [-0.331, 0.0])
 def test_force_shapes_agree_in_every_mode(q, c1):
     """The FP32 force shapes used by the mixed trajectory -- two-row chains
-    (variant 10), the corner field with a separate pass (14) and the corner
-    wave in one launch (19) -- give the same mixed trajectory (force +
-    exponential, force + momentum update + link update) and the same FP32
-    flow stage, to FP32 rounding; the wave's waits never give up (no
-    QGB_ERR_TIMEOUT from the read-backs)."""
-    ts = (4, 4, 4, 8)
+    (variant 10) and the corner field with its separate pass (14) -- give the
+    same mixed trajectory (force + exponential, force + momentum update + link
+    update) and the same FP32 flow stage, to FP32 rounding."""
+    ts = (8, 4, 4, 8)
     ga = q.GaugeAction(2.13, c1)
     gf = q.GaugeField(q.Geometry(ts))
     gf.set_rand(q.RngState("shapes").split("gf-init"), 0.3, 1)
@@ -238,7 +235,7 @@ def test_force_shapes_agree_in_every_mode(q, c1):
     saved = q.force_get_variant(q.F32, c1 != 0.0)
     res = {}
     try:
-        for v in (10, 14, 19):
+        for v in (10, 14):
             q.force_set_variant(q.F32, c1 != 0.0, v)
             g, m = gf.copy(), gm.copy()
             dh = q.run_hmc_evolve_pure_gauge(m, g, ga, None, 4, 1.0, precision="mixed", reunit_interval=4)
@@ -247,7 +244,7 @@ def test_force_shapes_agree_in_every_mode(q, c1):
             res[v] = (dh, np.asarray(g), np.asarray(w))
     finally:
         q.force_set_variant(q.F32, c1 != 0.0, saved)
-    for v in (14, 19):
+    for v in (14,):
         assert abs(res[v][0] - res[10][0]) < 1e-4 * max(1.0, abs(res[10][0])), (v, res[v][0], res[10][0])
         assert nrel(res[v][1], res[10][1]) < 1e-6, v
         assert nrel(res[v][2], res[10][2]) < 1e-6, v
