@@ -509,8 +509,9 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
   // that sweeps the lattice once per direction reads the link field from DRAM
   // four times when it exceeds L2)
   if constexpr (MAP >= 2) {
-    const long t = (long)(blockIdx.x >> 2) * BS + threadIdx.x;
-    if (t >= g.V) return;
+    const long w = (long)(blockIdx.x >> 2) * BS + threadIdx.x;
+    if (w >= g.V) return;
+    const long t = site_of_work(g, w, BS);
     const int mu = blockIdx.x & 3;
     M3<R> S;
     if constexpr (MAP == 5)
@@ -580,10 +581,12 @@ cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cud
   const bool fast = MAP >= 2 && SPLIT == 1 && g.off == 0 && padded_sites(g.V) * 36 < 2147483647L;
   if (MAP >= 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
   dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)(4 * ((g.V * SPLIT + BS - 1) / BS)), 1);
+  Geo gk = g;  // the linear maps traverse large lattices in z slabs
+  if (MAP >= 2) set_slab_order(gk, BS, (int)(18 * sizeof(R)));
   const bool rect = a.c1 != 0.0;
 #define QGB_LAUNCH(M)                                                                                  \
-  if (rect) k_force<R, M, true, BS, MINB, SPLIT, MAP><<<grid, BS, 0, st>>>(g, a); \
-  else k_force<R, M, false, BS, MINB, SPLIT, MAP><<<grid, BS, 0, st>>>(g, a);
+  if (rect) k_force<R, M, true, BS, MINB, SPLIT, MAP><<<grid, BS, 0, st>>>(gk, a); \
+  else k_force<R, M, false, BS, MINB, SPLIT, MAP><<<grid, BS, 0, st>>>(gk, a);
   switch (mode) {
     case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
     case FORCE_UPDATE: QGB_LAUNCH(FORCE_UPDATE) break;

@@ -171,6 +171,39 @@ struct LinkLd {
   }
 };
 
+// Site of linear work index w (chunks of bs consecutive sites) in the
+// traversal order of g.zs: linear when g.zs == 0; otherwise chunk c = w / bs
+// is (xy chunk, z in slab, t, slab) from fastest to slowest, which needs
+// X Y % bs == 0 and Z % g.zs == 0 (set_slab_order).
+__host__ __device__ __forceinline__ long site_of_work(const Geo& g, long w, int bs)
+{
+  if (g.zs == 0) return w;
+  const long xy = (long)g.d[0] * g.d[1];
+  const long per_plane = xy / bs;
+  long c = w / bs;
+  const long lane = w - c * bs;
+  const long cxy = c % per_plane;
+  c /= per_plane;
+  const long zz = c % g.zs;
+  c /= g.zs;
+  const long t = c % g.d[3];
+  const long zb = c / g.d[3];
+  return cxy * bs + lane + xy * ((zb * g.zs + zz) + (long)g.d[2] * t);
+}
+
+// z-slab order for site kernels with blocks of bs sites and links of
+// link_bytes (144 FP64, 72 FP32): slabs of 16 z-planes when a time slice of
+// the links exceeds 12 MB (then the +-2 slices a force reads no longer stay
+// in L2 under a linear sweep) and the lattice allows it; linear otherwise.
+__host__ __device__ __forceinline__ void set_slab_order(Geo& g, int bs, int link_bytes)
+{
+  const long xy = (long)g.d[0] * g.d[1];
+  const long slice_bytes = xy * g.d[2] * 4 * link_bytes;
+  g.zs = (g.off == 0 && g.r1 < 0 && xy % bs == 0 && g.d[2] % 16 == 0 && g.d[2] > 16 && slice_bytes > (12L << 20))
+             ? 16
+             : 0;
+}
+
 __device__ __forceinline__ int sel4(const int (&v)[4], int k)
 {
   return k == 0 ? v[0] : k == 1 ? v[1] : k == 2 ? v[2] : v[3];

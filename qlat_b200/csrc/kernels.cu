@@ -498,7 +498,7 @@ __device__ __forceinline__ double energy_of(const M3<R>& Fa)
 template <typename R>
 __global__ void __launch_bounds__(RED_BS) k_clover(Geo g, const Cx<R>* Up, R* ef, R* qf, double* partials)
 {
-  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long s = site_of_work(g, (long)blockIdx.x * blockDim.x + threadIdx.x, RED_BS);
   double v[2] = {0.0, 0.0};
   if (s < g.V && in_reduce(g, s)) {
     const CField<R> U{Up, g.V};
@@ -528,7 +528,9 @@ template <typename R>
 cudaError_t launch_clover(const Geo& g, const void* U, void* e_field, void* q_field, double* partials,
                           cudaStream_t st)
 {
-  k_clover<R><<<reduce_blocks(g), RED_BS, 0, st>>>(g, (const Cx<R>*)U, (R*)e_field, (R*)q_field, partials);
+  Geo gk = g;  // z slabs on large lattices (the leaves reach one slice either way)
+  set_slab_order(gk, RED_BS, (int)(18 * sizeof(R)));
+  k_clover<R><<<reduce_blocks(g), RED_BS, 0, st>>>(gk, (const Cx<R>*)U, (R*)e_field, (R*)q_field, partials);
   return cudaGetLastError();
 }
 

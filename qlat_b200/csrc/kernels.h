@@ -21,6 +21,11 @@ struct Geo {
   // per-site random streams of site s are those of global site s + rng_off
   long r0 = 0, r1 = -1;
   long rng_off = 0;
+  // z-slab traversal (slab_order): when zs > 0, the linear work index of a
+  // site kernel runs over the x-y planes of zs consecutive z in each time
+  // slice before the next slice, slab by slab in z, so that the time slices
+  // a running grid reads stay in L2 on large lattices
+  int zs = 0;
 };
 
 __host__ __device__ inline bool in_reduce(const Geo& g, long s) { return s >= g.r0 && (g.r1 < 0 || s < g.r1); }
