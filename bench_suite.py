@@ -244,6 +244,7 @@ def leg_c5(q, per_size=64, n_step=10, n_traj=10, warmup=5):
     for prec in ("mixed", "fp64"):
         b = q.ChainBatch(sizes, betas)
         b.set_rand([r.split("gf-init") for r in rs], 1.0, 1)
+        tuned = b.autotune(prec)  # the batched force's launch shape (untimed)
         for t in range(1, warmup + 1):
             b.run_hmc(t, rs, n_step, precision=prec, is_always_accept=True)
         acc = 0
@@ -253,7 +254,7 @@ def leg_c5(q, per_size=64, n_step=10, n_traj=10, warmup=5):
                 acc += sum(flags)
         link_updates = 4 * sites * n_step * n_traj
         out[prec] = {"ms_per_traj": tm.ms / n_traj, "link_updates_per_s": link_updates / (tm.ms / 1e3),
-                     "accept_rate": acc / (n * n_traj)}
+                     "accept_rate": acc / (n * n_traj), "force_variant": tuned[0], "force_ms": tuned[1]}
         plaqs[prec] = b.plaq()
         del b
     d = np.abs(plaqs["mixed"] - plaqs["fp64"])

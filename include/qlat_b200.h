@@ -315,6 +315,14 @@ int qgb_batch_run_hmc(qgb_batch* b, const uint32_t* rs, int32_t traj, int32_t n_
 int qgb_batch_accept(qgb_batch* b, const int32_t* flags);
 /* gf_avg_plaq of every chain. */
 int qgb_batch_plaq(qgb_batch* b, double* plaq);
+/* The batch's own force-kernel autotuner (no counterpart in the reference):
+ * times the launch shapes of the batched force (block size and register
+ * budget; 4 shapes) on the batch's current links in `precision` (QGB_F64 for
+ * the FP64 form, QGB_F32 for the mixed form's molecular dynamics), `reps`
+ * launches each, and keeps the fastest for that precision; returns it and
+ * its time per launch.  qgb_batch_set_force_variant picks one by hand. */
+int qgb_batch_autotune(qgb_batch* b, int32_t precision, int32_t reps, int32_t* best, double* best_ms);
+int qgb_batch_set_force_variant(qgb_batch* b, int32_t precision, int32_t variant);
 /* One chain's links in the reference memory image. */
 int qgb_batch_download_chain(qgb_batch* b, int32_t chain, double* host);
 int qgb_batch_upload_chain(qgb_batch* b, int32_t chain, const double* host);

@@ -157,6 +157,8 @@ SIGNATURES = {
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_dbl_p, c_i32_p],
     "qgb_batch_accept": [c_field, c_i32_p],
     "qgb_batch_plaq": [c_field, c_dbl_p],
+    "qgb_batch_autotune": [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, c_i32_p, c_dbl_p],
+    "qgb_batch_set_force_variant": [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32],
     "qgb_batch_download_chain": [c_field, ctypes.c_int32, c_dbl_p],
     "qgb_batch_upload_chain": [c_field, ctypes.c_int32, c_dbl_p],
     "qgb_launch_count": [c_i64_p],

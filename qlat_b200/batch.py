@@ -84,6 +84,21 @@ class ChainBatch:
              flags.ctypes.data_as(_lib.c_i32_p))
         return [bool(f) for f in flags], dh
 
+    def autotune(self, precision="mixed", reps=3):
+        """Time the batched force's launch shapes on the current links in the
+        precision of `precision`'s molecular dynamics and keep the fastest
+        (qgb_batch_autotune); returns (variant, ms per launch)."""
+        from .field import F32, F64
+        best = ctypes.c_int32()
+        ms = ctypes.c_double()
+        call("qgb_batch_autotune", self._h, F32 if precision == "mixed" else F64, int(reps), ctypes.byref(best),
+             ctypes.byref(ms))
+        return best.value, ms.value
+
+    def set_force_variant(self, precision, variant):
+        from .field import F32, F64
+        call("qgb_batch_set_force_variant", self._h, F32 if precision == "mixed" else F64, int(variant))
+
     def plaq(self) -> np.ndarray:
         out = np.zeros(self.n, dtype=np.float64)
         call("qgb_batch_plaq", self._h, out.ctypes.data_as(_lib.c_dbl_p))

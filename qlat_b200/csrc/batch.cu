@@ -26,6 +26,7 @@
 namespace qgb
 {
 void set_last_error(const std::string& msg);
+void add_launches(int64_t n);
 }
 
 struct qgb_batch_s {
@@ -54,6 +55,7 @@ struct qgb_batch_s {
   long max_chain_reals = 0;
   cudaStream_t stream = nullptr;
   std::map<std::tuple<int, double, int, int, int>, cudaGraphExec_t> graphs;
+  int force_variant[2] = {0, 0};  // batched-force launch shape per precision [FP64, FP32] (qgb_batch_autotune)
 };
 
 namespace
@@ -90,7 +92,8 @@ qgb::ForceArgs bargs(const void* U, void* out, double dt, int unit)
 template <typename R>
 int batch_force(qgb_batch_s* b, qgb::ForceMode mode, const qgb::ForceArgs& a)
 {
-  QB_CUDA(qgb::launch_force_batch<R>(b->Vtot, b->n, b->d_offs, b->d_chains, b->rect, mode, a, b->stream));
+  QB_CUDA(qgb::launch_force_batch<R>(b->Vtot, b->n, b->d_offs, b->d_chains, b->rect, mode, a, b->stream,
+                                     b->force_variant[sizeof(R) == 4 ? 1 : 0]));
   return QGB_OK;
 }
 
@@ -132,6 +135,29 @@ int batch_md(qgb_batch_s* b, void* gf, void* gm, void* tmp, int n_step, double m
         QB_RC(batch_force<R>(b, qgb::FORCE_UPDATE_EVOLVE, u));
       }
     }
+  } else if (integrator == QGB_INTEGRATOR_LEAPFROG && sizeof(R) == 4) {
+    // FP32: each step one launch, the two half steps of the link update that
+    // meet between force evaluations as one step of dt (the same P), written
+    // into the other of two link buffers (gf, tmp) -- as the single-lattice
+    // FP32 leapfrog
+    QB_RC(batch_evolve<R>(b, gf, gm, 0.5 * dt, unit_each));
+    void* cur = gf;
+    void* nxt = tmp;
+    for (int i = 0; i < n_step; ++i) {
+      const bool reunit = reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step;
+      qgb::ForceArgs u = bargs(cur, gm, dt, 1);
+      u.ev = nxt;
+      u.ev_from_u = 1;
+      u.ev_eps = i + 1 < n_step ? dt : 0.5 * dt;
+      u.ev_unit = reunit ? 2 : unit_each;
+      QB_RC(batch_force<R>(b, qgb::FORCE_UPDATE_EVOLVE, u));
+      void* t = cur;
+      cur = nxt;
+      nxt = t;
+    }
+    if (cur != gf)
+      QB_CUDA(cudaMemcpyAsync(gf, cur, (size_t)qgb::padded_sites(b->Vtot) * 72 * sizeof(R), cudaMemcpyDeviceToDevice,
+                              b->stream));
   } else if (integrator == QGB_INTEGRATOR_LEAPFROG) {
     for (int i = 0; i < n_step; ++i) {
       QB_RC(batch_evolve<R>(b, gf, gm, 0.5 * dt, unit_each));
@@ -436,6 +462,67 @@ int qgb_batch_upload_chain(qgb_batch* b, int32_t chain, const double* host)
   QB_CUDA(cudaMemcpyAsync(aos, host, ci.V * 72 * sizeof(double), cudaMemcpyHostToDevice, b->stream));
   QB_CUDA(qgb::launch_aos_to_store<double>(b->Vtot, ci.off, ci.V, 4, 18, aos, b->gf, b->stream));
   QB_CUDA(cudaStreamSynchronize(b->stream));
+  return QGB_OK;
+}
+
+
+int qgb_batch_autotune(qgb_batch* b, int32_t precision, int32_t reps, int32_t* best, double* best_ms)
+{
+  if (!b || (precision != QGB_F64 && precision != QGB_F32) || reps < 1)
+    return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_autotune: bad argument");
+  const bool f32 = precision == QGB_F32;
+  const long n = qgb::padded_sites(b->Vtot) * 72;
+  // the chains' links in the precision of the force; momenta updated into the scratch buffer
+  void* U = f32 ? (void*)b->gf32 : (void*)b->gf;
+  void* P = f32 ? (void*)b->tmp32 : (void*)b->tmp;
+  if (f32) QB_CUDA((qgb::launch_convert<double, float>(n, b->gf, b->gf32, b->stream)));
+  QB_CUDA(cudaMemsetAsync(P, 0, (size_t)n * (f32 ? sizeof(float) : sizeof(double)), b->stream));
+  cudaEvent_t e0, e1;
+  QB_CUDA(cudaEventCreate(&e0));
+  QB_CUDA(cudaEventCreate(&e1));
+  int best_v = 0;
+  float best_t = 1e30f;
+  for (int v = 0; v < qgb::batch_force_variant_count(); ++v) {
+    const qgb::ForceArgs a = bargs(U, P, 1e-3, 1);
+    auto launch = [&]() {
+      return f32 ? qgb::launch_force_batch<float>(b->Vtot, b->n, b->d_offs, b->d_chains, b->rect, qgb::FORCE_UPDATE,
+                                                  a, b->stream, v)
+                 : qgb::launch_force_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, b->rect,
+                                                   qgb::FORCE_UPDATE, a, b->stream, v);
+    };
+    QB_CUDA(launch());
+    QB_CUDA(cudaEventRecord(e0, b->stream));
+    for (int r = 0; r < reps; ++r) QB_CUDA(launch());
+    QB_CUDA(cudaEventRecord(e1, b->stream));
+    QB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    QB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    ms /= reps;
+    qgb::add_launches(reps + 1);
+    if (ms < best_t) {
+      best_t = ms;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->force_variant[f32 ? 1 : 0] = best_v;
+  // recorded trajectories hold the old launch shape: record them again
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  if (best) *best = best_v;
+  if (best_ms) *best_ms = best_t;
+  return QGB_OK;
+}
+
+int qgb_batch_set_force_variant(qgb_batch* b, int32_t precision, int32_t variant)
+{
+  if (!b || (precision != QGB_F64 && precision != QGB_F32) || variant < 0 ||
+      variant >= qgb::batch_force_variant_count())
+    return bfail(QGB_ERR_INVALID_ARG, "qgb_batch_set_force_variant: bad argument");
+  b->force_variant[precision == QGB_F32 ? 1 : 0] = variant;
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
   return QGB_OK;
 }
 

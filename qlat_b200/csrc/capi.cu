@@ -473,6 +473,32 @@ int md_trajectory(const Geo& g, void* gf, void* gm, void* tmp, double beta, doub
         QGB_RC(update_evolve(tmp, 0.5 * dt, eps, half == 1 && reunit));
       }
     }
+  } else if (integrator == QGB_INTEGRATOR_LEAPFROG && sizeof(R) == 4 && !hook) {
+    // FP32 leapfrog with each step in one launch: the half steps of the link
+    // update that meet between two force evaluations are one step of dt
+    // (exp(dt/2 P) exp(dt/2 P) = exp(dt P), the same P), fused into the force
+    // kernel, which writes the updated links into the other of two buffers
+    // (gf, tmp) while its neighbours still read the current ones.
+    QGB_RC(evolve<R>(g, gf, gm, 0.5 * dt, unit_each));
+    void* cur = gf;
+    void* nxt = tmp;
+    for (int i = 0; i < n_step; ++i) {
+      const bool reunit = reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step;
+      ForceArgs b = fargs(cur, gm, beta, c1, dt);
+      b.ev = nxt;
+      b.ev_from_u = 1;
+      b.ev_eps = i + 1 < n_step ? dt : 0.5 * dt;
+      b.ev_unit = reunit ? 2 : unit_each;
+      QGB_RC(force<R>(g, qgb::FORCE_UPDATE_EVOLVE, b));
+      void* t = cur;
+      cur = nxt;
+      nxt = t;
+    }
+    if (cur != gf) {
+      Prof p("copy", 0);
+      QGB_TRY_CUDA(cudaMemcpyAsync(gf, cur, (size_t)qgb::padded_sites(g.V) * 72 * sizeof(R), cudaMemcpyDeviceToDevice,
+                                   g_ctx.stream));
+    }
   } else if (integrator == QGB_INTEGRATOR_LEAPFROG) {
     for (int i = 0; i < n_step; ++i) {
       QGB_RC(evolve<R>(g, gf, gm, 0.5 * dt, unit_each));

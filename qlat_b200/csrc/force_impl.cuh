@@ -439,9 +439,10 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
     if (MODE == FORCE_UPDATE_EVOLVE) {
       // the link update that follows the momentum update in the integrators
       // (k_evolve, then k_unitarize<R, double> when ev_unit == 2), on this
-      // thread's own link of W
+      // thread's own link of W (or of U, written to W: the fused leapfrog
+      // step, whose next force reads W)
       const WField<R> W{(Cx<R>*)a.ev, stride};
-      M3<R> wn = mul(exp_ch(scale(R(a.ev_eps), p)), W.ld(s, mu));
+      M3<R> wn = mul(exp_ch(scale(R(a.ev_eps), p)), a.ev_from_u ? U.ld(s, mu) : W.ld(s, mu));
       if (a.ev_unit == 1) unitarize(wn);
       else if (a.ev_unit == 2) unitarize_as<double, R>(wn);
       W.st(s, mu, wn);
@@ -645,12 +646,35 @@ constexpr int batch_min_blocks()
   return sizeof(R) == 4 ? (RECT ? 4 : 8) : (RECT ? 1 : 3);
 }
 
-template <typename R, int MODE, bool RECT, bool FAST>
-__global__ void __launch_bounds__(128, FAST ? batch_min_blocks<R, RECT>() : 1)
+// Launch shapes of the batched force for the batch autotuner
+// (qgb_batch_autotune): block size and minimum resident blocks per SM
+// relative to the single-lattice register budget D = batch_min_blocks:
+//   0: 128 threads, D     1: 256 threads, max(1, D / 2)
+//   2: 128 threads, D + 1 (fewer registers, more warps)
+//   3: 64 threads, 2 D    (smaller blocks, finer tail)
+static const int N_BATCH_FORCE_VARIANTS = 4;
+
+template <typename R, bool RECT, int VAR>
+constexpr int batch_bs()
+{
+  return VAR == 1 ? 256 : (VAR == 3 ? 64 : 128);
+}
+
+template <typename R, bool RECT, int VAR>
+constexpr int batch_minb()
+{
+  return VAR == 0 ? batch_min_blocks<R, RECT>()
+                  : VAR == 1 ? (batch_min_blocks<R, RECT>() / 2 > 0 ? batch_min_blocks<R, RECT>() / 2 : 1)
+                             : VAR == 2 ? batch_min_blocks<R, RECT>() + 1 : 2 * batch_min_blocks<R, RECT>();
+}
+
+template <typename R, int MODE, bool RECT, bool FAST, int VAR>
+__global__ void __launch_bounds__(batch_bs<R, RECT, VAR>(), FAST ? batch_minb<R, RECT, VAR>() : 1)
     k_force_batch(long Vtot, int nchain, const long* __restrict__ offs, const ChainInfo* __restrict__ chains,
                   ForceArgs a)
 {
-  const long sg = (long)(blockIdx.x >> 2) * 128 + threadIdx.x;  // block = 4 * (site block) + mu
+  constexpr int BS = batch_bs<R, RECT, VAR>();
+  const long sg = (long)(blockIdx.x >> 2) * BS + threadIdx.x;  // block = 4 * (site block) + mu
   if (sg >= Vtot) return;
   const int c = chain_of(offs, nchain, sg);
   const ChainInfo ci = chains[c];
@@ -668,19 +692,21 @@ __global__ void __launch_bounds__(128, FAST ? batch_min_blocks<R, RECT>() : 1)
   force_epilogue<R, MODE>(a, U, Vtot, sg, mu, S, ci.beta);
 }
 
-template <typename R>
-cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
-                               ForceMode mode, const ForceArgs& a, cudaStream_t st)
+template <typename R, int VAR>
+cudaError_t launch_force_batch_v(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
+                                 ForceMode mode, const ForceArgs& a, cudaStream_t st)
 {
-  dim3 grid((unsigned)(4 * ((Vtot + 127) / 128)), 1);
   const bool fast = padded_sites(Vtot) * 36 < 2147483647L;
-#define QGB_LAUNCH(M)                                                                                  \
-  if (fast) {                                                                                          \
-    if (rect) k_force_batch<R, M, true, true><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);   \
-    else k_force_batch<R, M, false, true><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);       \
-  } else {                                                                                             \
-    if (rect) k_force_batch<R, M, true, false><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);  \
-    else k_force_batch<R, M, false, false><<<grid, 128, 0, st>>>(Vtot, nchain, offs, chains, a);      \
+  if (!fast && VAR != 0) return launch_force_batch_v<R, 0>(Vtot, nchain, offs, chains, rect, mode, a, st);
+  constexpr int BT = batch_bs<R, true, VAR>(), BF = batch_bs<R, false, VAR>();
+  const dim3 gt((unsigned)(4 * ((Vtot + BT - 1) / BT))), gf((unsigned)(4 * ((Vtot + BF - 1) / BF)));
+#define QGB_LAUNCH(M)                                                                                         \
+  if (fast) {                                                                                                 \
+    if (rect) k_force_batch<R, M, true, true, VAR><<<gt, BT, 0, st>>>(Vtot, nchain, offs, chains, a);         \
+    else k_force_batch<R, M, false, true, VAR><<<gf, BF, 0, st>>>(Vtot, nchain, offs, chains, a);             \
+  } else {                                                                                                    \
+    if (rect) k_force_batch<R, M, true, false, 0><<<gt, BT, 0, st>>>(Vtot, nchain, offs, chains, a);          \
+    else k_force_batch<R, M, false, false, 0><<<gf, BF, 0, st>>>(Vtot, nchain, offs, chains, a);              \
   }
   switch (mode) {
     case FORCE_SET: QGB_LAUNCH(FORCE_SET) break;
@@ -691,6 +717,19 @@ cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const Ch
   }
 #undef QGB_LAUNCH
   return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
+                               ForceMode mode, const ForceArgs& a, cudaStream_t st, int variant)
+{
+  switch (variant) {
+    case 0: return launch_force_batch_v<R, 0>(Vtot, nchain, offs, chains, rect, mode, a, st);
+    case 1: return launch_force_batch_v<R, 1>(Vtot, nchain, offs, chains, rect, mode, a, st);
+    case 2: return launch_force_batch_v<R, 2>(Vtot, nchain, offs, chains, rect, mode, a, st);
+    case 3: return launch_force_batch_v<R, 3>(Vtot, nchain, offs, chains, rect, mode, a, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace qgb

@@ -4,6 +4,7 @@
 namespace qgb
 {
 int force_variant_count() { return N_FORCE_VARIANTS; }
+int batch_force_variant_count() { return N_BATCH_FORCE_VARIANTS; }
 int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* map)
 {
   return force_variant_info(variant, bs, minb, split, map);

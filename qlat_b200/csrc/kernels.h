@@ -59,6 +59,8 @@ struct ForceArgs {
   void* ev;         // UPDATE_EVOLVE: W, evolved in place (never read at other links, so W != U)
   double ev_eps;    // UPDATE_EVOLVE: exponential step of W
   int ev_unit;      // UPDATE_EVOLVE: 0 none, 1 unitarize in R, 2 unitarize with FP64 arithmetic
+  int ev_from_u;    // UPDATE_EVOLVE: W = exp(ev_eps P) U at the thread's own link (W a second buffer)
+                    // instead of evolving W in place
   void* corners;    // site map 5: scratch for the 16 two-link products per site (corner_id), or null
 };
 
@@ -80,7 +82,8 @@ cudaError_t launch_corners(const Geo& g, const void* U, void* C, cudaStream_t st
 // All chains of a batch in one launch (offs: nchain + 1 ascending offsets on the device).
 template <typename R>
 cudaError_t launch_force_batch(long Vtot, int nchain, const long* offs, const ChainInfo* chains, bool rect,
-                               ForceMode mode, const ForceArgs& a, cudaStream_t st);
+                               ForceMode mode, const ForceArgs& a, cudaStream_t st, int variant = 0);
+int batch_force_variant_count();
 int force_variant_info_c(int variant, int* bs, int* minb, int* split, int* map);
 
 // U = exp(eps P) U (optionally unitarized; exp by Cayley-Hamilton series or the

@@ -75,3 +75,28 @@ def test_mixed_batch_close_to_fp64(q):
     d64 = b64.trajectory(m, 10, integrator="leapfrog")
     d32 = b32.trajectory(m, 10, integrator="leapfrog", precision="mixed")
     assert np.all(np.abs(d32 - d64) < 5e-3 * np.maximum(1.0, np.abs(d64)))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_force_shapes_agree(q, precision):
+    """Every launch shape of the batched force (qgb_batch_autotune's table)
+    gives the same trajectory; the autotuner keeps one of them.  The mixed
+    form's leapfrog runs each step as one launch (odd and even step counts:
+    the links end in either buffer)."""
+    res = {}
+    for v in range(4):
+        for n_step in (5, 6):
+            b, rs = make(q)
+            b.set_force_variant(precision, v)
+            m = [r.split("1").split("set_rand_gauge_momentum") for r in rs]
+            dh = b.trajectory(m, n_step, integrator="leapfrog", precision=precision)
+            b.accept([True] * len(SITES))
+            res[(v, n_step)] = (dh, b.plaq())
+    tol = 0.0 if precision == "fp64" else 1e-6
+    for (v, n_step), (dh, plaq) in res.items():
+        d0, p0 = res[(0, n_step)]
+        assert np.all(np.abs(dh - d0) <= tol * np.maximum(1.0, np.abs(d0))), (v, n_step)
+        assert np.all(np.abs(plaq - p0) <= tol), (v, n_step)
+    b, _ = make(q)
+    best, ms = b.autotune(precision, reps=2)
+    assert 0 <= best < 4 and ms > 0

@@ -197,3 +197,24 @@ def test_mixed_trajectory_equals_its_steps(q, ts):
     assert dh == h1 - h0
     assert np.array_equal(np.asarray(g1), np.asarray(g2))
     assert np.array_equal(np.asarray(m1), np.asarray(m2))
+
+
+@pytest.mark.parametrize("n_step", [5, 6])
+def test_mixed_leapfrog_close_to_fp64(q, n_step):
+    """The mixed form's leapfrog, each step one launch that writes the next
+    links into the other of two buffers (odd and even step counts end in
+    either), against the FP64 leapfrog of the reference's composition."""
+    ts = (6, 6, 6, 12)
+    ga = q.GaugeAction(5.5, 0.0)
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(q.RngState("mixed-lf").split("gf-init"), 0.3, 1)
+    gm = q.GaugeMomentum(gf.geo)
+    gm.set_rand(q.RngState("mixed-lf").split("mom"), 1.0)
+    g64, m64 = gf.copy(), gm.copy()
+    dh64 = q.run_hmc_evolve_pure_gauge(m64, g64, ga, None, n_step, 1.0, integrator="leapfrog", precision="fp64")
+    for reunit in (4, 0):
+        g32, m32 = gf.copy(), gm.copy()
+        dh32 = q.run_hmc_evolve_pure_gauge(m32, g32, ga, None, n_step, 1.0, integrator="leapfrog",
+                                           precision="mixed", reunit_interval=reunit)
+        assert abs(dh32 - dh64) < 2e-3 * max(1.0, abs(dh64)) + 5e-4, (reunit, dh32, dh64)
+        assert abs(q.gf_avg_plaq(g32) - q.gf_avg_plaq(g64)) < 1e-6
