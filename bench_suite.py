@@ -28,7 +28,7 @@ of one kernel family, for ncu -k captures):
     python bench_suite.py c1|c3|c4|c5
     python bench_suite.py profile-force [--lattice 24,24,24,48] [--variants 10,14] [--c1 -0.331]
     python bench_suite.py profile-flow [--lattice 32,32,32,32] [--steps 4]
-    python bench_suite.py profile-hmc [--lattice 24,24,24,48] [--trajs 1]
+    python bench_suite.py profile-hmc [--lattice 24,24,24,48] [--trajs 1] [--fp32-variant V]
 """
 
 from __future__ import annotations
@@ -255,6 +255,19 @@ def leg_c5(q, per_size=64, n_step=10, n_traj=10, warmup=5):
         link_updates = 4 * sites * n_step * n_traj
         out[prec] = {"ms_per_traj": tm.ms / n_traj, "link_updates_per_s": link_updates / (tm.ms / 1e3),
                      "accept_rate": acc / (n * n_traj), "force_variant": tuned[0], "force_ms": tuned[1]}
+        # the same proposals as one CUDA-graph replay and as direct launches: what a
+        # single persistent launch could at most save is the difference
+        direct = {}
+        for use_graph in (True, False):
+            m = [r.split("graph-check").split("set_rand_gauge_momentum") for r in rs]
+            b.trajectory(m, n_step, precision=prec, use_graph=use_graph)
+            l0 = q.launch_count()
+            with DeviceTimer(q) as tm:
+                for _ in range(n_traj):
+                    b.trajectory(m, n_step, precision=prec, use_graph=use_graph)
+            direct["graph" if use_graph else "direct"] = {"ms_per_proposal": tm.ms / n_traj,
+                                                          "kernels_per_proposal": (q.launch_count() - l0) / n_traj}
+        out[prec]["proposal_graph_vs_direct"] = direct
         plaqs[prec] = b.plaq()
         del b
     d = np.abs(plaqs["mixed"] - plaqs["fp64"])
@@ -353,7 +366,9 @@ def profile_hmc(args):
     rs = q.RngState("b200-c2-24x64-iwasaki")
     gf = q.GaugeField(q.Geometry(ts))
     gf.set_rand(rs.split("gf-init"), 0.3, 1)
-    out = {"lattice": list(ts)}
+    if args.fp32_variant >= 0:
+        q.force_set_variant(q.F32, True, args.fp32_variant)
+    out = {"lattice": list(ts), "fp32_variant": q.force_get_variant(q.F32, True)}
     for prec in ("mixed", "fp64"):
         dh = [q.run_hmc_pure_gauge(gf, ga, t, rs, n_step=8, precision=prec, reunit_interval=4)[1]
               for t in range(1, args.trajs + 1)]
@@ -377,6 +392,7 @@ def main():
     c = sub.add_parser("profile-hmc")
     c.add_argument("--lattice", default="24,24,24,48")
     c.add_argument("--trajs", type=int, default=1)
+    c.add_argument("--fp32-variant", type=int, default=-1, help="FP32 Iwasaki force variant (default: library's)")
     args = ap.parse_args()
     import torch
     torch.cuda.set_device(0)

@@ -56,6 +56,8 @@ struct qgb_batch_s {
   cudaStream_t stream = nullptr;
   std::map<std::tuple<int, double, int, int, int>, cudaGraphExec_t> graphs;
   int force_variant[2] = {0, 0};  // batched-force launch shape per precision [FP64, FP32] (qgb_batch_autotune)
+  int kernels = 0;                 // kernels enqueued by the last enqueue_trajectory
+  std::map<std::tuple<int, double, int, int, int>, int> graph_kernels;
 };
 
 namespace
@@ -71,6 +73,12 @@ int bfail(int code, const std::string& m)
   do {                                                                                              \
     cudaError_t e_ = (expr);                                                                        \
     if (e_ != cudaSuccess) return bfail(QGB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+// a kernel launch of a trajectory: counted (qgb_launch_count)
+#define QB_KERNEL(b, expr) \
+  do {                     \
+    ++(b)->kernels;        \
+    QB_CUDA(expr);         \
   } while (0)
 #define QB_RC(expr)              \
   do {                           \
@@ -92,7 +100,7 @@ qgb::ForceArgs bargs(const void* U, void* out, double dt, int unit)
 template <typename R>
 int batch_force(qgb_batch_s* b, qgb::ForceMode mode, const qgb::ForceArgs& a)
 {
-  QB_CUDA(qgb::launch_force_batch<R>(b->Vtot, b->n, b->d_offs, b->d_chains, b->rect, mode, a, b->stream,
+  QB_KERNEL(b, qgb::launch_force_batch<R>(b->Vtot, b->n, b->d_offs, b->d_chains, b->rect, mode, a, b->stream,
                                      b->force_variant[sizeof(R) == 4 ? 1 : 0]));
   return QGB_OK;
 }
@@ -103,7 +111,7 @@ int batch_evolve(qgb_batch_s* b, void* U, const void* P, double eps, int unit)
   qgb::Geo g;
   g.d[0] = g.d[1] = g.d[2] = g.d[3] = 1;
   g.V = b->Vtot;
-  QB_CUDA(qgb::launch_evolve<R>(g, U, P, eps, unit, 0, b->stream));
+  QB_KERNEL(b, qgb::launch_evolve<R>(g, U, P, eps, unit, 0, b->stream));
   return QGB_OK;
 }
 
@@ -164,7 +172,7 @@ int batch_md(qgb_batch_s* b, void* gf, void* gm, void* tmp, int n_step, double m
       QB_RC(batch_force<R>(b, qgb::FORCE_UPDATE, bargs(gf, gm, dt, 1)));
       QB_RC(batch_evolve<R>(b, gf, gm, 0.5 * dt, unit_each));
       if (reunit_every > 0 && (i + 1) % reunit_every == 0 && i + 1 < n_step)
-        QB_CUDA((qgb::launch_unitarize<R, double>(g, 4, gf, b->stream)));
+        QB_KERNEL(b, (qgb::launch_unitarize<R, double>(g, 4, gf, b->stream)));
     }
   } else {
     return bfail(QGB_ERR_INVALID_ARG, "unknown integrator");
@@ -175,14 +183,14 @@ int batch_md(qgb_batch_s* b, void* gf, void* gm, void* tmp, int n_step, double m
 // Per-chain Hamiltonian pieces of (gm, gf0) into d_sums[slot * n ...]: gm, plaq, rect.
 int batch_hamiltonian(qgb_batch_s* b, int slot)
 {
-  QB_CUDA(qgb::launch_site_values_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, 0, 0, b->gm, b->d_vals,
+  QB_KERNEL(b, qgb::launch_site_values_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, 0, 0, b->gm, b->d_vals,
                                                 b->stream));
-  QB_CUDA(qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals, b->d_sums + (long)slot * b->n, b->stream));
-  QB_CUDA(qgb::launch_site_values_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, 1, b->rect ? 1 : 0, b->gf0,
+  QB_KERNEL(b, qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals, b->d_sums + (long)slot * b->n, b->stream));
+  QB_KERNEL(b, qgb::launch_site_values_batch<double>(b->Vtot, b->n, b->d_offs, b->d_chains, 1, b->rect ? 1 : 0, b->gf0,
                                                 b->d_vals, b->stream));
-  QB_CUDA(qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals, b->d_sums + (long)(slot + 1) * b->n, b->stream));
+  QB_KERNEL(b, qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals, b->d_sums + (long)(slot + 1) * b->n, b->stream));
   if (b->rect)
-    QB_CUDA(qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals + b->Vtot, b->d_sums + (long)(slot + 2) * b->n,
+    QB_KERNEL(b, qgb::launch_segment_sum(b->n, b->d_offs, b->d_vals + b->Vtot, b->d_sums + (long)(slot + 2) * b->n,
                                     b->stream));
   else
     QB_CUDA(cudaMemsetAsync(b->d_sums + (long)(slot + 2) * b->n, 0, b->n * sizeof(double), b->stream));
@@ -192,25 +200,26 @@ int batch_hamiltonian(qgb_batch_s* b, int slot)
 // One trajectory of every chain, enqueued on b->stream (recordable as a graph).
 int enqueue_trajectory(qgb_batch_s* b, int n_step, double md_time, int integrator, int mixed, int reunit)
 {
+  b->kernels = 0;
   const size_t bytes64 = (size_t)qgb::padded_sites(b->Vtot) * 72 * sizeof(double);
   const long n = qgb::padded_sites(b->Vtot) * 72;
   qgb::Geo g;
   g.d[0] = g.d[1] = g.d[2] = g.d[3] = 1;
   g.V = b->Vtot;
   QB_CUDA(cudaMemcpyAsync(b->gf0, b->gf, bytes64, cudaMemcpyDeviceToDevice, b->stream));
-  QB_CUDA(qgb::launch_rand_momentum_batch<double>(b->Vtot, b->n, b->d_offs, b->d_rs, 1.0, b->gm, b->d_ambiguous,
+  QB_KERNEL(b, qgb::launch_rand_momentum_batch<double>(b->Vtot, b->n, b->d_offs, b->d_rs, 1.0, b->gm, b->d_ambiguous,
                                                   b->stream));
   QB_RC(batch_hamiltonian(b, 0));
   if (mixed) {
-    QB_CUDA((qgb::launch_convert<double, float>(n, b->gf0, b->gf32, b->stream)));
-    QB_CUDA((qgb::launch_convert<double, float>(n, b->gm, b->gm32, b->stream)));
+    QB_KERNEL(b, (qgb::launch_convert<double, float>(n, b->gf0, b->gf32, b->stream)));
+    QB_KERNEL(b, (qgb::launch_convert<double, float>(n, b->gm, b->gm32, b->stream)));
     QB_RC(batch_md<float>(b, b->gf32, b->gm32, b->tmp32, n_step, md_time, integrator, reunit > 0 ? 0 : 1, reunit));
-    QB_CUDA((qgb::launch_convert<float, double>(n, b->gf32, b->gf0, b->stream)));
-    QB_CUDA((qgb::launch_convert<float, double>(n, b->gm32, b->gm, b->stream)));
+    QB_KERNEL(b, (qgb::launch_convert<float, double>(n, b->gf32, b->gf0, b->stream)));
+    QB_KERNEL(b, (qgb::launch_convert<float, double>(n, b->gm32, b->gm, b->stream)));
   } else {
     QB_RC(batch_md<double>(b, b->gf0, b->gm, b->tmp, n_step, md_time, integrator, 1, 0));
   }
-  QB_CUDA((qgb::launch_unitarize<double, double>(g, 4, b->gf0, b->stream)));
+  QB_KERNEL(b, (qgb::launch_unitarize<double, double>(g, 4, b->gf0, b->stream)));
   QB_RC(batch_hamiltonian(b, 3));
   QB_CUDA(cudaMemcpyAsync(b->h_sums, b->d_sums, 6 * b->n * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
   return QGB_OK;
@@ -361,6 +370,7 @@ int qgb_batch_trajectory(qgb_batch* b, const uint32_t* rs_momentum, int32_t n_st
         return rc;
       }
       if (e != cudaSuccess) return bfail(QGB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+      b->graph_kernels[key] = b->kernels;
       cudaGraphExec_t exec = nullptr;
       e = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
@@ -368,8 +378,10 @@ int qgb_batch_trajectory(qgb_batch* b, const uint32_t* rs_momentum, int32_t n_st
       it = b->graphs.emplace(key, exec).first;
     }
     QB_CUDA(cudaGraphLaunch(it->second, b->stream));
+    qgb::add_launches(b->graph_kernels[key]);
   } else {
     QB_RC(enqueue_trajectory(b, n_step, md_time, integrator, mixed, reunit));
+    qgb::add_launches(b->kernels);
   }
   QB_CUDA(cudaStreamSynchronize(b->stream));
   const int n = b->n;
@@ -415,6 +427,7 @@ int qgb_batch_run_hmc(qgb_batch* b, const uint32_t* rs, int32_t traj, int32_t n_
   }
   QB_CUDA(cudaMemcpyAsync(b->d_flags, b->h_flags, b->n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   QB_CUDA(qgb::launch_accept_batch<double>(b->Vtot, b->n, b->d_offs, b->d_flags, b->gf, b->gf0, b->stream));
+  qgb::add_launches(1);
   QB_CUDA(cudaStreamSynchronize(b->stream));
   return QGB_OK;
 }
@@ -425,6 +438,7 @@ int qgb_batch_accept(qgb_batch* b, const int32_t* flags)
   for (int c = 0; c < b->n; ++c) b->h_flags[c] = flags[c] ? 1 : 0;
   QB_CUDA(cudaMemcpyAsync(b->d_flags, b->h_flags, b->n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   QB_CUDA(qgb::launch_accept_batch<double>(b->Vtot, b->n, b->d_offs, b->d_flags, b->gf, b->gf0, b->stream));
+  qgb::add_launches(1);
   QB_CUDA(cudaStreamSynchronize(b->stream));
   return QGB_OK;
 }
