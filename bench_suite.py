@@ -26,6 +26,8 @@ Command line (one JSON line each; the profile-* commands run one small case
 of one kernel family, for ncu -k captures):
 
     python bench_suite.py c1|c3|c4|c5
+    python bench_suite.py functions hmc|flow [--reps 20]
+    python bench_suite.py slabs [--lattice 24,24,24,64] [--precision mixed|fp64] [--halo 4|2]
     python bench_suite.py profile-force [--lattice 24,24,24,48] [--variants 10,14] [--c1 -0.331]
     python bench_suite.py profile-flow [--lattice 32,32,32,32] [--steps 4]
     python bench_suite.py profile-hmc [--lattice 24,24,24,48] [--trajs 1] [--fp32-variant V]
@@ -320,6 +322,126 @@ def reference_pairs(lattice, beta, c1, sigma, samples, threads):
 
 
 # ---------------------------------------------------------------------------
+# single API functions, as a user calls them
+
+def functions(q, which, reps=20, lattice=None):
+    """Seconds per call of single API functions (launch, kernels and, for the
+    scalar results, the read-back; a synchronisation after every call) on the
+    hot start set_rand(RngState(name).split('gf-init'), sigma, 1).  hmc: 24^3 x 64
+    Iwasaki set_gm_force, gf_evolve, the Hamiltonians, the momentum draw,
+    unitarize, gf_avg_plaq (the autotuner first); flow: 32^4 RK3 Wilson flow
+    step, energy density, clover and 5-loop charges."""
+    hmc = which == "hmc"
+    ts = lattice or ((24, 24, 24, 64) if hmc else (32, 32, 32, 32))
+    rs = q.RngState("b200-c2-24x64-iwasaki" if hmc else "b200-c3-32x32-flow")
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(rs.split("gf-init"), 0.3 if hmc else 0.5, 1)
+    out = {"set": which, "lattice": list(ts), "reps": reps}
+
+    def per_call(fn):
+        for _ in range(2):
+            fn()
+        q.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+            q.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    if hmc:
+        ga = q.GaugeAction(2.13, -0.331)
+        q.autotune_force(gf, ga.c1())
+        gm = q.GaugeMomentum(gf.geo)
+        gm.set_rand(rs.split("1").split("set_rand_gauge_momentum"), 1.0)
+        force = q.GaugeMomentum(gf.geo)
+        out["set_gm_force"] = per_call(lambda: q.set_gm_force(force, gf, ga))
+        out["gf_evolve"] = per_call(lambda: q.gf_evolve(gf, gm, 1e-3))
+        out["gm_hamilton_node"] = per_call(lambda: q.gm_hamilton_node(gm))
+        out["gf_hamilton_node"] = per_call(lambda: q.gf_hamilton_node(gf, ga))
+        out["set_rand_gauge_momentum"] = per_call(
+            lambda: gm.set_rand(rs.split("2").split("set_rand_gauge_momentum"), 1.0))
+        out["unitarize"] = per_call(lambda: q.unitarize(gf))
+        out["gf_avg_plaq"] = per_call(lambda: q.gf_avg_plaq(gf))
+    else:
+        out["gf_wilson_flow_step"] = per_call(lambda: q.gf_wilson_flow_step(gf, 0.05, c1=0.0))
+        out["gf_energy_density"] = per_call(lambda: q.gf_energy_density(gf))
+        out["clf_topology_sum"] = per_call(lambda: q.gf_topology_clf(gf))
+        out["topology_charge_5"] = per_call(lambda: q.topology_charge_5(gf))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# one chain held as a time slab (the multi-GPU decomposition) on one GPU
+
+def slabs(q, args):
+    """Iwasaki (beta 2.13, c1 -0.331) force-gradient trajectories of n_step steps,
+    always accepted, from one hot start: the plain single-GPU form and the same
+    chain held as a one-rank time slab, whose halo is its own periodic copy
+    refreshed through pack / unpack before every force evaluation.  The slab
+    form computes the extra halo slices and stops the stream at every
+    refresh, which is what a multi-rank run adds besides the network."""
+    import ctypes
+
+    import torch
+    ts = _lattice(args.lattice)
+    ga = q.GaugeAction(2.13, -0.331)
+    rs = q.RngState("b200-slabs-bench")
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(rs.split("gf-init"), 0.3, 1)
+    for prec in (q.F64, q.F32):
+        q.autotune_force(gf.copy(precision=prec), ga.c1())
+    sl = q.TimeSlabs(ts, halo=args.halo)
+    out = {"lattice": list(ts), "precision": args.precision, "n_step": args.n_step, "halo": sl.halo,
+           "local_time_extent": sl.nt + 2 * sl.halo}
+
+    def run(form):
+        if form == "plain":
+            g = gf.copy()
+            step = lambda t: q.run_hmc_pure_gauge(g, ga, t, rs, n_step=args.n_step, is_always_accept=True,
+                                                  precision=args.precision)
+        else:
+            g = sl.gauge_field()
+            sl.set_rand(g, rs.split("gf-init"), 0.3, 1)
+            step = lambda t: q.run_hmc_pure_gauge_slabs(sl, g, ga, t, rs, n_step=args.n_step,
+                                                        is_always_accept=True, precision=args.precision)
+        dhs, ms = [], []
+        for t in range(1, args.warmup + 1):
+            step(t)
+        torch.cuda.synchronize()
+        for t in range(args.warmup + 1, args.warmup + 1 + args.trajs):
+            t0 = time.perf_counter()
+            dhs.append(step(t)[1])
+            torch.cuda.synchronize()
+            ms.append(round((time.perf_counter() - t0) * 1e3, 2))
+        out[form + "_ms_per_traj"] = ms
+        return 1e3 * len(ms) / sum(ms), dhs
+
+    for form in args.order.split(","):
+        out[form + "_traj_per_s"], dh = run(form)
+        if form == "plain":
+            dh_plain = dh
+        else:
+            dh_slab = dh
+    out["slab_over_plain"] = out["slab_traj_per_s"] / out["plain_traj_per_s"]
+    out["max_delta_h_difference"] = max(abs(a - b) for a, b in zip(dh_plain, dh_slab))
+    g32 = sl.gauge_field().copy(precision=q.F32 if args.precision == "mixed" else q.F64)
+    for _ in range(3):
+        sl.exchange(g32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(20):
+        sl.exchange(g32)
+    torch.cuda.synchronize()
+    n = ctypes.c_int64()
+    q._lib.call("qgb_field_tslice_bytes", g32.handle, sl.halo, ctypes.byref(n))
+    out["exchange_ms"] = (time.perf_counter() - t0) / 20 * 1e3
+    out["exchange_bytes_each_way"] = 2 * n.value
+    out["exchanges_per_traj"] = 2 * args.n_step * (2 if args.halo < 4 else 1) + 2
+    return out
+
+
+
+# ---------------------------------------------------------------------------
 # small cases for ncu
 
 def profile_force(args):
@@ -381,6 +503,17 @@ def main():
     sub = ap.add_subparsers(dest="cmd", required=True)
     for name in ("c1", "c3", "c4", "c5"):
         sub.add_parser(name)
+    sl = sub.add_parser("slabs")
+    sl.add_argument("--lattice", default="24,24,24,64")
+    sl.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    sl.add_argument("--n-step", type=int, default=8)
+    sl.add_argument("--trajs", type=int, default=5)
+    sl.add_argument("--warmup", type=int, default=2)
+    sl.add_argument("--order", default="plain,slab")
+    sl.add_argument("--halo", type=int, default=4)
+    fn = sub.add_parser("functions")
+    fn.add_argument("set", choices=["hmc", "flow"])
+    fn.add_argument("--reps", type=int, default=20)
     a = sub.add_parser("profile-force")
     a.add_argument("--lattice", default="24,24,24,48")
     a.add_argument("--variants", default="10")
@@ -404,6 +537,10 @@ def main():
     legs = {"c1": leg_c1, "c3": leg_c3, "c4": leg_c4, "c5": leg_c5}
     if args.cmd in legs:
         res = legs[args.cmd](q)
+    elif args.cmd == "slabs":
+        res = slabs(q, args)
+    elif args.cmd == "functions":
+        res = functions(q, args.set, args.reps)
     else:
         res = {"profile-force": profile_force, "profile-flow": profile_flow, "profile-hmc": profile_hmc}[args.cmd](args)
     print(json.dumps(res))

@@ -549,8 +549,9 @@ int qgb_force_get_variant(int32_t precision, int32_t rect, int32_t* variant);
 /* Time every variant on gf with action coefficient c1 -- `reps` steps of the
  * force-gradient integrator's two force launches (force + link shift, then
  * force + momentum update + link update), each with the variant's own
- * passes -- select the fastest for gf's precision and (c1 != 0); returns it
- * and its time per force launch.  Shapes with site map 5 (a precomputed
+ * passes -- and select the fastest for gf's precision and (c1 != 0), keeping
+ * the current shape unless another is faster by more than 2%; returns the
+ * selection and its time per force launch.  Shapes with site map 5 (a precomputed
  * field of two-link products, 16 color matrices per site of scratch) are not
  * timed; qgb_force_set_variant selects them. */
 int qgb_autotune_force(const qgb_field* gf, double c1, int32_t reps, int32_t* best, double* best_ms);

@@ -363,9 +363,10 @@ __global__ void __launch_bounds__(RED_BS, 2) k_action_loops(Geo g, const Cx<R>* 
 //   rect, long side a = Re tr([U_a(x) U_a(x+a) U_b(x+2a)] [Pb U_a(x+a+b)]^+)
 //   rect, long side b = Re tr([U_b(x) U_b(x+b) U_a(x+2b)] [Pa U_b(x+a+b)]^+)
 // 8 products, 3 traces and 10 link loads per plane instead of 10, 3 and 16:
-// the loops of hmc.cpp:203-252, grouped differently.
+// the loops of hmc.cpp:203-252, grouped differently.  The plaquette-only sum
+// (gf_avg_plaq, Wilson actions) fits 128 registers and runs two blocks per SM.
 template <typename R, bool RECT>
-__global__ void __launch_bounds__(RED_BS, 1) k_action_corners(Geo g, const Cx<R>* Up, double* partials,
+__global__ void __launch_bounds__(RED_BS, RECT ? 1 : 2) k_action_corners(Geo g, const Cx<R>* Up, double* partials,
                                                               Cx<float>* copy)
 {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
