@@ -986,7 +986,7 @@ int qgb_field_copy(qgb_field* dst, const qgb_field* src)
             "qgb_field_copy: geometry / multiplicity / kind mismatch");
   if (dst == src) return QGB_OK;
   const long n = n_store(dst);
-  Prof p("convert");
+  Prof p("convert", dst->prec == src->prec ? 0 : 1);  // a same-precision copy is a memcpy, not a kernel
   if (dst->prec == src->prec) {
     QGB_TRY_CUDA(cudaMemcpyAsync(dst->d, src->d, dst->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
   } else if (src->prec == QGB_F64) {
