@@ -230,7 +230,10 @@ def our_arm(args):
     B.build()
     import qlat_b200 as q
     q.set_device(torch.cuda.current_device())
-    stream = torch.cuda.current_stream()
+    # one non-default stream for torch and the library: the legacy default
+    # stream cannot be captured, so trajectories replay as CUDA graphs only here
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     q.set_stream(stream.cuda_stream)
 
     lattice = tuple(int(v) for v in args.lattice.split(","))

@@ -142,7 +142,10 @@ def leg_matched(q, gf_start, ga, rs, first_traj, n_traj, n_step, reunit_interval
 def leg_c1(q, n_traj=10):
     """8^4 Wilson beta = 5.5 leapfrog, 6 steps per unit trajectory, hot start
     at scale 1 (RngState('b200-c1-8x4-wilson').split('gf-init')), through
-    run_hmc_pure_gauge; device time per trajectory."""
+    run_hmc_pure_gauge; device time per trajectory.  The n_traj trajectories
+    run three times from the same start with the same random streams: untimed
+    (the library records its trajectory graphs), timed with graph replay (the
+    default), and timed with the kernels launched one by one."""
     ts = (8, 8, 8, 8)
     ga = q.GaugeAction(5.5, 0.0)
     out = {"lattice": list(ts), "beta": 5.5, "integrator": "leapfrog", "n_step": 6, "trajectories": n_traj}
@@ -150,17 +153,29 @@ def leg_c1(q, n_traj=10):
         rs = q.RngState("b200-c1-8x4-wilson")
         gf = q.GaugeField(q.Geometry(ts))
         gf.set_rand(rs.split("gf-init"), 1.0, 1)
-        for t in range(1, 4):
-            q.run_hmc_pure_gauge(gf.copy(), ga, t, rs.split("warm"), n_step=6, integrator="leapfrog",
-                                 precision=prec)
-        fl = []
-        with DeviceTimer(q) as tm:
-            for t in range(1, n_traj + 1):
-                f, _ = q.run_hmc_pure_gauge(gf, ga, t, rs.split("hmc"), n_step=6, integrator="leapfrog",
-                                            precision=prec)
-                fl.append(f)
-        out[prec] = {"traj_per_s": n_traj / (tm.ms / 1e3), "ms_per_traj": tm.ms / n_traj, "accepts": _flags(fl),
-                     "plaq_end": q.gf_avg_plaq(gf)}
+        start = gf.copy()
+
+        def chain():
+            nonlocal gf
+            gf @= start
+            fl = []
+            with DeviceTimer(q) as tm:
+                for t in range(1, n_traj + 1):
+                    f, _ = q.run_hmc_pure_gauge(gf, ga, t, rs.split("hmc"), n_step=6, integrator="leapfrog",
+                                                precision=prec)
+                    fl.append(f)
+            return tm.ms, fl
+
+        chain()
+        ms, fl = chain()
+        plaq = q.gf_avg_plaq(gf)
+        q.set_trajectory_graphs(False)
+        ms_direct, fl_direct = chain()
+        q.set_trajectory_graphs(True)
+        assert fl_direct == fl
+        out[prec] = {"traj_per_s": n_traj / (ms / 1e3), "ms_per_traj": ms / n_traj, "accepts": _flags(fl),
+                     "plaq_end": plaq, "graph_replay": True,
+                     "direct_launches": {"ms_per_traj": ms_direct / n_traj, "plaq_end": q.gf_avg_plaq(gf)}}
     return out
 
 
@@ -533,6 +548,7 @@ def main():
     B.build()
     import qlat_b200 as q
     q.set_device(0)
+    torch.cuda.set_stream(torch.cuda.Stream())  # not the legacy default stream: trajectories replay as graphs
     q.set_stream(torch.cuda.current_stream().cuda_stream)
     legs = {"c1": leg_c1, "c3": leg_c3, "c4": leg_c4, "c5": leg_c5}
     if args.cmd in legs:

@@ -182,6 +182,17 @@ int qgb_run_hmc_evolve(qgb_field* gm, qgb_field* gf, double beta, double c1, int
 int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c1, int32_t n_step,
                              double md_time, int32_t integrator, int32_t reunit_interval,
                              double* delta_h);
+/* The two entry points above replay their kernels as a CUDA graph (no
+ * counterpart in the reference): the first call with given fields, geometry,
+ * parameters and force-kernel shapes launches directly, the second records
+ * the launches and replays them, later calls replay -- the same kernels with
+ * the same arguments, one graph launch instead of 40 or more kernel launches.
+ * Direct launches are used while per-kernel timing is on, while the caller
+ * captures the stream and on the legacy default stream.  enable = 0 switches
+ * graphs off (and frees the recorded ones); qgb_trajectory_graph_count gives
+ * the number held (at most 16, least recently used dropped first). */
+int qgb_set_trajectory_graphs(int32_t enable);
+int qgb_trajectory_graph_count(int32_t* n);
 
 /* Halo hook of a domain-decomposed trajectory: called with a link field
  * before a force evaluation reads it, after the kernels before it have been

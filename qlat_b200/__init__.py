@@ -68,6 +68,21 @@ def rng_ambiguous_count() -> int:
     return int(n.value)
 
 
+def set_trajectory_graphs(enable: bool = True) -> None:
+    """Replay trajectories (run_hmc_evolve_pure_gauge, both precisions) as
+    CUDA graphs (default) or launch their kernels one by one."""
+    from ._lib import call
+    call("qgb_set_trajectory_graphs", int(bool(enable)))
+
+
+def trajectory_graph_count() -> int:
+    import ctypes
+    from ._lib import call
+    n = ctypes.c_int32()
+    call("qgb_trajectory_graph_count", ctypes.byref(n))
+    return int(n.value)
+
+
 def launch_count() -> int:
     import ctypes
     from ._lib import call

@@ -116,6 +116,8 @@ SIGNATURES = {
                            ctypes.c_int32, c_dbl_p],
     "qgb_run_hmc_evolve_mixed": [c_field, c_field, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                  ctypes.c_double, ctypes.c_int32, ctypes.c_int32, c_dbl_p],
+    "qgb_set_trajectory_graphs": [ctypes.c_int32],
+    "qgb_trajectory_graph_count": [c_i32_p],
     "qgb_run_md_hooked": [c_field, c_field, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_double,
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, HALO_HOOK, ctypes.c_void_p],
     "qgb_set_wilson_flow_z": [c_field, c_field, ctypes.c_double],

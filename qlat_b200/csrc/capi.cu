@@ -414,6 +414,109 @@ ForceArgs fargs(const void* U, void* out, double beta, double c1, double dt)
   return a;
 }
 
+// ---- trajectories as CUDA graphs ----------------------------------------------
+//
+// The device work of a trajectory entry point (Hamiltonian sums, molecular
+// dynamics, conversions) is a fixed sequence of launches on the library
+// stream for a given set of buffers, geometry and parameters, so it can be
+// recorded once as a CUDA graph and replayed: one graph launch instead of 40
+// or more kernel launches, whose host cost (a few microseconds each) sets the
+// time of a trajectory on small lattices.  The key holds every device pointer
+// the recorded launches use, the geometry, the parameters and the force-kernel
+// shapes selected at recording, so a replay runs exactly the kernels a direct
+// call would, with the same arguments.  The first call with a key runs
+// directly (it may allocate the library's buffers), the second records and
+// replays, later calls replay.  Direct launches are used while per-kernel
+// timing is on, while the caller is capturing the stream, on the legacy
+// default stream, and when graphs are switched off (qgb_set_trajectory_graphs).
+struct TrajGraph {
+  cudaGraphExec_t exec = nullptr;
+  int64_t kernels = 0;  // the kernel launches the graph holds (qgb_launch_count)
+  int calls = 0;
+  bool direct_only = false;  // recording failed once: run this key directly
+  uint64_t last_use = 0;
+};
+std::map<std::vector<uint64_t>, TrajGraph> g_traj_graphs;
+bool g_traj_graphs_on = true;
+uint64_t g_traj_clock = 0;
+const int MAX_TRAJ_GRAPHS = 16;
+
+uint64_t key_bits(double v)
+{
+  uint64_t u;
+  memcpy(&u, &v, sizeof(u));
+  return u;
+}
+uint64_t key_ptr(const void* p) { return (uint64_t)(uintptr_t)p; }
+
+void drop_traj_graphs()
+{
+  for (auto& kv : g_traj_graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  g_traj_graphs.clear();
+}
+
+// Runs body() (launches on the library stream only: no allocation, no host
+// synchronisation) directly or through the graph cached for `key`.
+template <typename F>
+int run_graphed(std::vector<uint64_t> key, F&& body)
+{
+  if (!g_traj_graphs_on || g_ctx.prof_on || g_ctx.stream == nullptr || g_ctx.stream == cudaStreamLegacy) return body();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(g_ctx.stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    (void)cudaGetLastError();
+    return body();
+  }
+  key.push_back(key_ptr(g_ctx.partials));
+  key.push_back(key_ptr(g_ctx.results));
+  for (int p = 0; p < 2; ++p)
+    for (int r = 0; r < 2; ++r) key.push_back((uint64_t)g_force_variant[p][r]);
+  TrajGraph& e = g_traj_graphs[key];
+  e.last_use = ++g_traj_clock;
+  if (e.exec) {
+    QGB_TRY_CUDA(cudaGraphLaunch(e.exec, g_ctx.stream));
+    g_launches += e.kernels;
+    return QGB_OK;
+  }
+  if (e.direct_only || e.calls++ == 0) return body();
+  int held = 0;
+  for (auto& kv : g_traj_graphs) held += kv.second.exec != nullptr;
+  if (held >= MAX_TRAJ_GRAPHS) {
+    auto lru = g_traj_graphs.end();
+    for (auto it = g_traj_graphs.begin(); it != g_traj_graphs.end(); ++it)
+      if (it->second.exec && (lru == g_traj_graphs.end() || it->second.last_use < lru->second.last_use)) lru = it;
+    cudaGraphExecDestroy(lru->second.exec);
+    lru->second.exec = nullptr;
+  }
+  const int64_t l0 = g_launches;
+  if (cudaStreamBeginCapture(g_ctx.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    (void)cudaGetLastError();
+    e.direct_only = true;
+    return body();
+  }
+  const int rc = body();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(g_ctx.stream, &graph);
+  const int64_t nk = g_launches - l0;
+  g_launches = l0;  // recorded, not launched
+  cudaGraphExec_t exec = nullptr;
+  const bool ok = rc == QGB_OK && ce == cudaSuccess && graph != nullptr &&
+                  cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    // nothing recorded has run: run the work directly (a genuine error
+    // comes back from there)
+    (void)cudaGetLastError();
+    e.direct_only = true;
+    return body();
+  }
+  e.exec = exec;
+  e.kernels = nk;
+  QGB_TRY_CUDA(cudaGraphLaunch(e.exec, g_ctx.stream));
+  g_launches += nk;
+  return QGB_OK;
+}
+
 // Molecular dynamics of one trajectory in precision R on raw SoA buffers
 // (no Hamiltonians).  gf, gm updated in place; tmp: a link buffer.
 // Force-gradient: hmc.pyx:169-188 with gm_evolve_fg_pure_gauge fused as
@@ -715,6 +818,25 @@ int qgb_set_stream(void* stream)
   if (g_ctx.own_stream) cudaStreamDestroy(g_ctx.stream);
   g_ctx.stream = (cudaStream_t)stream;
   g_ctx.own_stream = false;
+  return QGB_OK;
+}
+
+int qgb_set_trajectory_graphs(int32_t enable)
+{
+  QGB_CTX();
+  QGB_TRY_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  g_traj_graphs_on = enable != 0;
+  if (!g_traj_graphs_on) drop_traj_graphs();
+  return QGB_OK;
+}
+
+int qgb_trajectory_graph_count(int32_t* n)
+{
+  QGB_CHECK(n, QGB_ERR_INVALID_ARG, "qgb_trajectory_graph_count: null output");
+  std::lock_guard<std::recursive_mutex> lock(g_mu);
+  int c = 0;
+  for (auto& kv : g_traj_graphs) c += kv.second.exec != nullptr;
+  *n = c;
   return QGB_OK;
 }
 
@@ -1395,13 +1517,30 @@ int qgb_run_hmc_evolve(qgb_field* gm, qgb_field* gf, double beta, double c1, int
   const Geo g = geo_of(gf);
   void* tmp = nullptr;
   QGB_RC(get_scratch(gf->bytes, 1, &tmp));
-  QGB_RC(hamiltonian_slots(gm, gf, c1, 0));
-  if (gf->prec == QGB_F64)
-    QGB_RC(md_trajectory<double>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, 1, 0));
-  else
-    QGB_RC(md_trajectory<float>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, 1, 0));
-  QGB_RC(qgb_unitarize(gf));
-  QGB_RC(hamiltonian_slots(gm, gf, c1, 3));
+  QGB_RC(ensure_partials((size_t)qgb::reduce_blocks(g) * 2));
+  const std::vector<uint64_t> key = {1,
+                                     key_ptr(gm->d),
+                                     key_ptr(gf->d),
+                                     key_ptr(tmp),
+                                     (uint64_t)gf->dims[0],
+                                     (uint64_t)gf->dims[1],
+                                     (uint64_t)gf->dims[2],
+                                     (uint64_t)gf->dims[3],
+                                     (uint64_t)gf->prec,
+                                     key_bits(beta),
+                                     key_bits(c1),
+                                     (uint64_t)n_step,
+                                     key_bits(md_time),
+                                     (uint64_t)integrator};
+  QGB_RC(run_graphed(key, [&]() -> int {
+    QGB_RC(hamiltonian_slots(gm, gf, c1, 0));
+    if (gf->prec == QGB_F64)
+      QGB_RC(md_trajectory<double>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, 1, 0));
+    else
+      QGB_RC(md_trajectory<float>(g, gf->d, gm->d, tmp, beta, c1, n_step, md_time, integrator, 1, 0));
+    QGB_RC(qgb_unitarize(gf));
+    return hamiltonian_slots(gm, gf, c1, 3);
+  }));
   double r[6];
   QGB_RC(read_results(0, 6, r));
   const double e0 = r[0] + gf_hamilton_from(r[1], r[2], beta, c1);
@@ -1425,31 +1564,49 @@ int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c
   QGB_RC(get_scratch(b32, 11, &gf32));
   QGB_RC(get_scratch(b32, 12, &gm32));
   QGB_RC(get_scratch(b32, 13, &tmp32));
-  // H0's two sums, each writing the FP32 copy of its field in the same pass
   const int nb = qgb::reduce_blocks(g);
   QGB_RC(ensure_partials((size_t)nb * 2));
-  {
-    Prof p("reduce", 4);
-    QGB_TRY_CUDA((qgb::launch_gm_hamilton_convert<double, float>(g, gm->d, gm32, g_ctx.partials, g_ctx.stream)));
-    QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 0, g_ctx.stream));
-    QGB_TRY_CUDA(qgb::launch_action<double>(g, gf->d, c1 != 0.0, g_ctx.partials, g_ctx.stream, gf32));
-    QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, c1 != 0.0 ? 2 : 1, nb, g_ctx.results, 1, g_ctx.stream));
-  }
   const int unit_each = reunit_interval > 0 ? 0 : 1;
-  QGB_RC(md_trajectory<float>(g, gf32, gm32, tmp32, beta, c1, n_step, md_time, integrator, unit_each,
-                              reunit_interval));
-  // back to FP64: the links unitarised in the same pass, the momenta with H1's
-  // kinetic sum
-  {
-    Prof p("unitarize");
-    QGB_TRY_CUDA(qgb::launch_unitarize_to_f64(g, gf32, gf->d, g_ctx.stream));
-  }
-  {
-    Prof p("reduce", 2);
-    QGB_TRY_CUDA((qgb::launch_gm_hamilton_convert<float, double>(g, gm32, gm->d, g_ctx.partials, g_ctx.stream)));
-    QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 3, g_ctx.stream));
-  }
-  QGB_RC(action_slot(gf, c1 != 0.0, 4));
+  const std::vector<uint64_t> key = {2,
+                                     key_ptr(gm->d),
+                                     key_ptr(gf->d),
+                                     key_ptr(gf32),
+                                     key_ptr(gm32),
+                                     key_ptr(tmp32),
+                                     (uint64_t)gf->dims[0],
+                                     (uint64_t)gf->dims[1],
+                                     (uint64_t)gf->dims[2],
+                                     (uint64_t)gf->dims[3],
+                                     key_bits(beta),
+                                     key_bits(c1),
+                                     (uint64_t)n_step,
+                                     key_bits(md_time),
+                                     (uint64_t)integrator,
+                                     (uint64_t)reunit_interval};
+  QGB_RC(run_graphed(key, [&]() -> int {
+    // H0's two sums, each writing the FP32 copy of its field in the same pass
+    {
+      Prof p("reduce", 4);
+      QGB_TRY_CUDA((qgb::launch_gm_hamilton_convert<double, float>(g, gm->d, gm32, g_ctx.partials, g_ctx.stream)));
+      QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 0, g_ctx.stream));
+      QGB_TRY_CUDA(qgb::launch_action<double>(g, gf->d, c1 != 0.0, g_ctx.partials, g_ctx.stream, gf32));
+      QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, c1 != 0.0 ? 2 : 1, nb, g_ctx.results, 1, g_ctx.stream));
+    }
+    QGB_RC(md_trajectory<float>(g, gf32, gm32, tmp32, beta, c1, n_step, md_time, integrator, unit_each,
+                                reunit_interval));
+    // back to FP64: the links unitarised in the same pass, the momenta with H1's
+    // kinetic sum
+    {
+      Prof p("unitarize");
+      QGB_TRY_CUDA(qgb::launch_unitarize_to_f64(g, gf32, gf->d, g_ctx.stream));
+    }
+    {
+      Prof p("reduce", 2);
+      QGB_TRY_CUDA((qgb::launch_gm_hamilton_convert<float, double>(g, gm32, gm->d, g_ctx.partials, g_ctx.stream)));
+      QGB_TRY_CUDA(qgb::launch_finalize(g_ctx.partials, 1, nb, g_ctx.results, 3, g_ctx.stream));
+    }
+    return action_slot(gf, c1 != 0.0, 4);
+  }));
   double r[6];
   QGB_RC(read_results(0, 6, r));
   const double e0 = r[0] + gf_hamilton_from(r[1], r[2], beta, c1);

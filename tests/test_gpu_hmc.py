@@ -218,3 +218,47 @@ def test_mixed_leapfrog_close_to_fp64(q, n_step):
                                            precision="mixed", reunit_interval=reunit)
         assert abs(dh32 - dh64) < 2e-3 * max(1.0, abs(dh64)) + 5e-4, (reunit, dh32, dh64)
         assert abs(q.gf_avg_plaq(g32) - q.gf_avg_plaq(g64)) < 1e-6
+
+
+@pytest.mark.parametrize("precision,integrator", [("fp64", "force-gradient"), ("mixed", "force-gradient"),
+                                                  ("mixed", "leapfrog")])
+def test_trajectory_graph_replay_matches_direct(q, precision, integrator):
+    """A trajectory replayed from its CUDA graph (second call records, later
+    calls replay) is bit for bit the trajectory of direct launches, with the
+    same kernel count."""
+    geo = q.Geometry((4, 4, 6, 8))
+    ga = q.GaugeAction(2.13, -0.331)
+    rs = q.RngState("test_graph_replay")
+    start = q.GaugeField(geo)
+    start.set_rand(rs.split("init"), 0.3, 2)
+    gm0 = q.GaugeMomentum(geo)
+    gm0.set_rand(rs.split("gm"), 1.0)
+    kw = dict(integrator=integrator, precision=precision, reunit_interval=2)
+    gf, gm = q.GaugeField(geo), q.GaugeMomentum(geo)
+    q.set_trajectory_graphs(False)
+    try:
+        gf @= start
+        gm @= gm0
+        l0 = q.launch_count()
+        dh_direct = q.run_hmc_evolve_pure_gauge(gm, gf, ga, None, 5, 1.0, **kw)
+        n_direct = q.launch_count() - l0
+        gf_direct, gm_direct = np.asarray(gf).copy(), np.asarray(gm).copy()
+    finally:
+        q.set_trajectory_graphs(True)
+    assert q.trajectory_graph_count() == 0
+    for call in range(4):
+        gf @= start
+        gm @= gm0
+        l0 = q.launch_count()
+        dh = q.run_hmc_evolve_pure_gauge(gm, gf, ga, None, 5, 1.0, **kw)
+        assert q.launch_count() - l0 == n_direct
+        assert dh == dh_direct, (call, dh, dh_direct)
+        assert np.array_equal(np.asarray(gf), gf_direct), call
+        assert np.array_equal(np.asarray(gm), gm_direct), call
+        assert q.trajectory_graph_count() == (0 if call == 0 else 1)
+    # another parameter is another graph
+    gf @= start
+    gm @= gm0
+    q.run_hmc_evolve_pure_gauge(gm, gf, ga, None, 6, 1.0, **kw)
+    q.run_hmc_evolve_pure_gauge(gm, gf, ga, None, 6, 1.0, **kw)
+    assert q.trajectory_graph_count() == 2
