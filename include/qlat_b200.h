@@ -597,7 +597,7 @@ int qgb_force_time_variant(const qgb_field* gf, double c1, int32_t variant, int3
  * fixed 1 MiB device array inside the library, which every GPU that loads the
  * library holds until the process exits.  The first call on each device looks
  * up that array's device address (cudaGetSymbolAddress) with the device
- * current; make that first call before any stream capture.  All calls share
+ * current.  All calls share
  * the one array and it keeps the last call's partial sums (each call
  * overwrites every entry it reads, so nothing needs to start at zero): calls
  * that overlap on the GPU -- two streams, or two host threads -- race and must
