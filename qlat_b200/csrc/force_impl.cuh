@@ -442,7 +442,7 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
       // thread's own link of W (or of U, written to W: the fused leapfrog
       // step, whose next force reads W)
       const WField<R> W{(Cx<R>*)a.ev, stride};
-      M3<R> wn = mul(exp_ch(scale(R(a.ev_eps), p)), a.ev_from_u ? U.ld(s, mu) : W.ld(s, mu));
+      M3<R> wn = mul(exp_md(scale(R(a.ev_eps), p)), a.ev_from_u ? U.ld(s, mu) : W.ld(s, mu));
       if (a.ev_unit == 1) unitarize(wn);
       else if (a.ev_unit == 2) unitarize_as<double, R>(wn);
       W.st(s, mu, wn);
@@ -454,7 +454,7 @@ __device__ __forceinline__ void force_epilogue(const ForceArgs& a, const CField<
       if (a.zp != nullptr && a.b != 0.0) axpy(Z, R(a.b), CField<R>{(const Cx<R>*)a.zp, stride}.ld(s, mu));
       if (a.z != nullptr) WField<R>{(Cx<R>*)a.z, stride}.st(s, mu, Z);
     }
-    M3<R> un = mul(exp_ch(scale(R(a.dt), Z)), u);
+    M3<R> un = mul(exp_md(scale(R(a.dt), Z)), u);
     if (a.unitarize) unitarize(un);
     WField<R>{(Cx<R>*)a.out, stride}.st(s, mu, un);
   }
