@@ -541,6 +541,46 @@ int qgb_field_tslice_bytes(const qgb_field* f, int32_t nt, int64_t* bytes);
 int qgb_field_pack_tslices(const qgb_field* f, int32_t t0, int32_t nt, void* dev);
 int qgb_field_unpack_tslices(qgb_field* f, int32_t t0, int32_t nt, const void* dev);
 
+/* ---- four-dimensional domain decomposition (Geometry's node partition and
+ * expanded fields: core.h:17-110 GeometryNode / node_site / expansion_left,
+ * field-expand.h:116-200 refresh_expanded, hmc.cpp:466-490) --------------- */
+
+/* Make f the domain of one rank of a decomposed lattice of global extents
+ * global_site: the rank owns the sites with global coordinates
+ * [origin_k, origin_k + dims_k - 2 halo_k) and f holds them with halo_k sites
+ * of the neighbouring domains on either side in each direction k (the
+ * reference's node_site with expansion_left = expansion_right = halo).  A
+ * direction with halo_k = 0 is not cut: f holds all of it (dims_k =
+ * global_site_k, origin_k = 0) and wraps periodically.  Then, on f:
+ *  - the force (qgb_set_gm_force, the fused kernels of qgb_run_md_hooked) is
+ *    evaluated on the owned sites only, reading the halo, which the caller
+ *    refreshes before each force (the hook of qgb_run_md_hooked);
+ *  - the _node sums (gm_hamilton_node, gf_hamilton_node, the _sites action
+ *    sums) are over the owned sites, as the reference's node sums are over
+ *    its node's sites;
+ *  - the per-site random streams (set_rand_gauge_momentum, set_rand) are
+ *    those of each local site's global index, so the owned sites draw what a
+ *    single field of the whole lattice draws (and the halo sites what their
+ *    owners draw);
+ *  - element-wise operations run on every local site;
+ *  - qgb_run_md_hooked with the force-gradient integrator needs
+ *    refresh_shifted = 1 (the shifted field, too, is evaluated on the owned
+ *    sites only);
+ *  - qgb_run_hmc_evolve[_mixed], the gradient flow, the clover and 5-loop
+ *    charges and gf_avg_plaq refuse it (QGB_ERR_INVALID_ARG).
+ * qgb_field_copy copies the domain with the data. */
+int qgb_field_set_domain(qgb_field* f, const int32_t global_site[4], const int32_t origin[4],
+                         const int32_t halo[4]);
+int qgb_field_domain(const qgb_field* f, int32_t* has_domain, int32_t global_site[4], int32_t origin[4],
+                     int32_t halo[4]);
+/* Copy the local sites [lo_k, lo_k + n_k) of every component of f into a
+ * device buffer of qgb_field_box_bytes(f, n) bytes (entry-major: for each
+ * component and matrix entry, the box's sites with x fastest), or back: the
+ * faces a halo exchange sends.  Asynchronous on the library stream. */
+int qgb_field_box_bytes(const qgb_field* f, const int32_t n[4], int64_t* bytes);
+int qgb_field_pack_box(const qgb_field* f, const int32_t lo[4], const int32_t n[4], void* dev);
+int qgb_field_unpack_box(qgb_field* f, const int32_t lo[4], const int32_t n[4], const void* dev);
+
 /* ---- force-kernel autotuner (no counterpart in the reference) ---------- */
 
 /* The force kernels (set_gm_force and its fused HMC / flow consumers) exist

@@ -28,6 +28,7 @@ from .topo_measure import (gf_energy_derivative_density_field_topo, gf_flow_topo
                            gf_plaq_action_density_field, gf_plaq_field, gf_plaq_flow_force,
                            gf_spatial_plaq_action_density, gf_spatial_plaq_action_density_field, smear_measure_topo)
 from .slabs import TimeSlabs, run_hmc_evolve_slabs, run_hmc_pure_gauge_slabs
+from .domains import Domains, domain_layout, run_hmc_evolve_domains, run_hmc_pure_gauge_domains
 from .flow_adjoint import (FlowedWilsonAction, gf_flow_action, gf_flow_action_grad, gf_wilson_flow_vjp,
                            run_flowed_hmc_pure_gauge, set_anti_hermitian_matrix_from_basis,
                            set_basis_from_anti_hermitian_matrix)

@@ -82,6 +82,11 @@ SIGNATURES = {
     "qgb_field_tslice_bytes": [c_field, ctypes.c_int32, c_i64_p],
     "qgb_field_pack_tslices": [c_field, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p],
     "qgb_field_unpack_tslices": [c_field, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p],
+    "qgb_field_set_domain": [c_field, c_i32_p, c_i32_p, c_i32_p],
+    "qgb_field_domain": [c_field, c_i32_p, c_i32_p, c_i32_p, c_i32_p],
+    "qgb_field_box_bytes": [c_field, c_i32_p, c_i64_p],
+    "qgb_field_pack_box": [c_field, c_i32_p, c_i32_p, ctypes.c_void_p],
+    "qgb_field_unpack_box": [c_field, c_i32_p, c_i32_p, ctypes.c_void_p],
     "qgb_field_info": [c_field, i32x4, c_i32_p, c_i32_p, c_i32_p],
     "qgb_field_upload": [c_field, c_dbl_p],
     "qgb_field_download": [c_field, c_dbl_p],

@@ -31,6 +31,11 @@ struct qgb_field_s {
   int32_t prec;
   void* d;
   size_t bytes;
+  // domain of a decomposed lattice (qgb_field_set_domain); dom == 0: none
+  int32_t dom = 0;
+  int32_t dom_global[4] = {0, 0, 0, 0};
+  int32_t dom_origin[4] = {0, 0, 0, 0};
+  int32_t dom_halo[4] = {0, 0, 0, 0};
 };
 
 namespace
@@ -197,7 +202,25 @@ Geo geo_of(const qgb_field_s* f)
   Geo g;
   for (int i = 0; i < 4; ++i) g.d[i] = f->dims[i];
   g.V = f->V;
+  if (f->dom) {
+    for (int i = 0; i < 4; ++i) {
+      g.bl[i] = f->dom_halo[i];
+      g.bn[i] = f->dims[i] - 2 * f->dom_halo[i];
+      g.gd[i] = f->dom_global[i];
+      g.go[i] = f->dom_origin[i] - f->dom_halo[i];
+    }
+  }
   return g;
+}
+
+// Entry points whose result needs the whole lattice, or halos refreshed
+// between kernels, refuse the domain of a decomposed lattice.
+int no_domain(const qgb_field_s* f, const char* what)
+{
+  if (f && f->dom)
+    return fail(QGB_ERR_INVALID_ARG, std::string(what) + ": not available on the domain of a decomposed lattice "
+                                     "(qgb_field_set_domain); use qgb_run_md_hooked and the _node sums");
+  return QGB_OK;
 }
 
 size_t elem_reals(const qgb_field_s* f) { return f->kind == QGB_KIND_COLOR_MATRIX ? 18 : 1; }
@@ -316,6 +339,7 @@ int action_slot(const qgb_field* gf, int rect, int slot)
 
 int clover_slot(const qgb_field* gf, qgb_field* ef, qgb_field* qf, int slot)
 {
+  QGB_RC(no_domain(gf, "clover sums"));
   const Geo g = geo_of(gf);
   const int nb = qgb::reduce_blocks(g);
   QGB_RC(ensure_partials((size_t)nb * 2));
@@ -334,6 +358,7 @@ int clover_slot(const qgb_field* gf, qgb_field* ef, qgb_field* qf, int slot)
 // (and the optional terms / total fields).
 int topology_5li_slot(const qgb_field* gf, qgb_field* terms, qgb_field* total, int slot)
 {
+  QGB_RC(no_domain(gf, "topology_charge_5"));
   const Geo g = geo_of(gf);
   const int nb = qgb::reduce_blocks(g);
   QGB_RC(ensure_partials((size_t)nb * 5));
@@ -653,6 +678,7 @@ static cudaError_t fg_pair(const Geo& g, const void* U, void* T1, void* P, void*
 // buffer swap, so the field handle ends up owning the result.
 static int flow_step(qgb_field* gf, double eps, double c1, bool rk3)
 {
+  QGB_RC(no_domain(gf, "gradient flow"));
   const Geo g = geo_of(gf);
   void *T = nullptr, *Z = nullptr;
   QGB_RC(get_scratch(gf->bytes, 21, &T));
@@ -1107,6 +1133,12 @@ int qgb_field_copy(qgb_field* dst, const qgb_field* src)
   QGB_CHECK(same_geo(dst, src) && dst->mult == src->mult && dst->kind == src->kind, QGB_ERR_MISMATCH,
             "qgb_field_copy: geometry / multiplicity / kind mismatch");
   if (dst == src) return QGB_OK;
+  dst->dom = src->dom;  // the copy holds the same sites of the lattice
+  for (int i = 0; i < 4; ++i) {
+    dst->dom_global[i] = src->dom_global[i];
+    dst->dom_origin[i] = src->dom_origin[i];
+    dst->dom_halo[i] = src->dom_halo[i];
+  }
   const long n = n_store(dst);
   Prof p("convert", dst->prec == src->prec ? 0 : 1);  // a same-precision copy is a memcpy, not a kernel
   if (dst->prec == src->prec) {
@@ -1415,11 +1447,120 @@ int qgb_field_unpack_tslices(qgb_field* f, int32_t t0, int32_t nt, const void* d
   return tslice_copy(f, t0, nt, const_cast<void*>(dev), false, "qgb_field_unpack_tslices");
 }
 
+int qgb_field_set_domain(qgb_field* f, const int32_t global_site[4], const int32_t origin[4],
+                         const int32_t halo[4])
+{
+  QGB_RC(check_field(f, -1, "qgb_field_set_domain"));
+  QGB_CHECK(global_site && origin && halo, QGB_ERR_INVALID_ARG, "qgb_field_set_domain: null argument");
+  for (int i = 0; i < 4; ++i) {
+    const long owned = (long)f->dims[i] - 2L * halo[i];
+    QGB_CHECK(halo[i] >= 0 && owned >= 1 && global_site[i] >= 1 && owned <= global_site[i] && origin[i] >= 0 &&
+                  origin[i] < global_site[i],
+              QGB_ERR_BAD_GEOMETRY, "qgb_field_set_domain: direction " + std::to_string(i) +
+                                        ": need 1 <= extent - 2 halo <= global extent and 0 <= origin < global extent");
+    // a direction without a halo is not cut: the field holds all of it and its own periodic wrap is the lattice's
+    QGB_CHECK(halo[i] > 0 || (f->dims[i] == global_site[i] && origin[i] == 0), QGB_ERR_BAD_GEOMETRY,
+              "qgb_field_set_domain: direction " + std::to_string(i) +
+                  " has no halo, so the field must hold the whole global extent from origin 0");
+  }
+  long gv = 1;
+  for (int i = 0; i < 4; ++i) gv *= global_site[i];
+  QGB_CHECK(gv < (1L << 40), QGB_ERR_BAD_GEOMETRY, "qgb_field_set_domain: global lattice too large");
+  f->dom = 1;
+  for (int i = 0; i < 4; ++i) {
+    f->dom_global[i] = global_site[i];
+    f->dom_origin[i] = origin[i];
+    f->dom_halo[i] = halo[i];
+  }
+  return QGB_OK;
+}
+
+int qgb_field_domain(const qgb_field* f, int32_t* has_domain, int32_t global_site[4], int32_t origin[4],
+                     int32_t halo[4])
+{
+  QGB_RC(check_field(f, -1, "qgb_field_domain"));
+  QGB_CHECK(has_domain, QGB_ERR_INVALID_ARG, "qgb_field_domain: null output");
+  *has_domain = f->dom;
+  for (int i = 0; i < 4; ++i) {
+    if (global_site) global_site[i] = f->dom_global[i];
+    if (origin) origin[i] = f->dom_origin[i];
+    if (halo) halo[i] = f->dom_halo[i];
+  }
+  return QGB_OK;
+}
+
+// entries per site component (K) and bytes per entry of a field's storage
+static void box_entries(const qgb_field* f, int* K, size_t* esize)
+{
+  *K = f->kind == QGB_KIND_COLOR_MATRIX ? 9 : 1;
+  const size_t r = f->prec == QGB_F64 ? sizeof(double) : sizeof(float);
+  *esize = f->kind == QGB_KIND_COLOR_MATRIX ? 2 * r : r;
+}
+
+int qgb_field_box_bytes(const qgb_field* f, const int32_t n[4], int64_t* bytes)
+{
+  QGB_RC(check_field(f, -1, "qgb_field_box_bytes"));
+  QGB_CHECK(n && bytes, QGB_ERR_INVALID_ARG, "qgb_field_box_bytes: null argument");
+  int K;
+  size_t es;
+  box_entries(f, &K, &es);
+  int64_t nb = 1;
+  for (int i = 0; i < 4; ++i) {
+    QGB_CHECK(n[i] >= 0 && n[i] <= f->dims[i], QGB_ERR_INVALID_ARG, "qgb_field_box_bytes: bad box extent");
+    nb *= n[i];
+  }
+  *bytes = nb * f->mult * K * (int64_t)es;
+  return QGB_OK;
+}
+
+static int box_copy(qgb_field* f, const int32_t lo[4], const int32_t n[4], void* dev, bool unpack, const char* what)
+{
+  QGB_CTX();
+  QGB_RC(check_field(f, -1, what));
+  QGB_CHECK(lo && n && dev, QGB_ERR_INVALID_ARG, std::string(what) + ": null argument");
+  int l[4], e[4];
+  for (int i = 0; i < 4; ++i) {
+    QGB_CHECK(lo[i] >= 0 && n[i] >= 0 && (long)lo[i] + n[i] <= f->dims[i], QGB_ERR_INVALID_ARG,
+              std::string(what) + ": the box leaves the field in direction " + std::to_string(i));
+    l[i] = lo[i];
+    e[i] = n[i];
+  }
+  int K;
+  size_t es;
+  box_entries(f, &K, &es);
+  QGB_CHECK(((uintptr_t)dev % es) == 0, QGB_ERR_INVALID_ARG, std::string(what) + ": misaligned buffer");
+  const Geo g = geo_of(f);
+  Prof p("box_copy");
+  if (f->kind == QGB_KIND_COLOR_MATRIX) {
+    if (f->prec == QGB_F64)
+      QGB_TRY_CUDA(qgb::launch_box_copy<double2>(g, f->mult, K, l, e, f->d, dev, unpack, g_ctx.stream));
+    else
+      QGB_TRY_CUDA(qgb::launch_box_copy<float2>(g, f->mult, K, l, e, f->d, dev, unpack, g_ctx.stream));
+  } else {
+    if (f->prec == QGB_F64)
+      QGB_TRY_CUDA(qgb::launch_box_copy<double>(g, f->mult, K, l, e, f->d, dev, unpack, g_ctx.stream));
+    else
+      QGB_TRY_CUDA(qgb::launch_box_copy<float>(g, f->mult, K, l, e, f->d, dev, unpack, g_ctx.stream));
+  }
+  return QGB_OK;
+}
+
+int qgb_field_pack_box(const qgb_field* f, const int32_t lo[4], const int32_t n[4], void* dev)
+{
+  return box_copy(const_cast<qgb_field*>(f), lo, n, dev, false, "qgb_field_pack_box");
+}
+
+int qgb_field_unpack_box(qgb_field* f, const int32_t lo[4], const int32_t n[4], const void* dev)
+{
+  return box_copy(f, lo, n, const_cast<void*>(dev), true, "qgb_field_unpack_box");
+}
+
 int qgb_gf_avg_plaq(const qgb_field* gf, double* out)
 {
   QGB_CTX();
   QGB_RC(check_field(gf, QGB_KIND_COLOR_MATRIX, "qgb_gf_avg_plaq"));
   QGB_CHECK(out && gf->mult == 4, QGB_ERR_INVALID_ARG, "qgb_gf_avg_plaq: bad argument");
+  QGB_RC(no_domain(gf, "qgb_gf_avg_plaq"));
   QGB_RC(action_slot(gf, 0, 0));
   double sp;
   QGB_RC(read_results(0, 1, &sp));
@@ -1514,6 +1655,7 @@ int qgb_run_hmc_evolve(qgb_field* gm, qgb_field* gf, double beta, double c1, int
   QGB_CHECK(gf->mult == 4 && gm->mult == 4 && same_geo(gf, gm) && gf->prec == gm->prec, QGB_ERR_MISMATCH,
             "qgb_run_hmc_evolve: field mismatch");
   QGB_CHECK(n_step >= 1 && delta_h, QGB_ERR_INVALID_ARG, "qgb_run_hmc_evolve: bad argument");
+  QGB_RC(no_domain(gf, "qgb_run_hmc_evolve"));
   const Geo g = geo_of(gf);
   void* tmp = nullptr;
   QGB_RC(get_scratch(gf->bytes, 1, &tmp));
@@ -1558,6 +1700,7 @@ int qgb_run_hmc_evolve_mixed(qgb_field* gm, qgb_field* gf, double beta, double c
   QGB_CHECK(gf->mult == 4 && gm->mult == 4 && same_geo(gf, gm) && gf->prec == QGB_F64 && gm->prec == QGB_F64,
             QGB_ERR_MISMATCH, "qgb_run_hmc_evolve_mixed: gm and gf must be FP64 fields of one geometry");
   QGB_CHECK(n_step >= 1 && delta_h, QGB_ERR_INVALID_ARG, "qgb_run_hmc_evolve_mixed: bad argument");
+  QGB_RC(no_domain(gf, "qgb_run_hmc_evolve_mixed"));
   const Geo g = geo_of(gf);
   const size_t b32 = gf->bytes / 2;
   void *gf32 = nullptr, *gm32 = nullptr, *tmp32 = nullptr;
@@ -1625,6 +1768,10 @@ int qgb_run_md_hooked(qgb_field* gm, qgb_field* gf, double beta, double c1, int3
   QGB_CHECK(gf->mult == 4 && gm->mult == 4 && same_geo(gf, gm) && gf->prec == gm->prec && gf != gm,
             QGB_ERR_MISMATCH, "qgb_run_md_hooked: field mismatch");
   QGB_CHECK(n_step >= 1 && reunit_interval >= 0, QGB_ERR_INVALID_ARG, "qgb_run_md_hooked: bad argument");
+  // on a domain the force-gradient shift is evaluated on the owned sites only,
+  // so its halo must be refreshed before the force that reads it
+  QGB_CHECK(!gf->dom || refresh_shifted || integrator != QGB_INTEGRATOR_FORCE_GRADIENT, QGB_ERR_INVALID_ARG,
+            "qgb_run_md_hooked: a domain field (qgb_field_set_domain) needs refresh_shifted = 1");
   const Geo g = geo_of(gf);
   void* tmp = nullptr;
   // slot 14: no entry point the hook may call (field copies, packing) uses it

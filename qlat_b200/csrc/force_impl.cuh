@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force(Geo g, ForceArgs a)
   // four times when it exceeds L2)
   if constexpr (MAP >= 2) {
     const long w = (long)(blockIdx.x >> 2) * BS + threadIdx.x;
-    if (w >= g.V) return;
+    if (w >= work_sites(g)) return;
     const long t = site_of_work(g, w, BS);
     const int mu = blockIdx.x & 3;
     M3<R> S;
@@ -581,7 +581,9 @@ cudaError_t launch_force_v(const Geo& g, ForceMode mode, const ForceArgs& a, cud
   if (MAP == 1 && !tiled) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
   const bool fast = MAP >= 2 && SPLIT == 1 && g.off == 0 && padded_sites(g.V) * 36 < 2147483647L;
   if (MAP >= 2 && !fast) return launch_force_v<R, BS, MINB, SPLIT, 0>(g, mode, a, st);
-  dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)(4 * ((g.V * SPLIT + BS - 1) / BS)), 1);
+  // the linear maps run over the owned sites of a domain only (the others are halo copies)
+  const long nw = MAP >= 2 ? work_sites(g) : g.V;
+  dim3 grid = tiled ? dim3((unsigned)(g.V / TL::sites), 1) : dim3((unsigned)(4 * ((nw * SPLIT + BS - 1) / BS)), 1);
   Geo gk = g;  // the linear maps traverse large lattices in z slabs
   if (MAP >= 2) set_slab_order(gk, BS, (int)(18 * sizeof(R)));
   const bool rect = a.c1 != 0.0;

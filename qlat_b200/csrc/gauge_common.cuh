@@ -172,11 +172,13 @@ struct LinkLd {
 };
 
 // Site of linear work index w (chunks of bs consecutive sites) in the
-// traversal order of g.zs: linear when g.zs == 0; otherwise chunk c = w / bs
+// traversal order of g: the owned box of a domain (box_site); linear when
+// g.zs == 0; otherwise chunk c = w / bs
 // is (xy chunk, z in slab, t, slab) from fastest to slowest, which needs
 // X Y % bs == 0 and Z % g.zs == 0 (set_slab_order).
 __host__ __device__ __forceinline__ long site_of_work(const Geo& g, long w, int bs)
 {
+  if (has_box(g)) return box_site(g, w);
   if (g.zs == 0) return w;
   const long xy = (long)g.d[0] * g.d[1];
   const long per_plane = xy / bs;
@@ -199,7 +201,7 @@ __host__ __device__ __forceinline__ void set_slab_order(Geo& g, int bs, int link
 {
   const long xy = (long)g.d[0] * g.d[1];
   const long slice_bytes = xy * g.d[2] * 4 * link_bytes;
-  g.zs = (g.off == 0 && g.r1 < 0 && xy % bs == 0 && g.d[2] % 16 == 0 && g.d[2] > 16 && slice_bytes > (12L << 20))
+  g.zs = (g.off == 0 && g.r1 < 0 && !has_box(g) && xy % bs == 0 && g.d[2] % 16 == 0 && g.d[2] > 16 && slice_bytes > (12L << 20))
              ? 16
              : 0;
 }

@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(128) k_rand_momentum(Geo g, RngArg ra, double 
   const bool active = s < g.V;
   Rng base, rs;
   rng_import(base, ra.v);
-  if (active) rng_split_long(rs, base, (int64_t)(s + g.rng_off));
+  if (active) rng_split_long(rs, base, (int64_t)rng_index(g, s));
   int amb = 0;
   const WField<R> Pf{P, g.V};
   // the 8 Gaussians of a link wait in shared memory (the draw index is a
@@ -823,7 +823,7 @@ __global__ void __launch_bounds__(128) k_hot_start(Geo g, RngArg ra, double s_si
   const bool active = s < g.V;
   Rng base, rs;
   rng_import(base, ra.v);
-  if (active) rng_split_long(rs, base, (int64_t)(s + g.rng_off));
+  if (active) rng_split_long(rs, base, (int64_t)rng_index(g, s));
   int amb = 0;
   hot_start_links<R>(rs, active, s_sigma, inv_sqrt3, n_step, WField<R>{U, g.V}, s, &amb);
   if (amb) atomicAdd(ambiguous, 1);
@@ -1243,4 +1243,50 @@ double rng_host_g_rand_gen(uint32_t rs[24], double center, double sigma)
   rng_export(rs, r);
   return v;
 }
+// ------------------------------------------------------------------------
+// box pack / unpack (halo exchange of a domain-decomposed field)
+
+template <typename E>
+__global__ void k_box_copy(Geo g, int K, int lo0, int lo1, int lo2, int lo3, int n0, int n1, int n2, long nbox,
+                           E* field, E* buf, bool unpack)
+{
+  const long w = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nbox) return;
+  const int c = blockIdx.y;  // component * K + entry
+  const int m = c / K, k = c - m * K;
+  long r = w;
+  const long x0 = r % n0 + lo0;
+  r /= n0;
+  const long x1 = r % n1 + lo1;
+  r /= n1;
+  const long x2 = r % n2 + lo2;
+  const long x3 = r / n2 + lo3;
+  const long s = x0 + (long)g.d[0] * (x1 + (long)g.d[1] * (x2 + (long)g.d[2] * x3));
+  const long fi = ((m * site_blocks(g.V) + (s >> 5)) * K + k) * 32 + (s & 31);
+  const long bi = (long)c * nbox + w;
+  if (unpack) field[fi] = buf[bi];
+  else buf[bi] = field[fi];
+}
+
+template <typename E>
+cudaError_t launch_box_copy(const Geo& g, int m, int K, const int lo[4], const int n[4], void* field, void* buf,
+                            bool unpack, cudaStream_t st)
+{
+  const long nbox = (long)n[0] * n[1] * n[2] * n[3];
+  if (nbox == 0) return cudaSuccess;
+  dim3 grid((unsigned)((nbox + 255) / 256), (unsigned)(m * K));
+  k_box_copy<E><<<grid, 256, 0, st>>>(g, K, lo[0], lo[1], lo[2], lo[3], n[0], n[1], n[2], nbox, (E*)field, (E*)buf,
+                                      unpack);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_box_copy<double2>(const Geo&, int, int, const int*, const int*, void*, void*, bool,
+                                              cudaStream_t);
+template cudaError_t launch_box_copy<float2>(const Geo&, int, int, const int*, const int*, void*, void*, bool,
+                                             cudaStream_t);
+template cudaError_t launch_box_copy<double>(const Geo&, int, int, const int*, const int*, void*, void*, bool,
+                                             cudaStream_t);
+template cudaError_t launch_box_copy<float>(const Geo&, int, int, const int*, const int*, void*, void*, bool,
+                                            cudaStream_t);
+
 }  // namespace qgb

@@ -26,9 +26,70 @@ struct Geo {
   // slice before the next slice, slab by slab in z, so that the time slices
   // a running grid reads stay in L2 on large lattices
   int zs = 0;
+  // one domain of a lattice decomposed over ranks in up to four directions
+  // (qgb_field_set_domain): the field holds the owned box of sites with
+  // coordinates [bl_k, bl_k + bn_k) in each direction k and a halo around it.
+  // Kernels that only need the owned sites (the force) run over the box,
+  // reductions sum over it, and the random streams of local site x are those
+  // of global site (x + go) mod gd.  bn[0] == 0: no domain.
+  int bl[4] = {0, 0, 0, 0}, bn[4] = {0, 0, 0, 0};
+  int gd[4] = {0, 0, 0, 0}, go[4] = {0, 0, 0, 0};
 };
 
-__host__ __device__ inline bool in_reduce(const Geo& g, long s) { return s >= g.r0 && (g.r1 < 0 || s < g.r1); }
+__host__ __device__ inline bool has_box(const Geo& g) { return g.bn[0] > 0; }
+
+// sites a site kernel that needs only the owned sites runs over
+__host__ __device__ inline long work_sites(const Geo& g)
+{
+  return has_box(g) ? (long)g.bn[0] * g.bn[1] * g.bn[2] * g.bn[3] : g.V;
+}
+
+// local site of the w-th owned site (x fastest) of a domain
+__host__ __device__ inline long box_site(const Geo& g, long w)
+{
+  long c = w;
+  const long x0 = c % g.bn[0] + g.bl[0];
+  c /= g.bn[0];
+  const long x1 = c % g.bn[1] + g.bl[1];
+  c /= g.bn[1];
+  const long x2 = c % g.bn[2] + g.bl[2];
+  const long x3 = c / g.bn[2] + g.bl[3];
+  return x0 + (long)g.d[0] * (x1 + (long)g.d[1] * (x2 + (long)g.d[2] * x3));
+}
+
+__host__ __device__ inline bool in_box(const Geo& g, long s)
+{
+  long c = s;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long x = k < 3 ? c % g.d[k] : c;
+    if (k < 3) c /= g.d[k];
+    if (x < g.bl[k] || x >= g.bl[k] + g.bn[k]) return false;
+  }
+  return true;
+}
+
+__host__ __device__ inline bool in_reduce(const Geo& g, long s)
+{
+  return s >= g.r0 && (g.r1 < 0 || s < g.r1) && (!has_box(g) || in_box(g, s));
+}
+
+// global index of local site s for the per-site random streams
+__host__ __device__ inline long rng_index(const Geo& g, long s)
+{
+  if (g.gd[0] == 0) return s + g.rng_off;
+  long c = s, idx = 0, mul = 1;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long x = k < 3 ? c % g.d[k] : c;
+    if (k < 3) c /= g.d[k];
+    long y = (x + g.go[k]) % g.gd[k];
+    if (y < 0) y += g.gd[k];
+    idx += y * mul;
+    mul *= g.gd[k];
+  }
+  return idx;
+}
 
 // One chain of a batch: its lattice, offset in the concatenated field and action.
 struct ChainInfo {
@@ -183,6 +244,14 @@ cudaError_t launch_store_to_aos(long Vf, long off, long n, int m, int k_per, con
 // (n counts the padded storage).
 template <typename RI, typename RO>
 cudaError_t launch_convert(long n, const void* in, void* out, cudaStream_t st);
+// Copy the sites of the box [lo_k, lo_k + n_k) of every component of a field
+// (V sites, m components of K entries of E = the entry type: a complex number
+// of a color matrix or a real) into a contiguous buffer, entry (c, w) at
+// c * nbox + w for c = component * K + entry and w the box site (x fastest),
+// or back (unpack).
+template <typename E>
+cudaError_t launch_box_copy(const Geo& g, int m, int K, const int lo[4], const int n[4], void* field, void* buf,
+                            bool unpack, cudaStream_t st);
 
 }  // namespace qgb
 
