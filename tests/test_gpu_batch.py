@@ -100,3 +100,37 @@ def test_batch_force_shapes_agree(q, precision):
     b, _ = make(q)
     best, ms = b.autotune(precision, reps=2)
     assert 0 <= best < 4 and ms > 0
+
+
+def test_batch_at_c5_size(q):
+    """The 256-chain batch of the batched-chains workload (64 each of 4^4,
+    6^4, 8^4, 12^4, Wilson, betas 5.6 .. 6.2, hot starts at scale 1, leapfrog
+    of 10 steps): one chain of each size against the same chain run alone
+    through run_hmc_pure_gauge (same decisions, delta_h, plaquette), and the
+    mixed form's per-chain plaquettes against the FP64 form's."""
+    sizes = [(L, L, L, L) for L in (4, 6, 8, 12) for _ in range(64)]
+    betas = list(np.linspace(5.6, 6.2, len(sizes)))
+    rs = [q.RngState("c5-size").split(f"chain-{c}") for c in range(len(sizes))]
+    plaqs = {}
+    for prec in ("fp64", "mixed"):
+        b = q.ChainBatch(sizes, betas)
+        b.set_rand([r.split("gf-init") for r in rs], 1.0, 1)
+        rows = []
+        for traj in (1, 2):
+            flags, dh = b.run_hmc(traj, rs, 10, precision=prec, is_always_accept=traj < 2)
+            rows.append((list(flags), np.array(dh), b.plaq()))
+        plaqs[prec] = rows[-1][2]
+        if prec != "fp64":
+            continue
+        for c in (0, 64, 128, 255):
+            gf = q.GaugeField(q.Geometry(sizes[c]))
+            gf.set_rand(rs[c].split("gf-init"), 1.0, 1)
+            ga = q.GaugeAction(betas[c], 0.0)
+            for traj in (1, 2):
+                flag, dh = q.run_hmc_pure_gauge(gf, ga, traj, rs[c], n_step=10, integrator="leapfrog",
+                                                is_always_accept=traj < 2)
+                bflags, bdh, bplaq = rows[traj - 1]
+                assert bool(bflags[c]) == bool(flag), (c, traj)
+                assert abs(bdh[c] - dh) < 1e-9 * max(1.0, np.prod(sizes[c]) / 100), (c, traj, bdh[c], dh)
+                assert abs(bplaq[c] - q.gf_avg_plaq(gf)) < 1e-12, (c, traj)
+    assert np.abs(plaqs["mixed"] - plaqs["fp64"]).max() < 2e-5
