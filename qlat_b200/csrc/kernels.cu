@@ -529,6 +529,8 @@ template <typename R>
 cudaError_t launch_clover(const Geo& g, const void* U, void* e_field, void* q_field, double* partials,
                           cudaStream_t st)
 {
+  // the grid covers every site of the field: a domain's owned-box traversal does not apply here
+  if (has_box(g)) return cudaErrorInvalidValue;
   Geo gk = g;  // z slabs on large lattices (the leaves reach one slice either way)
   set_slab_order(gk, RED_BS, (int)(18 * sizeof(R)));
   k_clover<R><<<reduce_blocks(g), RED_BS, 0, st>>>(gk, (const Cx<R>*)U, (R*)e_field, (R*)q_field, partials);
