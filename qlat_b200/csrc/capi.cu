@@ -741,12 +741,24 @@ static int flow_vjp_impl(const qgb_field* gf, double eps, double c1, int steps, 
     fa.z = zo;
     return force<R>(g, qgb::FORCE_FLOW, fa);
   };
-  auto step = [&](const void* in, void* out) -> int {  // one RK3 step in -> out, Z0..Z2 kept
-    QGB_RC(stage(in, W1, 0.25, 0.0, nullptr, Z0));
-    QGB_RC(stage(W1, W2, 8.0 / 9.0, -17.0 / 9.0, Z0, Z1));
-    QGB_RC(stage(W2, out, 0.75, -1.0, Z1, Z2));
+  // one RK3 step in -> out, keeping its stage fields w1, w2 (links after
+  // stages 1, 2) and z0, z1, z2 (the stages' Z)
+  auto step_into = [&](const void* in, void* out, void* w1, void* w2, void* z0, void* z1, void* z2) -> int {
+    QGB_RC(stage(in, w1, 0.25, 0.0, nullptr, z0));
+    QGB_RC(stage(w1, w2, 8.0 / 9.0, -17.0 / 9.0, z0, z1));
+    QGB_RC(stage(w2, out, 0.75, -1.0, z1, z2));
     return QGB_OK;
   };
+  auto step = [&](const void* in, void* out) -> int { return step_into(in, out, W1, W2, Z0, Z1, Z2); };
+  // When the five stage fields of every step of a segment fit in 4 GiB, the
+  // segment's recomputation keeps them, and the pull-back reads them instead
+  // of recomputing each step a second time.
+  const bool keep = (size_t)5 * every * bytes <= ((size_t)4 << 30);
+  std::vector<void*> kept;
+  if (keep) {
+    kept.resize((size_t)5 * every);
+    for (int i = 0; i < 5 * every; ++i) QGB_RC(get_scratch(bytes, 2000 + i, &kept[i]));
+  }
   // forward pass: checkpoints
   QGB_TRY_CUDA(cudaMemcpyAsync(cps[0], gf->d, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
   for (int c = 1; c < ncp; ++c) {
@@ -762,19 +774,38 @@ static int flow_vjp_impl(const qgb_field* gf, double eps, double c1, int steps, 
   for (int c = ncp - 1; c >= 0; --c) {
     const int s0 = c * every, s1 = (s0 + every < steps) ? s0 + every : steps;
     QGB_TRY_CUDA(cudaMemcpyAsync(wst[0], cps[c], bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
-    for (int j = 1; j < s1 - s0; ++j) QGB_RC(step(wst[j - 1], wst[j]));
-    for (int j = s1 - s0 - 1; j >= 0; --j) {
-      QGB_RC(step(wst[j], Wx));  // stage fields of this step: wst[j], W1, W2 and Z0, Z1, Z2
+    const int n = s1 - s0;
+    if (keep) {
+      for (int j = 0; j < n; ++j) {
+        void** k = &kept[(size_t)5 * j];
+        QGB_RC(step_into(wst[j], j + 1 < n ? wst[j + 1] : Wx, k[0], k[1], k[2], k[3], k[4]));
+      }
+    } else {
+      for (int j = 1; j < n; ++j) QGB_RC(step(wst[j - 1], wst[j]));
+    }
+    for (int j = n - 1; j >= 0; --j) {
+      // stage fields of this step: wst[j], w1, w2 and z0, z1, z2
+      const void *w1 = W1, *w2 = W2, *z0 = Z0, *z1 = Z1, *z2 = Z2;
+      if (keep) {
+        void** k = &kept[(size_t)5 * j];
+        w1 = k[0];
+        w2 = k[1];
+        z0 = k[2];
+        z1 = k[3];
+        z2 = k[4];
+      } else {
+        QGB_RC(step(wst[j], Wx));
+      }
       {
         Prof p("flow_adjoint", 6);
         // stage 3: W3 = exp(eps Z2) W2, Z2 = 3/4 F(W2) - Z1
-        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z2, nullptr, 0.0, eps, mua, laml, g_ctx.stream));
-        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W2, mua, laml, lam, 3.0, c1, 0.75, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, z2, nullptr, 0.0, eps, mua, laml, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, w2, mua, laml, lam, 3.0, c1, 0.75, g_ctx.stream));
         // stage 2: W2 = exp(eps Z1) W1, Z1 = 8/9 F(W1) - 17/9 Z0; carry -mu2 into Z1
-        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z1, mua, -1.0, eps, mub, laml, g_ctx.stream));
-        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, W1, mub, laml, lam, 3.0, c1, 8.0 / 9.0, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, z1, mua, -1.0, eps, mub, laml, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, w1, mub, laml, lam, 3.0, c1, 8.0 / 9.0, g_ctx.stream));
         // stage 1: W1 = exp(eps Z0) W0, Z0 = 1/4 F(W0); carry -17/9 mu1 into Z0
-        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, Z0, mub, -17.0 / 9.0, eps, mua, laml, g_ctx.stream));
+        QGB_TRY_CUDA(qgb::launch_flow_adj_local<R>(g.V, lam, z0, mub, -17.0 / 9.0, eps, mua, laml, g_ctx.stream));
         QGB_TRY_CUDA(qgb::launch_force_vjp<R>(g, wst[j], mua, laml, lam, 3.0, c1, 0.25, g_ctx.stream));
       }
     }
