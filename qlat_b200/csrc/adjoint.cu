@@ -105,6 +105,47 @@ __device__ __forceinline__ void dual_acc(M3<R>& S, M3<R>& dS, R w, const Dual<R>
   axpy(dS, w, P.d);
 }
 
+// The staple sums S and dS of a thread, kept in shared memory (entry k at
+// [k][threadIdx.x]) while its paths are walked: the dual matrices of a path
+// then have the registers to themselves.
+template <typename R>
+struct SmemAcc {
+  Cx<R> (*s)[128];
+  Cx<R> (*ds)[128];
+  __device__ __forceinline__ void zero()
+  {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s[k][threadIdx.x] = ds[k][threadIdx.x] = cx<R>(R(0), R(0));
+  }
+  __device__ __forceinline__ void add(R w, const Dual<R>& P)
+  {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      Cx<R> a = s[k][threadIdx.x], b = ds[k][threadIdx.x];
+      a.re = fma(w, P.v.e[k].re, a.re);
+      a.im = fma(w, P.v.e[k].im, a.im);
+      b.re = fma(w, P.d.e[k].re, b.re);
+      b.im = fma(w, P.d.e[k].im, b.im);
+      s[k][threadIdx.x] = a;
+      ds[k][threadIdx.x] = b;
+    }
+  }
+  __device__ __forceinline__ M3<R> S() const
+  {
+    M3<R> m;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m.e[k] = s[k][threadIdx.x];
+    return m;
+  }
+  __device__ __forceinline__ M3<R> dS() const
+  {
+    M3<R> m;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m.e[k] = ds[k][threadIdx.x];
+    return m;
+  }
+};
+
 // lambda_out = lambda_local + a (DF[Y] + [F, Y]) at every link, F the force
 // of GaugeAction(beta, c1) (hmc.cpp:48-75: staples (1 - 8 c1) plaq + c1 rect,
 // the paths of hmc.cpp:27-46), DF[Y] its derivative along Y, every path
@@ -119,30 +160,33 @@ __global__ void __launch_bounds__(128) k_force_vjp(Geo g, const Cx<R>* Up, const
   const CField<R> U{Up, g.V}, Y{Yp, g.V};
   const Coord x = coord_of(g, s);
   const R cp = R(1.0 - 8.0 * c1), cr = R(c1);
-  M3<R> S = m3_zero<R>(), dS = m3_zero<R>();
+  __shared__ Cx<R> sh_s[9][128], sh_ds[9][128];
+  SmemAcc<R> acc{sh_s, sh_ds};
+  acc.zero();
 #pragma unroll 1
   for (int k = 0; k < 6; ++k) {
     const DualDir<R> d{U, Y, g, x, mu, (mu + 1 + (k >> 1)) & 3, (k & 1) ? -1 : 1};
     // plaq (nu, mu, -nu) = hop(x) U_mu(x+e) back(x+e+mu)
-    dual_acc(S, dS, cp, dmul(dmul(d.hop(0, 0), d.umu(0, 1)), d.back(1, 1)));
+    acc.add(cp, dmul(dmul(d.hop(0, 0), d.umu(0, 1)), d.back(1, 1)));
     if (RECT) {
       // rect1 (nu, nu, mu, -nu, -nu)
       Dual<R> C = dmul(d.hop(0, 0), d.hop(0, 1));
       C = dmul(C, d.umu(0, 2));
       C = dmul(C, d.back(1, 2));
-      dual_acc(S, dS, cr, dmul(C, d.back(1, 1)));
+      acc.add(cr, dmul(C, d.back(1, 1)));
       // rect2 (nu, mu, mu, -nu, -mu)
       C = dmul(d.hop(0, 0), d.umu(0, 1));
       C = dmul(C, d.umu(1, 1));
       C = dmul(C, d.back(2, 1));
-      dual_acc(S, dS, cr, dmul(C, d.umu(1, 0, true)));
+      acc.add(cr, dmul(C, d.umu(1, 0, true)));
       // rect3 (-mu, nu, mu, mu, -nu)
       C = dmul(d.umu(-1, 0, true), d.hop(-1, 0));
       C = dmul(C, d.umu(-1, 1));
       C = dmul(C, d.umu(0, 1));
-      dual_acc(S, dS, cr, dmul(C, d.back(1, 1)));
+      acc.add(cr, dmul(C, d.back(1, 1)));
     }
   }
+  const M3<R> S = acc.S(), dS = acc.dS();
   const M3<R> u = U.ld(s, mu);
   const M3<R> y = Y.ld(s, mu);
   const M3<R> du = mul(y, u);
