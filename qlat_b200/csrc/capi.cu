@@ -714,7 +714,7 @@ static int flow_step(qgb_field* gf, double eps, double c1, bool rk3)
 // recomputed with their Z fields, then pulled back stage by stage.
 template <typename R>
 static int flow_vjp_impl(const qgb_field* gf, double eps, double c1, int steps, int every, const void* lam_in,
-                         void* grad)
+                         void* grad, bool cps_ready = false)
 {
   const Geo g = geo_of(gf);
   const size_t bytes = gf->bytes;
@@ -759,9 +759,11 @@ static int flow_vjp_impl(const qgb_field* gf, double eps, double c1, int steps, 
     kept.resize((size_t)5 * every);
     for (int i = 0; i < 5 * every; ++i) QGB_RC(get_scratch(bytes, 2000 + i, &kept[i]));
   }
-  // forward pass: checkpoints
-  QGB_TRY_CUDA(cudaMemcpyAsync(cps[0], gf->d, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
-  for (int c = 1; c < ncp; ++c) {
+  // forward pass: checkpoints (the states after 0, every, 2 every, ... steps
+  // in the scratch buffers 100 + c; cps_ready: the caller's forward flow
+  // already left them there)
+  if (!cps_ready) QGB_TRY_CUDA(cudaMemcpyAsync(cps[0], gf->d, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  for (int c = 1; c < ncp && !cps_ready; ++c) {
     QGB_TRY_CUDA(cudaMemcpyAsync(Wx, cps[c - 1], bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
     for (int j = 0; j < every; ++j) {
       QGB_RC(step(Wx, wst[0]));
@@ -1971,11 +1973,21 @@ int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, 
   void *V = nullptr, *lamN = nullptr;
   QGB_RC(get_scratch(gf->bytes, 61, &V));
   QGB_RC(get_scratch(gf->bytes, 62, &lamN));
-  // flowed field V_t
+  // flowed field V_t, keeping the adjoint's checkpoints on the way (the
+  // states after 0, every, 2 every, ... steps, in the scratch buffers that
+  // flow_vjp_impl reads)
+  const int every = steps > 0 ? (checkpoint_every < steps ? checkpoint_every : steps) : 1;
   QGB_TRY_CUDA(cudaMemcpyAsync(V, gf->d, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
   qgb_field_s fv = *gf;
   fv.d = V;
-  for (int i = 0; i < steps; ++i) QGB_RC(flow_step(&fv, epsilon, c1, true));
+  for (int i = 0; i < steps; ++i) {
+    if (i % every == 0) {
+      void* cp = nullptr;
+      QGB_RC(get_scratch(gf->bytes, 100 + i / every, &cp));
+      QGB_TRY_CUDA(cudaMemcpyAsync(cp, fv.d, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    }
+    QGB_RC(flow_step(&fv, epsilon, c1, true));
+  }
   V = fv.d;  // flow_step hands the result buffer to the handle
   // loss and its gradient at V_t: dL = -2 <F(V_t), X> in the su(3) pairing
   QGB_RC(action_slot(&fv, c1_loss != 0.0, 0));
@@ -1995,9 +2007,8 @@ int qgb_gf_flow_action_grad(const qgb_field* gf, double epsilon, int32_t steps, 
     QGB_TRY_CUDA(cudaMemcpyAsync(grad->d, lamN, gf->bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
     return QGB_OK;
   }
-  const int every = checkpoint_every < steps ? checkpoint_every : steps;
-  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, c1, steps, every, lamN, grad->d);
-  return flow_vjp_impl<float>(gf, epsilon, c1, steps, every, lamN, grad->d);
+  if (gf->prec == QGB_F64) return flow_vjp_impl<double>(gf, epsilon, c1, steps, every, lamN, grad->d, true);
+  return flow_vjp_impl<float>(gf, epsilon, c1, steps, every, lamN, grad->d, true);
 }
 
 int qgb_set_anti_hermitian_matrix_from_basis(qgb_field* fc, const qgb_field* basis)
