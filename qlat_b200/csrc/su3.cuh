@@ -634,73 +634,79 @@ static __constant__ float qgb_inv_nf[21] = {0.0f,       1.0f / 1,  1.0f / 2,  1.
                                             1.0f / 18,  1.0f / 19, 1.0f / 20};
 #endif
 
-// exp(a) of an su(3) matrix (anti-hermitian, traceless) in FP32: the same
-// polynomial as exp_ch (the reference's order-20 Taylor polynomial, cut at
-// FP32 resolution), with the structure of su(3) used in the Cayley-Hamilton
-// coefficients: t = tr a = 0, s = -tr(a^2)/2 is real, d = det a = tr(a^3)/3
-// is imaginary (i delta), and a^2 is hermitian, so
+// exp(a) of an su(3) matrix (anti-hermitian, traceless): the same polynomial
+// as exp_ch (the reference's order-20 Taylor polynomial), with the structure
+// of su(3) used in the Cayley-Hamilton coefficients: t = tr a = 0,
+// s = -tr(a^2)/2 is real, d = det a = tr(a^3)/3 is imaginary (i delta), and
+// a^2 is hermitian, so
 //   - a^2 needs its real diagonal and upper triangle (half a product),
 //   - delta = Im tr(a^3)/3 = Im sum_ij (a^2)_ij a_ji replaces the cofactor
 //     determinant,
 //   - a recursion step (x, y, z) <- ((i delta z), x - s z, y) / n costs real
 //     multiplies instead of complex ones,
 //   - the Frobenius norm is sqrt(2 s).
-// The fused molecular-dynamics and flow epilogues of the FP32 force call it:
-// their arguments (momenta, TA-projected forces, flow combinations of them)
-// are in su(3) up to FP32 rounding, and that rounding-size remainder is what
-// the specialisation drops.
-QGB_HD M3<float> exp_su3(const M3<float>& a)
+// The recursion stops once the omitted Taylor terms are bounded (Frobenius
+// norm, sum_{k>n} |a|^k / k! <= 2 |a|^(n+1) / (n+1)! when |a| < (n+2)/2) below
+// the type's resolution: 2^-27 in FP32, 2^-56 in FP64 -- the 20-term
+// polynomial to rounding, in fewer steps for small arguments (a large |a|
+// still runs all 20).  The fused molecular-dynamics and flow epilogues of the
+// force call it: their arguments (momenta, TA-projected forces, flow
+// combinations of them) are in su(3) up to rounding, and that rounding-size
+// remainder is what the specialisation drops.
+template <typename R>
+QGB_HD M3<R> exp_su3(const M3<R>& a)
 {
   // (a^2)_ii (real) and (a^2)_ij, i < j
-  float h[3];
+  R h[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    float v = 0.f;
+    R v = R(0);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) v = fmaf(a.e[3 * i + k].re, a.e[3 * k + i].re, fmaf(-a.e[3 * i + k].im, a.e[3 * k + i].im, v));
+    for (int k = 0; k < 3; ++k) v = fma(a.e[3 * i + k].re, a.e[3 * k + i].re, fma(-a.e[3 * i + k].im, a.e[3 * k + i].im, v));
     h[i] = v;
   }
-  Cx<float> u[3];  // (0,1), (0,2), (1,2)
+  Cx<R> u[3];  // (0,1), (0,2), (1,2)
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     const int i = q == 2 ? 1 : 0, j = q == 0 ? 1 : 2;
-    float re = 0.f, im = 0.f;
+    R re = R(0), im = R(0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      re = fmaf(a.e[3 * i + k].re, a.e[3 * k + j].re, fmaf(-a.e[3 * i + k].im, a.e[3 * k + j].im, re));
-      im = fmaf(a.e[3 * i + k].re, a.e[3 * k + j].im, fmaf(a.e[3 * i + k].im, a.e[3 * k + j].re, im));
+      re = fma(a.e[3 * i + k].re, a.e[3 * k + j].re, fma(-a.e[3 * i + k].im, a.e[3 * k + j].im, re));
+      im = fma(a.e[3 * i + k].re, a.e[3 * k + j].im, fma(a.e[3 * i + k].im, a.e[3 * k + j].re, im));
     }
-    u[q] = cx<float>(re, im);
+    u[q] = cx<R>(re, im);
   }
-  const float s = -0.5f * (h[0] + h[1] + h[2]);
+  const R s = R(-0.5) * (h[0] + h[1] + h[2]);
   // Im tr(a^3) = sum_i (a^2)_ii Im a_ii + sum_{i<j} Im[(a^2)_ij a_ji + conj((a^2)_ij) a_ij]
-  float t3 = h[0] * a.e[0].im;
-  t3 = fmaf(h[1], a.e[4].im, t3);
-  t3 = fmaf(h[2], a.e[8].im, t3);
+  R t3 = h[0] * a.e[0].im;
+  t3 = fma(h[1], a.e[4].im, t3);
+  t3 = fma(h[2], a.e[8].im, t3);
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     const int i = q == 2 ? 1 : 0, j = q == 0 ? 1 : 2;
-    const Cx<float> aij = a.e[3 * i + j], aji = a.e[3 * j + i];
-    t3 = fmaf(u[q].re, aji.im + aij.im, t3);
-    t3 = fmaf(u[q].im, aji.re - aij.re, t3);
+    const Cx<R> aij = a.e[3 * i + j], aji = a.e[3 * j + i];
+    t3 = fma(u[q].re, aji.im + aij.im, t3);
+    t3 = fma(u[q].im, aji.re - aij.re, t3);
   }
-  const float delta = t3 * (1.0f / 3.0f);
-  const float nrm = sqrtf(fmaxf(2.f * s, 0.f));
+  const R delta = t3 * (R(1) / R(3));
+  const R nrm = sqrt(fmax(R(2) * s, R(0)));
+  const R tol = sizeof(R) == 4 ? R(7.450580596923828e-9) : R(1.3877787807814457e-17);
   // (x, y, z)_n: a^n / n! = x 1 + y a + z a^2; f = sum_n (x, y, z)_n
-  Cx<float> x = cx<float>(1.f, 0.f), y = cx<float>(0.f, 0.f), z = cx<float>(0.f, 0.f);
-  Cx<float> f0 = x, f1 = y, f2 = z;
-  float term = 1.f;  // |a|^n / n!
+  Cx<R> x = cx<R>(R(1), R(0)), y = cx<R>(R(0), R(0)), z = cx<R>(R(0), R(0));
+  Cx<R> f0 = x, f1 = y, f2 = z;
+  R term = R(1);  // |a|^n / n!
 #pragma unroll 1
   for (int n = 1; n <= 20; ++n) {
 #if defined(__CUDA_ARCH__)
-    const float inv = qgb_inv_nf[n];
+    const R inv = sizeof(R) == 4 ? R(qgb_inv_nf[n]) : R(qgb_inv_n[n]);
 #else
-    const float inv = 1.0f / (float)n;
+    const R inv = R(1) / R(n);
 #endif
-    const float di = delta * inv;
-    const Cx<float> xn = cx<float>(-di * z.im, di * z.re);
-    const Cx<float> yn = cx<float>(fmaf(-s, z.re, x.re) * inv, fmaf(-s, z.im, x.im) * inv);
-    z = cx<float>(y.re * inv, y.im * inv);
+    const R di = delta * inv;
+    const Cx<R> xn = cx<R>(-di * z.im, di * z.re);
+    const Cx<R> yn = cx<R>(fma(-s, z.re, x.re) * inv, fma(-s, z.im, x.im) * inv);
+    z = cx<R>(y.re * inv, y.im * inv);
     x = xn;
     y = yn;
     f0.re += x.re;
@@ -709,39 +715,36 @@ QGB_HD M3<float> exp_su3(const M3<float>& a)
     f1.im += y.im;
     f2.re += z.re;
     f2.im += z.im;
-    // the stopping rule of exp_ch: remainder below 2^-27 in the Frobenius norm
     term *= nrm * inv;
-    if (2.f * term * nrm < 7.450580596923828e-9f * (float)(n + 1) && nrm < 0.5f * (float)(n + 2)) break;
+    if (R(2) * term * nrm < tol * R(n + 1) && nrm < R(0.5) * R(n + 2)) break;
   }
   // r = f0 1 + f1 a + f2 a^2, with (a^2)_ji = conj((a^2)_ij)
-  M3<float> r;
+  M3<R> r;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      Cx<float> q2;
-      if (i == j) q2 = cx<float>(h[i], 0.f);
+      Cx<R> q2;
+      if (i == j) q2 = cx<R>(h[i], R(0));
       else if (i < j) q2 = u[i + j - 1];
-      else q2 = cx<float>(u[i + j - 1].re, -u[i + j - 1].im);
-      const Cx<float> ae = a.e[3 * i + j];
-      float re = fmaf(f1.re, ae.re, fmaf(-f1.im, ae.im, fmaf(f2.re, q2.re, -f2.im * q2.im)));
-      float im = fmaf(f1.re, ae.im, fmaf(f1.im, ae.re, fmaf(f2.re, q2.im, f2.im * q2.re)));
+      else q2 = cx<R>(u[i + j - 1].re, -u[i + j - 1].im);
+      const Cx<R> ae = a.e[3 * i + j];
+      R re = fma(f1.re, ae.re, fma(-f1.im, ae.im, fma(f2.re, q2.re, -f2.im * q2.im)));
+      R im = fma(f1.re, ae.im, fma(f1.im, ae.re, fma(f2.re, q2.im, f2.im * q2.re)));
       if (i == j) {
         re += f0.re;
         im += f0.im;
       }
-      r.e[3 * i + j] = cx<float>(re, im);
+      r.e[3 * i + j] = cx<R>(re, im);
     }
   return r;
 }
 
-// The exponential of the fused epilogues: exp_su3 in FP32, exp_ch (the
-// reference's 20 terms, any matrix) in FP64.
+// The exponential of the fused epilogues (both precisions).
 template <typename R>
 QGB_HD M3<R> exp_md(const M3<R>& a)
 {
-  if constexpr (sizeof(R) == 4) return exp_su3(a);
-  else return exp_ch(a);
+  return exp_su3(a);
 }
 
 }  // namespace qgb
