@@ -456,6 +456,67 @@ def slabs(q, args):
 
 
 
+def domains(q, args):
+    """The same chain as `slabs`, held as one rank's domain with the directions
+    of --cut cut (halo of --halo sites on either side, each refreshed from the
+    rank's own opposite face before every force evaluation) against the plain
+    single-GPU form.  The domain's force runs on the owned sites only, so what
+    it adds is the exchanges (four faces per cut direction and force
+    evaluation, stopping the stream each time) and the element-wise kernels'
+    sweep over the halo -- what a decomposed run adds besides the network."""
+    import torch
+    ts = _lattice(args.lattice)
+    cut = tuple(bool(int(c)) for c in args.cut.split(","))
+    ga = q.GaugeAction(2.13, -0.331)
+    rs = q.RngState("b200-domains-bench")
+    gf = q.GaugeField(q.Geometry(ts))
+    gf.set_rand(rs.split("gf-init"), 0.3, 1)
+    for prec in (q.F64, q.F32):
+        q.autotune_force(gf.copy(precision=prec), ga.c1())
+    dom = q.Domains(ts, (1, 1, 1, 1), halo=args.halo, cut=cut)
+    local = 1
+    for v in dom.dims:
+        local *= v
+    out = {"lattice": list(ts), "precision": args.precision, "n_step": args.n_step, "halo": args.halo,
+           "cut": list(cut), "local_extents": list(dom.dims), "local_over_owned_sites": local / dom.total_volume}
+    dhs = {}
+    for form in ("plain", "domain"):
+        if form == "plain":
+            g = gf.copy()
+            step = lambda t: q.run_hmc_pure_gauge(g, ga, t, rs, n_step=args.n_step, is_always_accept=True,
+                                                  precision=args.precision)
+        else:
+            g = dom.gauge_field()
+            dom.set_rand(g, rs.split("gf-init"), 0.3, 1)
+            step = lambda t: q.run_hmc_pure_gauge_domains(dom, g, ga, t, rs, n_step=args.n_step,
+                                                          is_always_accept=True, precision=args.precision)
+        for t in range(1, args.warmup + 1):
+            step(t)
+        torch.cuda.synchronize()
+        ms, dh = [], []
+        for t in range(args.warmup + 1, args.warmup + 1 + args.trajs):
+            t0 = time.perf_counter()
+            dh.append(step(t)[1])
+            torch.cuda.synchronize()
+            ms.append(round((time.perf_counter() - t0) * 1e3, 2))
+        out[form + "_ms_per_traj"] = ms
+        out[form + "_traj_per_s"] = 1e3 * len(ms) / sum(ms)
+        dhs[form] = dh
+    out["domain_over_plain"] = out["domain_traj_per_s"] / out["plain_traj_per_s"]
+    out["max_delta_h_difference"] = max(abs(a - b) for a, b in zip(dhs["plain"], dhs["domain"]))
+    g32 = dom.gauge_field().copy(precision=q.F32 if args.precision == "mixed" else q.F64)
+    for _ in range(3):
+        dom.exchange(g32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(20):
+        dom.exchange(g32)
+    torch.cuda.synchronize()
+    out["exchange_ms"] = (time.perf_counter() - t0) / 20 * 1e3
+    out["exchanges_per_traj"] = 4 * args.n_step + 2
+    return out
+
+
 # ---------------------------------------------------------------------------
 # small cases for ncu
 
@@ -526,6 +587,14 @@ def main():
     sl.add_argument("--warmup", type=int, default=2)
     sl.add_argument("--order", default="plain,slab")
     sl.add_argument("--halo", type=int, default=4)
+    dm = sub.add_parser("domains")
+    dm.add_argument("--lattice", default="24,24,24,64")
+    dm.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    dm.add_argument("--n-step", type=int, default=8)
+    dm.add_argument("--trajs", type=int, default=5)
+    dm.add_argument("--warmup", type=int, default=2)
+    dm.add_argument("--halo", type=int, default=2)
+    dm.add_argument("--cut", default="1,1,1,1", help="per direction: 1 = cut (halo exchanged with itself)")
     fn = sub.add_parser("functions")
     fn.add_argument("set", choices=["hmc", "flow"])
     fn.add_argument("--reps", type=int, default=20)
@@ -555,6 +624,8 @@ def main():
         res = legs[args.cmd](q)
     elif args.cmd == "slabs":
         res = slabs(q, args)
+    elif args.cmd == "domains":
+        res = domains(q, args)
     elif args.cmd == "functions":
         res = functions(q, args.set, args.reps)
     else:

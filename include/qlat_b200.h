@@ -558,10 +558,11 @@ int qgb_field_unpack_tslices(qgb_field* f, int32_t t0, int32_t nt, const void* d
  *  - the _node sums (gm_hamilton_node, gf_hamilton_node, the _sites action
  *    sums) are over the owned sites, as the reference's node sums are over
  *    its node's sites;
- *  - the per-site random streams (set_rand_gauge_momentum, set_rand) are
- *    those of each local site's global index, so the owned sites draw what a
- *    single field of the whole lattice draws (and the halo sites what their
- *    owners draw);
+ *  - the per-site random streams are those of each local site's global
+ *    index, so the owned sites draw what a single field of the whole lattice
+ *    draws: set_rand draws every local site (the halo sites what their owners
+ *    draw), set_rand_gauge_momentum the owned sites only (halo momenta are set
+ *    to zero: no force or sum reads them);
  *  - element-wise operations run on every local site;
  *  - qgb_run_md_hooked with the force-gradient integrator needs
  *    refresh_shifted = 1 (the shifted field, too, is evaluated on the owned

@@ -744,14 +744,20 @@ __global__ void __launch_bounds__(128) k_rand_momentum(Geo g, RngArg ra, double 
                                                        Cx<R>* P, int* ambiguous)
 {
   // every lane of the warp stays to the end (warp-wide refills); lanes past
-  // the last site draw nothing
+  // the last site draw nothing, and so do the halo sites of a domain, whose
+  // momenta no force or sum reads (they are set to zero)
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = s < g.V;
+  const bool inside = s < g.V;
+  const bool active = inside && (!has_box(g) || in_box(g, s));
   Rng base, rs;
   rng_import(base, ra.v);
   if (active) rng_split_long(rs, base, (int64_t)rng_index(g, s));
   int amb = 0;
   const WField<R> Pf{P, g.V};
+  if (inside && !active) {
+#pragma unroll 1
+    for (int mu = 0; mu < 4; ++mu) Pf.st(s, mu, m3_zero<R>());
+  }
   // the 8 Gaussians of a link wait in shared memory (the draw index is a
   // run-time value; a per-thread array would live in local memory)
   __shared__ double sb[8 * 128];

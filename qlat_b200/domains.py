@@ -13,8 +13,9 @@ qgb_field_set_domain, so that the library
 
 - evaluates the force on the owned sites only (no work on halo sites),
 - sums the _node Hamiltonians over the owned sites,
-- draws every local site's momenta and hot-start links from the random stream
-  of its global site (the halo sites draw what their owners draw);
+- draws the owned sites' momenta, and every local site's hot-start links, from
+  the random stream of the site's global index (halo momenta are zero: no
+  force or sum reads them);
 
 and the molecular dynamics is the library's own kernel sequence
 (qgb_run_md_hooked), which calls back into ``exchange`` before every force
@@ -54,15 +55,18 @@ def index_from_coordinate(coor, size) -> int:
     return idx
 
 
-def domain_layout(total_site, size_node, rank: int, halo: int = 2):
+def domain_layout(total_site, size_node, rank: int, halo: int = 2, cut=None):
     """The domain of rank ``rank`` on the grid ``size_node``: a dict with the
     local field extents, the global origin of its owned sites, the halo depth
     per direction, the owned extents and the neighbouring ranks (down, up) per
-    direction."""
+    direction.  A direction is cut (carries a halo) when it has more than one
+    rank or when ``cut[k]`` is true; a cut direction with one rank exchanges
+    with itself (its halo is its own periodic copy)."""
     total_site = tuple(int(v) for v in total_site)
     size_node = tuple(int(v) for v in size_node)
     if len(total_site) != 4 or len(size_node) != 4 or min(size_node) < 1:
         raise ValueError("domain_layout: total_site and size_node need four positive entries")
+    cut = tuple(bool(c) for c in cut) if cut is not None else (False,) * 4
     coor = coordinate_from_index(rank, size_node)
     owned, halos, dims, origin, nbr = [], [], [], [], []
     for k in range(4):
@@ -70,7 +74,7 @@ def domain_layout(total_site, size_node, rank: int, halo: int = 2):
         if G % R:
             raise ValueError(f"domain_layout: extent {G} in direction {k} is not divisible by {R} ranks")
         n = G // R
-        h = halo if R > 1 else 0
+        h = halo if (R > 1 or cut[k]) else 0
         if h > n:
             raise ValueError(f"domain_layout: {n} owned sites in direction {k}, fewer than the halo depth {h}")
         owned.append(n)
@@ -90,7 +94,7 @@ class Domains:
     """The domain of this rank of ``total_site`` cut over a ``size_node`` grid
     of ranks (the product of size_node must be the group's size)."""
 
-    def __init__(self, total_site, size_node, *, halo: int = 2, group=None):
+    def __init__(self, total_site, size_node, *, halo: int = 2, cut=None, group=None):
         import torch.distributed as dist
         self._dist = dist if dist.is_available() and dist.is_initialized() else None
         self.group = group
@@ -102,7 +106,7 @@ class Domains:
             n *= v
         if n != self.world:
             raise ValueError(f"Domains: a {size_node} grid needs {n} ranks, the group has {self.world}")
-        lay = domain_layout(total_site, size_node, self.rank, halo)
+        lay = domain_layout(total_site, size_node, self.rank, halo, cut)
         self.total_site = tuple(int(v) for v in total_site)
         self.total_volume = 1
         for v in self.total_site:
@@ -176,11 +180,32 @@ class Domains:
             if self.halo[k] == 0:
                 continue
             send_dn, send_up, halo_lo, halo_hi = self.faces(k)
+            if self._self_exchange(k):
+                self._copy_faces(handle, k)
+                continue
             up = self._pack(handle, send_up, ("send_up", k))
             dn = self._pack(handle, send_dn, ("send_dn", k))
             rlo, rhi = self._swap(k, up, dn)
             self._unpack(handle, halo_lo, rlo)
             self._unpack(handle, halo_hi, rhi)
+
+    def _self_exchange(self, k: int) -> bool:
+        """Direction k is cut but has one rank: its halo is its own periodic copy."""
+        dn, up = self.neighbours[k]
+        return self.world == 1 or (dn == self.rank and up == self.rank)
+
+    def _copy_faces(self, handle, k: int) -> None:
+        """The self-exchange of direction k, queued on the library stream
+        without waiting: each face packed into a device buffer and unpacked
+        into the opposite halo, in stream order."""
+        i4 = ctypes.c_int32 * 4
+        send_dn, send_up, halo_lo, halo_hi = self.faces(k)
+        for src, dst, key in ((send_up, halo_lo, "face_up"), (send_dn, halo_hi, "face_dn")):
+            nb = ctypes.c_int64()
+            call("qgb_field_box_bytes", handle, i4(*src[1]), ctypes.byref(nb))
+            buf = self._buffer((key, k), nb.value, "cuda")
+            call("qgb_field_pack_box", handle, i4(*src[0]), i4(*src[1]), ctypes.c_void_p(buf.data_ptr()))
+            call("qgb_field_unpack_box", handle, i4(*dst[0]), i4(*dst[1]), ctypes.c_void_p(buf.data_ptr()))
 
     def _pack(self, handle, box, key):
         """The sites of ``box`` of the field as a message: a device buffer over
@@ -193,7 +218,8 @@ class Domains:
         buf = self._buffer(key, nb.value, "cuda")
         call("qgb_field_pack_box", handle, i4(*lo), i4(*n), ctypes.c_void_p(buf.data_ptr()))
         synchronize()
-        return buf if self.backend == "nccl" else buf.cpu()
+        # one rank exchanges with itself: the message stays on the device
+        return buf if (self.backend == "nccl" or self.world == 1) else buf.cpu()
 
     def _unpack(self, handle, box, msg) -> None:
         import torch

@@ -72,7 +72,39 @@ def _numpy_domains_cls():
             handle[lo[3]:lo[3] + n[3], lo[2]:lo[2] + n[2], lo[1]:lo[1] + n[1], lo[0]:lo[0] + n[0]] = \
                 msg.numpy().reshape(n[3], n[2], n[1], n[0])
 
+        def _self_exchange(self, k):
+            return False  # the self-exchange, too, through the message path above
+
     return NumpyDomains
+
+
+def _fill_and_exchange(d):
+    """A local array with its global site index on owned sites and -1 in the
+    halo, exchanged; returns (array, the global index every local site should
+    hold)."""
+    X, Y, Z, T = d.dims
+    a = np.full((T, Z, Y, X), -1.0)
+    h, n, o, G = d.halo, d.owned, d.origin, d.total_site
+    gx = (np.arange(X) - h[0] + o[0]) % G[0]
+    gy = (np.arange(Y) - h[1] + o[1]) % G[1]
+    gz = (np.arange(Z) - h[2] + o[2]) % G[2]
+    gt = (np.arange(T) - h[3] + o[3]) % G[3]
+    want = gx[None, None, None, :] + G[0] * (gy[None, None, :, None] + G[1] * (
+        gz[None, :, None, None] + G[2] * gt[:, None, None, None]))
+    own = (slice(h[3], h[3] + n[3]), slice(h[2], h[2] + n[2]), slice(h[1], h[1] + n[1]), slice(h[0], h[0] + n[0]))
+    a[own] = want[own]
+    d._exchange_handle(a)
+    return a, want
+
+
+def test_one_rank_with_every_direction_cut_exchanges_with_itself():
+    """One rank, all four directions cut: every halo site, edges and corners
+    included, ends up with its periodic image's value."""
+    sys.path.insert(0, ROOT)
+    d = _numpy_domains_cls()((6, 4, 4, 8), (1, 1, 1, 1), halo=2, cut=(1, 1, 1, 1))
+    assert d.dims == (10, 8, 8, 12) and d.halo == (2, 2, 2, 2)
+    a, want = _fill_and_exchange(d)
+    assert (a == want).all()
 
 
 def _exchange_main(rank, world, port, out_dir):
@@ -183,9 +215,15 @@ def _compare(rows, ref_rows, links, ref_links, origin, owned):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_one_rank_domain_matches_global(q, precision):
-    dom = q.Domains(TS, (1, 1, 1, 1))
+@pytest.mark.parametrize("precision,cut", [("fp64", None), ("mixed", None), ("fp64", (1, 1, 1, 1)),
+                                           ("mixed", (1, 1, 1, 1))])
+def test_one_rank_domain_matches_global(q, precision, cut):
+    """One rank: nothing cut (the owned box is the whole field), or every
+    direction cut with halos of 2 refreshed from the rank's own faces (the
+    force on the owned box only, four face exchanges per direction and force
+    evaluation, edge halo sites filled through the direction exchanged
+    second) -- against the whole-lattice chain."""
+    dom = q.Domains(TS, (1, 1, 1, 1), cut=cut)
     rows, links = _domain_run(q, dom, precision)
     ref_rows, ref_links = _global_run(q, precision)
     _compare(rows, ref_rows, links, ref_links, dom.origin, dom.owned)
