@@ -344,7 +344,7 @@ def our_arm(args):
         host_in = torch.empty((V, 4, 3, 3), dtype=torch.complex128, pin_memory=True)
         host_in.numpy()[...] = start.to_numpy()
         host_out = [torch.empty((V, 4, 3, 3), dtype=torch.complex128, pin_memory=True) for _ in range(2)]
-        n_e2e = max(2, min(args.steps, 10))
+        n_e2e = max(2, args.steps)  # the same number of trajectories as the device-resident measurement
         g_e2e = q.GaugeField(geo)
         # allocate the staging slots outside the timed region (no prefetch left pending)
         g_e2e.upload_host_pipelined(host_in.data_ptr(), host_in.data_ptr())
