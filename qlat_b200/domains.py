@@ -157,6 +157,15 @@ class Domains:
             self._bufs[(key, nbytes, device)] = b
         return b
 
+    def _host_buffer(self, key, nbytes):
+        """A cached pinned host buffer (the gloo path's messages)."""
+        import torch
+        b = self._bufs.get(("host", key, nbytes))
+        if b is None:
+            b = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            self._bufs[("host", key, nbytes)] = b
+        return b
+
     def faces(self, k: int):
         """The boxes of direction k's exchange: (the owned layers sent down,
         the owned layers sent up, the lower halo, the upper halo), each as
@@ -219,7 +228,11 @@ class Domains:
         call("qgb_field_pack_box", handle, i4(*lo), i4(*n), ctypes.c_void_p(buf.data_ptr()))
         synchronize()
         # one rank exchanges with itself: the message stays on the device
-        return buf if (self.backend == "nccl" or self.world == 1) else buf.cpu()
+        if self.backend == "nccl" or self.world == 1:
+            return buf
+        host = self._host_buffer(key, nb.value)
+        host.copy_(buf)
+        return host
 
     def _unpack(self, handle, box, msg) -> None:
         import torch
@@ -227,10 +240,22 @@ class Domains:
         i4 = ctypes.c_int32 * 4
         (lo, n) = box
         if msg.device.type != "cuda":
-            msg = msg.to("cuda")
+            dev = self._buffer(("recv_dev", box), msg.numel(), "cuda")
+            dev.copy_(msg)
+            msg = dev
         torch.cuda.current_stream().synchronize()
         call("qgb_field_unpack_box", handle, i4(*lo), i4(*n), ctypes.c_void_p(msg.data_ptr()))
         synchronize()
+
+    def _recv_buffer(self, key, like):
+        """A cached receive buffer of the shape, type and device of ``like``."""
+        import torch
+        full = key + (tuple(like.shape), like.dtype, like.device.type)
+        b = self._bufs.get(full)
+        if b is None:
+            b = torch.empty_like(like)
+            self._bufs[full] = b
+        return b
 
     def _swap(self, k: int, send_up, send_dn):
         """Send the top owned layers of direction k up and the bottom ones
@@ -238,15 +263,12 @@ class Domains:
         top layers) and for the upper halo (the upper neighbour's bottom
         layers).  With two ranks along k both neighbours are the same rank;
         the tags keep the two messages apart."""
-        import torch
         dn, up = self.neighbours[k]
         if self.world == 1 or (dn == self.rank and up == self.rank):
             return send_up, send_dn
         dist = self._dist
-        rlo = self._bufs.setdefault(("recv_lo", k, tuple(send_up.shape), send_up.dtype, send_up.device.type),
-                                    torch.empty_like(send_up))
-        rhi = self._bufs.setdefault(("recv_hi", k, tuple(send_dn.shape), send_dn.dtype, send_dn.device.type),
-                                    torch.empty_like(send_dn))
+        rlo = self._recv_buffer(("recv_lo", k), send_up)
+        rhi = self._recv_buffer(("recv_hi", k), send_dn)
         # posted in the same order on every rank: NCCL pairs the operations
         # between two ranks in order, gloo by tag
         ops = [dist.P2POp(dist.isend, send_up, up, self.group, 2 * k),
