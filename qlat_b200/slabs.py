@@ -87,6 +87,15 @@ class TimeSlabs:
             self._bufs[(key, nbytes, device)] = b
         return b
 
+    def _host_buffer(self, key, nbytes):
+        """A cached pinned host buffer (the gloo path's messages)."""
+        import torch
+        b = self._bufs.get(("host", key, nbytes))
+        if b is None:
+            b = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            self._bufs[("host", key, nbytes)] = b
+        return b
+
     def exchange(self, f) -> None:
         """Refresh the halo slices of f from the neighbouring ranks (the ring
         of time slabs is periodic)."""
@@ -108,10 +117,18 @@ class TimeSlabs:
             rbot, rtop = up_dev, dn_dev
         else:
             on_host = self.backend != "nccl"
-            rbot, rtop = self._swap(up_dev.cpu() if on_host else up_dev, dn_dev.cpu() if on_host else dn_dev)
-            if on_host:
-                rbot = rbot.to("cuda")
-                rtop = rtop.to("cuda")
+            if on_host:  # gloo: through cached pinned host buffers
+                up_h = self._host_buffer("send_up", nbytes)
+                dn_h = self._host_buffer("send_dn", nbytes)
+                up_h.copy_(up_dev)
+                dn_h.copy_(dn_dev)
+                rbot_h, rtop_h = self._swap(up_h, dn_h)
+                rbot = self._buffer("recv_bot_dev", nbytes, "cuda")
+                rtop = self._buffer("recv_top_dev", nbytes, "cuda")
+                rbot.copy_(rbot_h)
+                rtop.copy_(rtop_h)
+            else:
+                rbot, rtop = self._swap(up_dev, dn_dev)
             torch.cuda.current_stream().synchronize()
         call("qgb_field_unpack_tslices", handle, 0, h, ctypes.c_void_p(rbot.data_ptr()))
         call("qgb_field_unpack_tslices", handle, nt + h, h, ctypes.c_void_p(rtop.data_ptr()))
